@@ -1,0 +1,188 @@
+/*
+ * warpflow_b200.h -- C ABI of libwfb200.so, the B200 (sm_100a) kernels for
+ * the warpflow-les per-step hot path: Heun RK2 stage (4th-order convection,
+ * 4th-order variable-viscosity diffusion, WALE, ghost fills) and the
+ * fractional-step projection with its red-black Gauss-Seidel multigrid.
+ *
+ * Conventions
+ *   - Every field is a C-contiguous float64 device array of (n+6)^3 doubles
+ *     indexed [i][j][k], k fastest, real cells NPL..NPL+n-1 with NPL = 3
+ *     (reference kernels.py:9-12, topology.py:15).  Only cubic grids.
+ *   - Multigrid level l >= 1 arrays are (n_l+2)^3, n_l = n >> l, one ring.
+ *     Level 0 has no arrays of its own: it reads `su` and solves into `pp`
+ *     in place.  Element type is double, or float when `mg_fp32` is set.
+ *   - All memory is allocated and owned by the caller.  Nothing here calls
+ *     cudaMalloc / cudaFree on the step path.  Only the step context keeps
+ *     CUDA graph handles.
+ *   - Every entry returns 0 on success or a WF_E* code; wf_last_error()
+ *     gives a thread-local message.  Launches are asynchronous on `stream`
+ *     (a cudaStream_t passed as void*); there are no host syncs inside
+ *     except where a function says so.
+ *   - Device-detected conditions (dt collapse, divergence, non-convergence)
+ *     are written to wf_scalars.status, which the caller reads.
+ */
+#ifndef WARPFLOW_B200_H
+#define WARPFLOW_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define WF_API __attribute__((visibility("default")))
+#else
+#define WF_API
+#endif
+
+#define WF_NPL 3
+#define WF_MAX_LEVELS 8
+#define WF_NFIELDS 13
+
+/* field slots, in the order of the reference FlowSolver.f (solver.py:43-46) */
+enum wf_field {
+  WF_U = 0, WF_V, WF_W, WF_P, WF_USTAR, WF_VSTAR, WF_WSTAR,
+  WF_UOO, WF_VOO, WF_WOO, WF_VIS, WF_SU, WF_PP
+};
+
+enum wf_err {
+  WF_OK = 0,
+  WF_EINVAL = 1,     /* bad extent / pointer / configuration */
+  WF_EUNSUPPORTED = 2,
+  WF_ECUDA = 3,      /* a CUDA call or launch failed */
+  WF_ESTATUS = 4     /* device status word reports a failure */
+};
+
+/* device status word values (wf_scalars.status) */
+enum wf_status {
+  WF_ST_OK = 0,
+  WF_ST_DT_COLLAPSE = 1,   /* solver.py:143-144 */
+  WF_ST_DIVERGED = 2,      /* solver.py:190-193 */
+  WF_ST_NOT_CONVERGED = 3, /* solver.py:205-209 (warning only) */
+  WF_ST_WAIT_TIMEOUT = 4   /* a bounded device-side wait gave up */
+};
+
+/* Device-resident scalar block of one case.  The step kernels read dt from
+ * here and write every per-step scalar back, so the host reads one small
+ * struct per step instead of the reference's 5+ blocking readbacks. */
+typedef struct wf_scalars {
+  double dt;          /* time step in use (FlowSolver.dt) */
+  double ctime;       /* simulated time (FlowSolver.ctime) */
+  double rmax;        /* last 4th-order divergence max (FlowSolver.rmax) */
+  double cfl;         /* dt_old / dtmax (FlowSolver.cfl) */
+  double dtmax;       /* min(dtvisc, dtcfl) of the last checkdt */
+  double umax, vmax, wmax, dtvisc;      /* last checkdt reductions */
+  double rmax_trace[32];                /* rmax of every outer iteration */
+  unsigned long long red[6];            /* reduction scratch (bit patterns) */
+  int32_t itime;      /* step counter (FlowSolver.itime) */
+  int32_t iters;      /* outer iterations of the last step (outer_iters) */
+  int32_t status;     /* wf_status */
+  int32_t loop;       /* device loop flag of the projection */
+  uint32_t ticket;    /* last-block-done counter */
+  int32_t pad;
+} wf_scalars;
+
+/* One cavity case: geometry, physics, numerics and the caller's buffers. */
+typedef struct wf_case {
+  int32_t n;            /* cells per axis */
+  int32_t nlev;         /* multigrid levels (config mg_levels) */
+  int32_t sgs;          /* WALE on (physics.sgs.enabled) */
+  int32_t variable_dt;  /* time.variable_dt */
+  int32_t maxcy;        /* numerics.max_outer_iters */
+  int32_t mg_fp32;      /* 0: FP64 multigrid, 1: FP32 V-cycle in FP64 defect correction */
+  int32_t n_pre, n_post, n_coarse, n_vcycles;   /* multigrid.py:257-260 */
+  double dx, dy, dz;    /* cell sizes */
+  double rrey;          /* 1/Re */
+  double cw;            /* WALE coefficient */
+  double ulid;          /* lid velocity */
+  double dt_growth, safety, eps;  /* time.dt_growth, time.safety_factor, div_tolerance */
+  double* fld[WF_NFIELDS];        /* (n+6)^3 each, order of enum wf_field */
+  void* mg_phi[WF_MAX_LEVELS];    /* level l >= 1 (entry 0 unused in FP64) */
+  void* mg_rhs[WF_MAX_LEVELS];    /* level l >= 1; in FP32 mode entry 0 is the FP32 level-0 pair */
+  wf_scalars* sc;                 /* device scalar block */
+} wf_case;
+
+/* ---- library ---------------------------------------------------------- */
+WF_API int wf_version(void);
+WF_API const char* wf_last_error(void);
+/* sizeof(wf_scalars), sizeof(wf_case) as compiled, for binding checks */
+WF_API int wf_struct_sizes(int64_t* scalars, int64_t* casebytes);
+/* solver.py:60-65 initial scalars: dt = dt0, ctime = 0, itime = 0, ... */
+WF_API int wf_scalars_init(wf_scalars* sc, double dt0, void* stream);
+/* bytes of MG workspace a case needs at each level (caller allocates) */
+WF_API int wf_mg_level_elems(int32_t n, int32_t nlev, int32_t level, int64_t* elems);
+
+/* ---- initial state ---------------------------------------------------- */
+/* kernels.py:452-471 init_noise: u = v = amp*r, w = -amp*r (uint32 hash). */
+WF_API int wf_init_noise(double* u, double* v, double* w, int32_t n, double amp,
+                  int32_t seed, void* stream);
+/* bcs.py:313-323 BoundaryKernels.apply: boundu/v/w + full-depth p mirror. */
+WF_API int wf_fill_initial(const wf_case* c, void* stream);
+
+/* ---- ghost fills (bcs.py) --------------------------------------------- */
+/* bcs.py:201-223 apply_u */
+WF_API int wf_fill_u(double* u, int32_t n, double ulid, void* stream);
+/* bcs.py:225-244 apply_v */
+WF_API int wf_fill_v(double* v, int32_t n, void* stream);
+/* bcs.py:246-265 apply_w */
+WF_API int wf_fill_w(double* w, int32_t n, void* stream);
+/* bcs.py:267-293 apply_vis */
+WF_API int wf_fill_vis(double* vis, int32_t n, double rrey, void* stream);
+/* bcs.py:295-302 apply_pbound */
+WF_API int wf_fill_pbound(double* p, int32_t n, void* stream);
+/* bcs.py:304-311 apply_p_mirror */
+WF_API int wf_fill_p_mirror(double* p, int32_t n, void* stream);
+
+/* ---- stencil operators (kernels.py) ----------------------------------- */
+/* kernels.py:53-168 conv4th_{u,v,w}; comp 0/1/2; dt read from *dt_dev. */
+WF_API int wf_conv(const wf_case* c, int32_t comp, double alpha, const double* dt_dev,
+            void* stream);
+/* kernels.py:189-225 diff4th_{u,v,w} */
+WF_API int wf_diff(const wf_case* c, int32_t comp, double alpha, const double* dt_dev,
+            void* stream);
+/* kernels.py:232-264 calvel_{u,v,w} (all three components, one launch) */
+WF_API int wf_calvel(const wf_case* c, double alpha, const double* dt_dev, void* stream);
+/* kernels.py:271-289 calmas: su = div/dt, sc->rmax = max|div dV| */
+WF_API int wf_calmas(const wf_case* c, void* stream);
+/* kernels.py:297-367 wale_viscosity (or kernels.py:442-449 fill_const when
+ * sgs is off) followed by bcs.py:267-293 apply_vis. */
+WF_API int wf_wale_vis(const wf_case* c, void* stream);
+/* solver.py:122-150 compute_dt with kernels.py:374-402: reductions and the
+ * dt / cfl update, all on the device; also itime += 1, ctime += dt. */
+WF_API int wf_checkdt(const wf_case* c, void* stream);
+/* kernels.py:405-414 add_inplace: p += pp over real cells + one ring. */
+WF_API int wf_add_ring(double* p, const double* pp, int32_t n, void* stream);
+
+/* ---- multigrid (multigrid.py) ----------------------------------------- */
+/* multigrid.py:324-337 Multigrid.solve(su, pp): pp = 4 V-cycles from zero
+ * on A pp = su (7-point Neumann, RBGS 6/6/300).  Level 0 works in place in
+ * `pp`; level >= 1 buffers come from the case. */
+WF_API int wf_mg_solve(const wf_case* c, void* stream);
+/* multigrid.py:301-322 one V-cycle on an explicit level-0 pair (phi, rhs)
+ * of (n+2)^3 doubles each (the standalone harness of tests/test_mg.py). */
+WF_API int wf_mg_vcycle(const wf_case* c, double* phi0, const double* rhs0, void* stream);
+/* multigrid.py:289-299 `nsweeps` RBGS sweeps + ring refill on level 0 pair */
+WF_API int wf_mg_relax(const wf_case* c, double* phi0, const double* rhs0,
+                int32_t nsweeps, void* stream);
+/* tests/test_mg.py:16-32 residual: *out = max|rhs - A phi| over level 0. */
+WF_API int wf_mg_residual_max(const wf_case* c, const double* phi0, const double* rhs0,
+                       double* out_dev, void* stream);
+/* bcs.py:326-360 _mk_neumann on all six faces of a level-0 pair. */
+WF_API int wf_mg_refill(const wf_case* c, double* phi0, void* stream);
+
+/* ---- whole step (solver.py:217-271) ------------------------------------ */
+typedef struct wf_stepper wf_stepper;
+/* Build the per-case step as one CUDA graph (device-side dt control and a
+ * device-driven projection loop through conditional graph nodes).  `c` is
+ * copied.  mode 0 = graph, 1 = plain stream launches with host-driven
+ * projection loop (one 8-byte readback per outer iteration). */
+WF_API int wf_stepper_create(const wf_case* c, int32_t mode, wf_stepper** out);
+/* One FlowSolver.step(): enqueue the step on `stream`.  No host sync. */
+WF_API int wf_stepper_step(wf_stepper* s, void* stream);
+WF_API int wf_stepper_destroy(wf_stepper* s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WARPFLOW_B200_H */

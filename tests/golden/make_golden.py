@@ -1,0 +1,127 @@
+"""Generate the golden vectors in this folder by running the reference
+solver's own source (warpflow-les v0.1.0: warpflow/{kernels,bcs,multigrid,
+solver,config,topology}.py) unmodified on the CPU through ``refshim/``, a
+stand-in for NVIDIA Warp and a one-rank mpi4py.
+
+Run once, in a container that has the reference checkout:
+
+    python tests/golden/make_golden.py /path/to/warpflow-les
+
+Writes ``golden_*.npz`` next to this file.  Nothing at test time reads the
+reference; tests only read the committed ``.npz`` files.
+"""
+import os
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+CASE = """
+case: {name}
+domain:  {{lx: 1.0, ly: 1.0, lz: 1.0}}
+grid:    {{nx: {n}, ny: {n}, nz: {n}}}
+physics:
+  reynolds: {re}
+  sgs: {{enabled: {sgs}, model: wale, cw: 0.46}}
+initial: {{type: rest, noise: {noise}}}
+boundaries:
+  west: wall
+  east: wall
+  south: slip
+  north: slip
+  bottom: wall
+  top: moving_lid
+  lid_velocity: {ulid}
+numerics:
+  mg_levels: {levels}
+  max_outer_iters: 30
+  div_tolerance: 1.0e-6
+time: {{n_steps: {steps}, variable_dt: {vdt}, dt_init: 3.0e-4,
+       safety_factor: 0.8, dt_growth: 1.1}}
+output: {{n_out: 100000, log_interval: 1, outdir: /tmp/wf_golden}}
+mpi: {{domains: [1, 1, 1]}}
+"""
+
+# (tag, n, levels, steps, Re, sgs, noise, ulid, variable_dt, fields-after-step)
+CAVITY_CASES = [
+    ("c8_l3_vdt", 8, 3, 3, 400, "true", 0.01, 1.0, "true", (1, 3)),
+    ("c12_l3_fdt_re100", 12, 3, 2, 100, "true", 0.01, 0.75, "false", (1, 2)),
+    ("c8_l2_nosgs", 8, 2, 2, 400, "false", 0.01, 1.0, "true", (2,)),
+    ("c16_l3_vdt", 16, 3, 1, 400, "true", 0.01, 1.0, "true", (1,)),
+]
+
+ALL_FIELDS = ("u", "v", "w", "p", "ustar", "vstar", "wstar", "uoo", "voo",
+              "woo", "vis", "su", "pp")
+
+
+def main():
+    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    sys.path.insert(0, os.path.join(HERE, "refshim"))
+    sys.path.insert(0, ref)
+    from warpflow.config import load_case
+    from warpflow.multigrid import Multigrid
+    from warpflow.solver import FlowSolver
+    from warpflow.topology import build_topology
+
+    tmp = tempfile.mkdtemp()
+    for tag, n, lev, steps, re, sgs, noise, ulid, vdt, keep in CAVITY_CASES:
+        path = os.path.join(tmp, tag + ".yaml")
+        with open(path, "w") as fh:
+            fh.write(CASE.format(name=tag, n=n, re=re, sgs=sgs, noise=noise,
+                                 ulid=ulid, levels=lev, steps=steps, vdt=vdt))
+        cfg = load_case(path)
+        topo = build_topology(cfg)
+        t0 = time.time()
+        sol = FlowSolver(cfg, topo, "cpu")
+        out = {"case_yaml": np.array(open(path).read())}
+        for name in ("u", "v", "w", "p", "vis"):
+            out["init_" + name] = sol.f[name].numpy().copy()
+        infos = []
+        for s in range(1, steps + 1):
+            info = sol.step()
+            infos.append([info["ctime"], info["dt"], info["rmax"],
+                          info["iters"], info["cfl"]])
+            if s in keep:
+                names = ALL_FIELDS if s == keep[0] else ("u", "v", "w", "p", "vis")
+                for name in names:
+                    out["s%d_%s" % (s, name)] = sol.f[name].numpy().copy()
+        out["info"] = np.array(infos, dtype=np.float64)
+        np.savez_compressed(os.path.join(HERE, "golden_%s.npz" % tag), **out)
+        print(tag, "%.1fs" % (time.time() - t0), infos[-1], flush=True)
+
+    # standalone multigrid harness (tests/test_mg.py:35-66): 16^3, 3 levels
+    path = os.path.join(tmp, "mg.yaml")
+    with open(path, "w") as fh:
+        fh.write(CASE.format(name="mg", n=16, re=400, sgs="true", noise=0.01,
+                             ulid=1.0, levels=3, steps=1, vdt="true"))
+    cfg = load_case(path)
+    topo = build_topology(cfg)
+    mg = Multigrid(cfg, topo, "cpu", 1.0 / 16, 1.0 / 16, 1.0 / 16)
+    lev0 = mg.levels[0]
+    rng = np.random.default_rng(0)
+    h = rng.standard_normal(lev0.rhs.shape)
+    h[0, :, :] = 0.0
+    h[-1, :, :] = 0.0
+    h[:, 0, :] = 0.0
+    h[:, -1, :] = 0.0
+    h[:, :, 0] = 0.0
+    h[:, :, -1] = 0.0
+    h[1:-1, 1:-1, 1:-1] -= h[1:-1, 1:-1, 1:-1].mean()
+    lev0.rhs.assign(h)
+    lev0.phi.zero_()
+    mg._refill(lev0)
+    out = {"rhs": h}
+    for c in range(2):
+        mg._vcycle()
+        out["phi_c%d" % c] = lev0.phi.numpy().copy()
+        out["phi1_c%d" % c] = mg.levels[1].phi.numpy().copy()
+        out["phi2_c%d" % c] = mg.levels[2].phi.numpy().copy()
+    np.savez_compressed(os.path.join(HERE, "golden_mg16_l3.npz"), **out)
+    print("mg16 done", flush=True)
+
+
+if __name__ == "__main__":
+    main()

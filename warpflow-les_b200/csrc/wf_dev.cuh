@@ -1,0 +1,74 @@
+// Device helpers shared by the libwfb200 kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace wf {
+
+// bit patterns of non-negative doubles order like the doubles themselves,
+// so max/min reductions of |x| and of positive values are integer atomics
+__device__ __forceinline__ unsigned long long dbits(double x) {
+  return (unsigned long long)__double_as_longlong(x);
+}
+__device__ __forceinline__ double bitsd(unsigned long long b) {
+  return __longlong_as_double((long long)b);
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_min(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// block-wide max / min; every thread gets the result (blockDim <= 1024)
+__device__ __forceinline__ double block_max(double v, double* sm) {
+  v = warp_max(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  const int nw = (blockDim.x + 31) >> 5;
+  __syncthreads();
+  if (l == 0) sm[w] = v;
+  __syncthreads();
+  v = (threadIdx.x < nw) ? sm[threadIdx.x] : 0.0;
+  if (w == 0) v = warp_max(v);
+  if (threadIdx.x == 0) sm[0] = v;
+  __syncthreads();
+  return sm[0];
+}
+__device__ __forceinline__ double block_min(double v, double* sm, double ident) {
+  v = warp_min(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  const int nw = (blockDim.x + 31) >> 5;
+  __syncthreads();
+  if (l == 0) sm[w] = v;
+  __syncthreads();
+  v = (threadIdx.x < nw) ? sm[threadIdx.x] : ident;
+  if (w == 0) v = warp_min(v);
+  if (threadIdx.x == 0) sm[0] = v;
+  __syncthreads();
+  return sm[0];
+}
+
+// "last block done": returns true in exactly one block, after every other
+// block's preceding global writes are visible; resets the ticket.
+__device__ __forceinline__ bool last_block(unsigned int* ticket) {
+  __shared__ bool is_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned int t = atomicAdd(ticket, 1u);
+    is_last = (t == gridDim.x * gridDim.y * gridDim.z - 1);
+    if (is_last) {
+      __threadfence();
+      *ticket = 0u;
+    }
+  }
+  __syncthreads();
+  return is_last;
+}
+
+}  // namespace wf

@@ -1,0 +1,74 @@
+// Internal declarations shared by the libwfb200 translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+
+#include "warpflow_b200.h"
+
+namespace wf {
+
+constexpr int NPL = WF_NPL;
+
+// ---- error plumbing ------------------------------------------------------
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define WF_CK(expr)                                                  \
+  do {                                                               \
+    cudaError_t _e = (expr);                                         \
+    if (_e != cudaSuccess) return ::wf::cuda_fail(_e, #expr);        \
+  } while (0)
+
+#define WF_CKL(what)                                                 \
+  do {                                                               \
+    cudaError_t _e = cudaGetLastError();                             \
+    if (_e != cudaSuccess) return ::wf::cuda_fail(_e, what);         \
+  } while (0)
+
+#define WF_TRY(expr)                                                 \
+  do {                                                               \
+    int _r = (expr);                                                 \
+    if (_r != WF_OK) return _r;                                      \
+  } while (0)
+
+inline int64_t padded(int n) { return (int64_t)n + 2 * NPL; }
+
+int validate_case(const wf_case& c);
+
+// ---- ghost fills ---------------------------------------------------------
+enum FillKind { FILL_U = 0, FILL_V, FILL_W, FILL_VIS, FILL_PBOUND, FILL_PMIRROR };
+struct FillReq {
+  double* fld;
+  int kind;
+  double val;   // ulid for u, 1/Re for vis
+};
+// up to 3 independent field fills, executed as 3 ordered axis phases
+int launch_fills(const FillReq* reqs, int nreq, int n, cudaStream_t s);
+
+// ---- operators -----------------------------------------------------------
+int launch_init_noise(double* u, double* v, double* w, int n, double amp,
+                      int seed, cudaStream_t s);
+int launch_checkdt(const wf_case& c, cudaStream_t s);
+int launch_copy_oo(const wf_case& c, cudaStream_t s);
+int launch_wale(const wf_case& c, cudaStream_t s);
+int launch_conv(const wf_case& c, int comp, double alpha, const double* dt, cudaStream_t s);
+int launch_diff(const wf_case& c, int comp, double alpha, const double* dt, cudaStream_t s);
+int launch_calvel(const wf_case& c, double alpha, const double* dt, cudaStream_t s);
+// calmas + projection-loop control (sets graph conditionals when h != 0)
+int launch_calmas(const wf_case& c, unsigned long long h_if,
+                  unsigned long long h_loop, cudaStream_t s);
+int launch_add_ring(double* p, const double* pp, int n, cudaStream_t s);
+int launch_scalars_init(wf_scalars* sc, double dt0, cudaStream_t s);
+
+// ---- multigrid -----------------------------------------------------------
+int mg_solve(const wf_case& c, cudaStream_t s);
+int mg_vcycle_pair(const wf_case& c, double* phi0, const double* rhs0, cudaStream_t s);
+int mg_relax_pair(const wf_case& c, double* phi0, const double* rhs0, int nsweeps,
+                  cudaStream_t s);
+int mg_refill_pair(const wf_case& c, double* phi0, cudaStream_t s);
+int mg_residual_max_pair(const wf_case& c, const double* phi0, const double* rhs0,
+                         double* out, cudaStream_t s);
+
+}  // namespace wf

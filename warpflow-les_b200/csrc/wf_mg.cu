@@ -1,0 +1,429 @@
+// Geometric multigrid for the pressure Poisson equation (reference
+// multigrid.py): 7-point Neumann operator with the boundary coefficients
+// zeroed (multigrid.py:23-67), red-black Gauss-Seidel with one ring refill
+// per full sweep (multigrid.py:70-90, 289-299), full-weighting residual
+// restriction (93-119), trilinear prolongation (122-146) and the fixed
+// V-cycle schedule (301-337).
+//
+// No coefficient arrays: the face coefficient is 1/h^2 of the level or 0
+// across a physical face, decided from the cell index.
+//
+// Ring refill fused into the updates: a ring cell of a face has exactly one
+// real neighbour and is multiplied by a zero coefficient everywhere, so the
+// thread that updates that neighbour writes the mirror right away.  At the
+// end of each sweep (and after prolongation) the ring therefore holds what
+// the reference's separate refill launch writes; edge and corner ring cells
+// are never written, as in bcs.py:326-360.
+//
+// Level 0 works in place: phi is the (n+2)^3 core of `pp` and rhs the core
+// of `su`, both with the padded (n+6) strides.
+#include <algorithm>
+#include <vector>
+
+#include "wf_dev.cuh"
+#include "wf_internal.h"
+
+namespace wf {
+
+constexpr int MG_TPB = 256;
+
+template <class T>
+struct Lvl {
+  T* phi;        // ring cell (0,0,0)
+  const T* rhs;  // same layout as phi
+  int n;         // real cells per axis
+  long sI, sJ;   // strides (k stride 1)
+  T ax, ay, az;  // 1/h^2 per axis of this level
+};
+
+template <class T>
+__device__ __forceinline__ long lid(const Lvl<T>& L, int i, int j, int k) {
+  return (long)i * L.sI + (long)j * L.sJ + k;
+}
+
+// write the face-ring mirrors of real cell (i,j,k) (0-based) with value x
+template <class T>
+__device__ __forceinline__ void ring_mirror(const Lvl<T>& L, int i, int j, int k, long c,
+                                            T x) {
+  const int n = L.n;
+  if (i == 0) L.phi[c - L.sI] = x;
+  if (i == n - 1) L.phi[c + L.sI] = x;
+  if (j == 0) L.phi[c - L.sJ] = x;
+  if (j == n - 1) L.phi[c + L.sJ] = x;
+  if (k == 0) L.phi[c - 1] = x;
+  if (k == n - 1) L.phi[c + 1] = x;
+}
+
+// one colour half-sweep (multigrid.py:70-90): update where (i+j+k+color)%2==1
+template <class T>
+__global__ void __launch_bounds__(MG_TPB) k_rbgs(const Lvl<T> L, int color) {
+  const int n = L.n;
+  const int nh = (n + 1) >> 1;
+  const long tot = (long)n * n * nh;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
+       t += (long)gridDim.x * blockDim.x) {
+    const int kk = (int)(t % nh);
+    const int j = (int)((t / nh) % n);
+    const int i = (int)(t / ((long)nh * n));
+    const int k = 2 * kk + ((1 + i + j + color) & 1);
+    if (k >= n) continue;
+    const long c = lid(L, i + 1, j + 1, k + 1);
+    const T aw = i > 0 ? L.ax : T(0), ae = i < n - 1 ? L.ax : T(0);
+    const T as = j > 0 ? L.ay : T(0), an = j < n - 1 ? L.ay : T(0);
+    const T ab = k > 0 ? L.az : T(0), at = k < n - 1 ? L.az : T(0);
+    const T ap = -(aw + ae + as + an + ab + at);
+    const T* phi = L.phi;
+    const T s = aw * phi[c - L.sI] + ae * phi[c + L.sI] + as * phi[c - L.sJ] +
+                an * phi[c + L.sJ] + ab * phi[c - 1] + at * phi[c + 1];
+    const T x = (L.rhs[c] - s) / ap;
+    L.phi[c] = x;
+    ring_mirror(L, i, j, k, c, x);
+  }
+}
+
+// restriction (multigrid.py:93-119): rhs_c = 1/8 sum of the 8 fine residuals
+template <class T>
+__global__ void __launch_bounds__(MG_TPB) k_restrict(const Lvl<T> F, T* rhs_c, Lvl<T> C) {
+  const int nc = C.n, n = F.n;
+  const long tot = (long)nc * nc * nc;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
+       t += (long)gridDim.x * blockDim.x) {
+    const int ck = (int)(t % nc);
+    const int cj = (int)((t / nc) % nc);
+    const int ci = (int)(t / ((long)nc * nc));
+    T acc = T(0);
+#pragma unroll
+    for (int di = 0; di < 2; ++di)
+#pragma unroll
+      for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+        for (int dk = 0; dk < 2; ++dk) {
+          const int i = 2 * ci + di, j = 2 * cj + dj, k = 2 * ck + dk;
+          const long c = lid(F, i + 1, j + 1, k + 1);
+          const T aw = i > 0 ? F.ax : T(0), ae = i < n - 1 ? F.ax : T(0);
+          const T as = j > 0 ? F.ay : T(0), an = j < n - 1 ? F.ay : T(0);
+          const T ab = k > 0 ? F.az : T(0), at = k < n - 1 ? F.az : T(0);
+          const T ap = -(aw + ae + as + an + ab + at);
+          const T* p = F.phi;
+          const T res = F.rhs[c] - (aw * p[c - F.sI] + ae * p[c + F.sI] + as * p[c - F.sJ] +
+                                    an * p[c + F.sJ] + ab * p[c - 1] + at * p[c + 1] +
+                                    ap * p[c]);
+          acc = acc + res;
+        }
+    rhs_c[lid(C, ci + 1, cj + 1, ck + 1)] = acc * T(0.125);
+  }
+}
+
+// zero a whole (n+2)^3 ring-layout level array
+template <class T>
+__global__ void k_zero(T* a, long cnt) {
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < cnt;
+       t += (long)gridDim.x * blockDim.x)
+    a[t] = T(0);
+}
+
+// zero a (n+2)^3 block embedded with strides (sI, sJ)
+template <class T>
+__global__ void k_zero_strided(T* a, int m, long sI, long sJ) {
+  const long tot = (long)m * m * m;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
+       t += (long)gridDim.x * blockDim.x) {
+    const int k = (int)(t % m);
+    const int j = (int)((t / m) % m);
+    const int i = (int)(t / ((long)m * m));
+    a[(long)i * sI + (long)j * sJ + k] = T(0);
+  }
+}
+
+// prolongation (multigrid.py:122-146) + the ring refill that follows it
+template <class T>
+__global__ void __launch_bounds__(MG_TPB) k_prolong(const Lvl<T> C, Lvl<T> F) {
+  const int n = F.n;
+  const long tot = (long)n * n * n;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
+       t += (long)gridDim.x * blockDim.x) {
+    const int k = (int)(t % n);
+    const int j = (int)((t / n) % n);
+    const int i = (int)(t / ((long)n * n));
+    const int c0x = (i % 2 == 0) ? i / 2 - 1 : i / 2;
+    const T wx0 = (i % 2 == 0) ? T(0.25) : T(0.75);
+    const int c0y = (j % 2 == 0) ? j / 2 - 1 : j / 2;
+    const T wy0 = (j % 2 == 0) ? T(0.25) : T(0.75);
+    const int c0z = (k % 2 == 0) ? k / 2 - 1 : k / 2;
+    const T wz0 = (k % 2 == 0) ? T(0.25) : T(0.75);
+    T acc = T(0);
+#pragma unroll
+    for (int di = 0; di < 2; ++di) {
+      const T wxi = di == 0 ? wx0 : T(1) - wx0;
+#pragma unroll
+      for (int dj = 0; dj < 2; ++dj) {
+        const T wyj = dj == 0 ? wy0 : T(1) - wy0;
+#pragma unroll
+        for (int dk = 0; dk < 2; ++dk) {
+          const T wzk = dk == 0 ? wz0 : T(1) - wz0;
+          acc = acc + wxi * wyj * wzk * C.phi[lid(C, c0x + di + 1, c0y + dj + 1, c0z + dk + 1)];
+        }
+      }
+    }
+    const long c = lid(F, i + 1, j + 1, k + 1);
+    const T x = F.phi[c] + acc;
+    F.phi[c] = x;
+    ring_mirror(F, i, j, k, c, x);
+  }
+}
+
+// ---- a whole relax() of a small level inside one CTA's shared memory ------
+// phi and rhs of the real cells live in shared memory ([i][j][k]); the
+// ring is not needed there because every ring term has a zero coefficient.
+// After the last sweep the interior and the face rings go back to global.
+template <class T>
+__global__ void __launch_bounds__(1024) k_relax_smem(Lvl<T> L, int nsweeps) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* sphi = reinterpret_cast<T*>(smraw);
+  const int n = L.n;
+  const int n3 = n * n * n;
+  T* srhs = sphi + n3;
+  for (int t = threadIdx.x; t < n3; t += blockDim.x) {
+    const int k = t % n, j = (t / n) % n, i = t / (n * n);
+    const long c = lid(L, i + 1, j + 1, k + 1);
+    sphi[t] = L.phi[c];
+    srhs[t] = L.rhs[c];
+  }
+  __syncthreads();
+  const int nh = (n + 1) >> 1;
+  const int half = n * n * nh;
+  const int SI = n * n, SJ = n;
+  for (int s = 0; s < nsweeps; ++s) {
+    for (int color = 0; color < 2; ++color) {
+      for (int t = threadIdx.x; t < half; t += blockDim.x) {
+        const int kk = t % nh;
+        const int j = (t / nh) % n;
+        const int i = t / (nh * n);
+        const int k = 2 * kk + ((1 + i + j + color) & 1);
+        if (k >= n) continue;
+        const int c = i * SI + j * SJ + k;
+        const T aw = i > 0 ? L.ax : T(0), ae = i < n - 1 ? L.ax : T(0);
+        const T as = j > 0 ? L.ay : T(0), an = j < n - 1 ? L.ay : T(0);
+        const T ab = k > 0 ? L.az : T(0), at = k < n - 1 ? L.az : T(0);
+        const T ap = -(aw + ae + as + an + ab + at);
+        // out-of-range neighbours have a zero coefficient; read a valid
+        // cell instead (the product is then exactly zero)
+        const T W = sphi[i > 0 ? c - SI : c], E = sphi[i < n - 1 ? c + SI : c];
+        const T S = sphi[j > 0 ? c - SJ : c], N = sphi[j < n - 1 ? c + SJ : c];
+        const T B = sphi[k > 0 ? c - 1 : c], Tt = sphi[k < n - 1 ? c + 1 : c];
+        const T sum = aw * W + ae * E + as * S + an * N + ab * B + at * Tt;
+        sphi[c] = (srhs[c] - sum) / ap;
+      }
+      __syncthreads();
+    }
+  }
+  for (int t = threadIdx.x; t < n3; t += blockDim.x) {
+    const int k = t % n, j = (t / n) % n, i = t / (n * n);
+    const long c = lid(L, i + 1, j + 1, k + 1);
+    const T x = sphi[t];
+    L.phi[c] = x;
+    if (nsweeps > 0) ring_mirror(L, i, j, k, c, x);
+  }
+}
+
+// max |rhs - A phi| over a level (tests/test_mg.py:16-32)
+__global__ void k_resmax(const Lvl<double> L, double* out, unsigned int* ticket,
+                         unsigned long long* acc) {
+  __shared__ double sm[32];
+  const int n = L.n;
+  const long tot = (long)n * n * n;
+  double m = 0.0;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
+       t += (long)gridDim.x * blockDim.x) {
+    const int k = (int)(t % n);
+    const int j = (int)((t / n) % n);
+    const int i = (int)(t / ((long)n * n));
+    const long c = lid(L, i + 1, j + 1, k + 1);
+    const double aw = i > 0 ? L.ax : 0.0, ae = i < n - 1 ? L.ax : 0.0;
+    const double as = j > 0 ? L.ay : 0.0, an = j < n - 1 ? L.ay : 0.0;
+    const double ab = k > 0 ? L.az : 0.0, at = k < n - 1 ? L.az : 0.0;
+    const double ap = -(aw + ae + as + an + ab + at);
+    const double* p = L.phi;
+    const double r = L.rhs[c] - (ap * p[c] + aw * p[c - L.sI] + ae * p[c + L.sI] +
+                                 as * p[c - L.sJ] + an * p[c + L.sJ] + ab * p[c - 1] +
+                                 at * p[c + 1]);
+    m = fmax(m, fabs(r));
+  }
+  m = block_max(m, sm);
+  if (threadIdx.x == 0) atomicMax(acc, dbits(m));
+  if (!last_block(ticket)) return;
+  if (threadIdx.x == 0) {
+    *out = bitsd(atomicAdd(acc, 0ull));
+    *acc = 0ull;
+  }
+}
+
+// --------------------------------------------------------------------------
+// host side
+// --------------------------------------------------------------------------
+static inline int mg_blocks(long work) {
+  long b = (work + MG_TPB - 1) / MG_TPB;
+  b = std::min<long>(b, 148L * 8);
+  return (int)std::max<long>(b, 1);
+}
+
+template <class T>
+static size_t smem_bytes(int n) {
+  return 2ull * (size_t)n * n * n * sizeof(T);
+}
+
+constexpr size_t SMEM_CAP = 220 * 1024;
+
+template <class T>
+static int relax(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
+  if (nsweeps <= 0) return WF_OK;
+  const size_t sb = smem_bytes<T>(L.n);
+  if (sb <= SMEM_CAP) {
+    static bool attr_set = false;
+    if (!attr_set) {
+      WF_CK(cudaFuncSetAttribute(k_relax_smem<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)SMEM_CAP));
+      attr_set = true;
+    }
+    const int n3 = L.n * L.n * L.n;
+    int tpb = 1024;
+    if (n3 / 2 < 1024) tpb = std::max(32, ((n3 / 2 + 31) / 32) * 32);
+    k_relax_smem<T><<<1, tpb, sb, s>>>(L, nsweeps);
+    WF_CKL("k_relax_smem");
+    return WF_OK;
+  }
+  const long half = (long)L.n * L.n * ((L.n + 1) / 2);
+  const int nb = mg_blocks(half);
+  for (int sw = 0; sw < nsweeps; ++sw) {
+    k_rbgs<T><<<nb, MG_TPB, 0, s>>>(L, 0);
+    k_rbgs<T><<<nb, MG_TPB, 0, s>>>(L, 1);
+  }
+  WF_CKL("k_rbgs");
+  return WF_OK;
+}
+
+template <class T>
+static int vcycle(std::vector<Lvl<T>>& lv, const wf_case& c, cudaStream_t s) {
+  const int L = (int)lv.size();
+  for (int l = 0; l < L; ++l) {
+    if (l > 0) {
+      Lvl<T>& C = lv[l];
+      const long m = (long)C.n + 2;
+      k_zero<T><<<mg_blocks(m * m * m), MG_TPB, 0, s>>>(C.phi, m * m * m);
+      WF_CKL("k_zero");
+      k_restrict<T><<<mg_blocks((long)C.n * C.n * C.n), MG_TPB, 0, s>>>(
+          lv[l - 1], const_cast<T*>(C.rhs), C);
+      WF_CKL("k_restrict");
+    }
+    WF_TRY(relax(lv[l], l < L - 1 ? c.n_pre : c.n_coarse, s));
+  }
+  for (int l = L - 2; l >= 0; --l) {
+    k_prolong<T><<<mg_blocks((long)lv[l].n * lv[l].n * lv[l].n), MG_TPB, 0, s>>>(lv[l + 1],
+                                                                                 lv[l]);
+    WF_CKL("k_prolong");
+    WF_TRY(relax(lv[l], c.n_post, s));
+  }
+  return WF_OK;
+}
+
+// build the level views of a case; level 0 = (phi0, rhs0) with strides sI, sJ
+template <class T>
+static int build_levels(const wf_case& c, T* phi0, const T* rhs0, long sI, long sJ,
+                        std::vector<Lvl<T>>& lv) {
+  lv.clear();
+  if (c.nlev < 1 || c.nlev > WF_MAX_LEVELS) return fail(WF_EINVAL, "nlev out of range");
+  for (int l = 0; l < c.nlev; ++l) {
+    Lvl<T> L;
+    const double s2 = (double)(1 << l);
+    const double dxl = c.dx * s2, dyl = c.dy * s2, dzl = c.dz * s2;
+    L.ax = (T)(1.0 / (dxl * dxl));
+    L.ay = (T)(1.0 / (dyl * dyl));
+    L.az = (T)(1.0 / (dzl * dzl));
+    L.n = c.n >> l;
+    if ((L.n << l) != c.n || L.n < 1)
+      return fail(WF_EINVAL, "n must be divisible by 2^(nlev-1)");
+    if (l == 0) {
+      L.phi = phi0;
+      L.rhs = rhs0;
+      L.sI = sI;
+      L.sJ = sJ;
+    } else {
+      if (!c.mg_phi[l] || !c.mg_rhs[l]) return fail(WF_EINVAL, "missing multigrid level buffer");
+      L.phi = (T*)c.mg_phi[l];
+      L.rhs = (const T*)c.mg_rhs[l];
+      L.sJ = L.n + 2;
+      L.sI = (long)(L.n + 2) * (L.n + 2);
+    }
+    lv.push_back(L);
+  }
+  return WF_OK;
+}
+
+int mg_solve(const wf_case& c, cudaStream_t s) {
+  if (c.mg_fp32) return fail(WF_EUNSUPPORTED, "mixed-precision solve not built");
+  const long P = padded(c.n);
+  const long off = (long)(NPL - 1) * (P * P + P + 1);
+  double* pp = c.fld[WF_PP];
+  const double* su = c.fld[WF_SU];
+  std::vector<Lvl<double>> lv;
+  WF_TRY(build_levels<double>(c, pp + off, su + off, P * P, P, lv));
+  // multigrid.py:332-333: pp and level-0 phi start from zero
+  k_zero<double><<<mg_blocks(P * P * P), MG_TPB, 0, s>>>(pp, P * P * P);
+  WF_CKL("k_zero pp");
+  for (int cyc = 0; cyc < c.n_vcycles; ++cyc) WF_TRY(vcycle<double>(lv, c, s));
+  return WF_OK;
+}
+
+int mg_vcycle_pair(const wf_case& c, double* phi0, const double* rhs0, cudaStream_t s) {
+  const long m = c.n + 2;
+  std::vector<Lvl<double>> lv;
+  WF_TRY(build_levels<double>(c, phi0, rhs0, m * m, m, lv));
+  return vcycle<double>(lv, c, s);
+}
+
+int mg_relax_pair(const wf_case& c, double* phi0, const double* rhs0, int nsweeps,
+                  cudaStream_t s) {
+  const long m = c.n + 2;
+  std::vector<Lvl<double>> lv;
+  WF_TRY(build_levels<double>(c, phi0, rhs0, m * m, m, lv));
+  return relax<double>(lv[0], nsweeps, s);
+}
+
+__global__ void k_refill(Lvl<double> L) {
+  const int n = L.n;
+  const long tot = (long)n * n;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
+       t += (long)gridDim.x * blockDim.x) {
+    const int a = 1 + (int)(t / n), b = 1 + (int)(t % n);
+    double* p = L.phi;
+    p[lid(L, 0, a, b)] = p[lid(L, 1, a, b)];
+    p[lid(L, n + 1, a, b)] = p[lid(L, n, a, b)];
+    p[lid(L, a, 0, b)] = p[lid(L, a, 1, b)];
+    p[lid(L, a, n + 1, b)] = p[lid(L, a, n, b)];
+    p[lid(L, a, b, 0)] = p[lid(L, a, b, 1)];
+    p[lid(L, a, b, n + 1)] = p[lid(L, a, b, n)];
+  }
+}
+
+int mg_refill_pair(const wf_case& c, double* phi0, cudaStream_t s) {
+  const long m = c.n + 2;
+  std::vector<Lvl<double>> lv;
+  WF_TRY(build_levels<double>(c, phi0, phi0, m * m, m, lv));
+  k_refill<<<mg_blocks((long)c.n * c.n), MG_TPB, 0, s>>>(lv[0]);
+  WF_CKL("k_refill");
+  return WF_OK;
+}
+
+int mg_residual_max_pair(const wf_case& c, const double* phi0, const double* rhs0,
+                         double* out, cudaStream_t s) {
+  if (!c.sc) return fail(WF_EINVAL, "residual needs the case scalar block");
+  const long m = c.n + 2;
+  std::vector<Lvl<double>> lv;
+  WF_TRY(build_levels<double>(c, const_cast<double*>(phi0), rhs0, m * m, m, lv));
+  k_resmax<<<mg_blocks((long)c.n * c.n * c.n), MG_TPB, 0, s>>>(lv[0], out, &c.sc->ticket,
+                                                               &c.sc->red[5]);
+  WF_CKL("k_resmax");
+  return WF_OK;
+}
+
+}  // namespace wf

@@ -1,0 +1,581 @@
+// Stencil operators of one LES step (reference kernels.py) and the device
+// side of the time-step control (solver.py compute_dt) and of the
+// projection loop (solver.py _project).
+//
+// Field layout: (n+6)^3 doubles, [i][j][k] with k contiguous, real cells
+// NPL..NPL+n-1.  One thread per output cell; consecutive threads walk k so
+// every access of a warp is a contiguous run.
+#include "wf_dev.cuh"
+#include "wf_internal.h"
+
+namespace wf {
+
+constexpr int TPB = 256;
+
+struct Geo {
+  long P, sI, sJ;   // padded extent and strides
+  int n;
+  __device__ __forceinline__ long at(int i, int j, int k) const {
+    return (long)i * sI + (long)j * sJ + k;
+  }
+};
+
+static inline Geo geo_of(int n) {
+  Geo g;
+  g.n = n;
+  g.P = n + 2 * NPL;
+  g.sJ = g.P;
+  g.sI = g.P * g.P;
+  return g;
+}
+
+static inline int nblocks(long work, int tpb = TPB, int cap = 148 * 16) {
+  long b = (work + tpb - 1) / tpb;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+#define LD(p, idx) __ldg((p) + (idx))
+
+// --------------------------------------------------------------------------
+// scalar block
+// --------------------------------------------------------------------------
+__global__ void k_scalars_init(wf_scalars* sc, double dt0) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  sc->dt = dt0;
+  sc->ctime = 0.0;
+  sc->rmax = 0.0;
+  sc->cfl = 0.0;
+  sc->dtmax = 0.0;
+  sc->umax = sc->vmax = sc->wmax = 0.0;
+  sc->dtvisc = 0.0;
+  for (int i = 0; i < 32; ++i) sc->rmax_trace[i] = 0.0;
+  sc->red[0] = sc->red[1] = sc->red[2] = 0ull;
+  sc->red[3] = dbits(1.0e10);  // solver.py:127 initialiser of the min
+  sc->red[4] = 0ull;
+  sc->red[5] = 0ull;
+  sc->itime = 0;
+  sc->iters = 0;
+  sc->status = WF_ST_OK;
+  sc->loop = 0;
+  sc->ticket = 0u;
+  sc->pad = 0;
+}
+
+int launch_scalars_init(wf_scalars* sc, double dt0, cudaStream_t s) {
+  if (!sc) return fail(WF_EINVAL, "null scalar block");
+  k_scalars_init<<<1, 32, 0, s>>>(sc, dt0);
+  WF_CKL("k_scalars_init");
+  return WF_OK;
+}
+
+// --------------------------------------------------------------------------
+// init_noise (kernels.py:452-471)
+// --------------------------------------------------------------------------
+__global__ void k_init_noise(double* u, double* v, double* w, Geo g, double amp,
+                             int seed) {
+  const long tot = (long)g.n * g.n * g.n;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
+       t += (long)gridDim.x * blockDim.x) {
+    const int k = NPL + (int)(t % g.n);
+    const int j = NPL + (int)((t / g.n) % g.n);
+    const int i = NPL + (int)(t / ((long)g.n * g.n));
+    uint32_t h = ((uint32_t)i * 73856093u) ^ ((uint32_t)j * 19349663u) ^
+                 ((uint32_t)k * 83492791u) ^ (uint32_t)seed;
+    h = h ^ (h >> 13);
+    h = h * 1274126177u;
+    h = h ^ (h >> 16);
+    const double r = ((double)h / 4294967295.0) * 2.0 - 1.0;
+    const long id = g.at(i, j, k);
+    u[id] = amp * r;
+    v[id] = amp * r;
+    w[id] = -amp * r;
+  }
+}
+
+int launch_init_noise(double* u, double* v, double* w, int n, double amp, int seed,
+                      cudaStream_t s) {
+  if (!u || !v || !w || n < 1) return fail(WF_EINVAL, "init_noise: bad args");
+  Geo g = geo_of(n);
+  k_init_noise<<<nblocks((long)n * n * n), TPB, 0, s>>>(u, v, w, g, amp, seed);
+  WF_CKL("k_init_noise");
+  return WF_OK;
+}
+
+// --------------------------------------------------------------------------
+// checkdt (solver.py:122-150, kernels.py:374-402): max|u|, max|v|, max|w|
+// and the viscous/advective min in one pass; the last block finishes the
+// dt update on the device.
+// --------------------------------------------------------------------------
+__global__ void __launch_bounds__(TPB) k_checkdt(const wf_case c, Geo g) {
+  __shared__ double sm[32];
+  const double* u = c.fld[WF_U];
+  const double* v = c.fld[WF_V];
+  const double* w = c.fld[WF_W];
+  const double* vis = c.fld[WF_VIS];
+  const double dx = c.dx, dy = c.dy, dz = c.dz;
+  const double inv2 = 1.0 / (dx * dx) + 1.0 / (dy * dy) + 1.0 / (dz * dz);
+  double mu = 0.0, mv = 0.0, mw = 0.0, mdt = 1.0e10;
+  const long tot = (long)g.n * g.n * g.n;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
+       t += (long)gridDim.x * blockDim.x) {
+    const int k = NPL + (int)(t % g.n);
+    const int j = NPL + (int)((t / g.n) % g.n);
+    const int i = NPL + (int)(t / ((long)g.n * g.n));
+    const long id = g.at(i, j, k);
+    const double uu = LD(u, id), vv = LD(v, id), ww = LD(w, id);
+    mu = fmax(mu, fabs(uu));
+    mv = fmax(mv, fabs(vv));
+    mw = fmax(mw, fabs(ww));
+    const double uc = 0.5 * (uu + LD(u, id - g.sI));
+    const double vc = 0.5 * (vv + LD(v, id - g.sJ));
+    const double wc = 0.5 * (ww + LD(w, id - 1));
+    const double val = 1.0 / (fabs(uc) / dx + fabs(vc) / dy + fabs(wc) / dz +
+                              2.0 * LD(vis, id) * inv2 + 1.0e-30);
+    mdt = fmin(mdt, val);
+  }
+  mu = block_max(mu, sm);
+  mv = block_max(mv, sm);
+  mw = block_max(mw, sm);
+  mdt = block_min(mdt, sm, 1.0e10);
+  wf_scalars* sc = c.sc;
+  if (threadIdx.x == 0) {
+    atomicMax(&sc->red[0], dbits(mu));
+    atomicMax(&sc->red[1], dbits(mv));
+    atomicMax(&sc->red[2], dbits(mw));
+    atomicMin(&sc->red[3], dbits(mdt));
+  }
+  if (!last_block(&sc->ticket)) return;
+  if (threadIdx.x != 0) return;
+  const double umax = bitsd(atomicAdd(&sc->red[0], 0ull));
+  const double vmax = bitsd(atomicAdd(&sc->red[1], 0ull));
+  const double wmax = bitsd(atomicAdd(&sc->red[2], 0ull));
+  const double dtvisc = bitsd(atomicAdd(&sc->red[3], 0ull));
+  sc->red[0] = sc->red[1] = sc->red[2] = 0ull;
+  sc->red[3] = dbits(1.0e10);
+  const double big = 1.0e10;
+  double dtcfl = big;
+  if (umax > 0.0) dtcfl = fmin(dtcfl, dx / umax);
+  if (vmax > 0.0) dtcfl = fmin(dtcfl, dy / vmax);
+  if (wmax > 0.0) dtcfl = fmin(dtcfl, dz / wmax);
+  const double dtmax = fmin(dtvisc, dtcfl);
+  sc->umax = umax;
+  sc->vmax = vmax;
+  sc->wmax = wmax;
+  sc->dtvisc = dtvisc;
+  sc->dtmax = dtmax;
+  sc->itime += 1;
+  sc->iters = 0;
+  if (dtmax <= 0.0 || !(dtmax < big)) sc->status = WF_ST_DT_COLLAPSE;
+  const double dt_old = sc->dt;
+  sc->cfl = dt_old / dtmax;
+  double dt = dt_old;
+  if (c.variable_dt) dt = fmin(dt_old * c.dt_growth, c.safety * dtmax);
+  sc->dt = dt;
+  sc->ctime += dt;
+}
+
+int launch_checkdt(const wf_case& c, cudaStream_t s) {
+  Geo g = geo_of(c.n);
+  k_checkdt<<<nblocks((long)c.n * c.n * c.n, TPB, 148 * 4), TPB, 0, s>>>(c, g);
+  WF_CKL("k_checkdt");
+  return WF_OK;
+}
+
+// --------------------------------------------------------------------------
+// uoo/voo/woo = u/v/w over the full padded arrays (solver.py:223-225)
+// --------------------------------------------------------------------------
+__global__ void k_copy3(const double2* __restrict__ a0, double2* __restrict__ b0,
+                        const double2* __restrict__ a1, double2* __restrict__ b1,
+                        const double2* __restrict__ a2, double2* __restrict__ b2,
+                        long n2) {
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n2;
+       t += (long)gridDim.x * blockDim.x) {
+    b0[t] = __ldg(a0 + t);
+    b1[t] = __ldg(a1 + t);
+    b2[t] = __ldg(a2 + t);
+  }
+}
+__global__ void k_copy_tail(const double* a0, double* b0, const double* a1, double* b1,
+                            const double* a2, double* b2, long idx) {
+  b0[idx] = a0[idx];
+  b1[idx] = a1[idx];
+  b2[idx] = a2[idx];
+}
+
+int launch_copy_oo(const wf_case& c, cudaStream_t s) {
+  const long tot = padded(c.n) * padded(c.n) * padded(c.n);
+  const long n2 = tot / 2;
+  k_copy3<<<nblocks(n2, TPB, 148 * 8), TPB, 0, s>>>(
+      (const double2*)c.fld[WF_U], (double2*)c.fld[WF_UOO], (const double2*)c.fld[WF_V],
+      (double2*)c.fld[WF_VOO], (const double2*)c.fld[WF_W], (double2*)c.fld[WF_WOO], n2);
+  WF_CKL("k_copy3");
+  if (tot & 1) {
+    k_copy_tail<<<1, 1, 0, s>>>(c.fld[WF_U], c.fld[WF_UOO], c.fld[WF_V], c.fld[WF_VOO],
+                                c.fld[WF_W], c.fld[WF_WOO], tot - 1);
+    WF_CKL("k_copy_tail");
+  }
+  return WF_OK;
+}
+
+// --------------------------------------------------------------------------
+// WALE eddy viscosity (kernels.py:297-367)
+// --------------------------------------------------------------------------
+__global__ void __launch_bounds__(TPB) k_wale(const wf_case c, Geo g) {
+  const double* u = c.fld[WF_U];
+  const double* v = c.fld[WF_V];
+  const double* w = c.fld[WF_W];
+  double* vis = c.fld[WF_VIS];
+  const double dx = c.dx, dy = c.dy, dz = c.dz;
+  const double delta = pow(dx * dy * dz, 1.0 / 3.0);
+  const double ls = c.cw * delta;
+  const long sI = g.sI, sJ = g.sJ;
+  const long tot = (long)g.n * g.n * g.n;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
+       t += (long)gridDim.x * blockDim.x) {
+    const int k = NPL + (int)(t % g.n);
+    const int j = NPL + (int)((t / g.n) % g.n);
+    const int i = NPL + (int)(t / ((long)g.n * g.n));
+    const long id = g.at(i, j, k);
+#define U_(a) LD(u, id + (a))
+#define V_(a) LD(v, id + (a))
+#define W_(a) LD(w, id + (a))
+    const double dudx = (U_(0) - U_(-sI)) / dx;
+    const double dudy = (0.25 * (U_(sJ) + U_(-sI + sJ) - U_(-sJ) - U_(-sI - sJ))) / dy;
+    const double dudz = (0.25 * (U_(1) + U_(-sI + 1) - U_(-1) - U_(-sI - 1))) / dz;
+    const double dvdx = (0.25 * (V_(sI) + V_(sI - sJ) - V_(-sI) - V_(-sI - sJ))) / dx;
+    const double dvdy = (V_(0) - V_(-sJ)) / dy;
+    const double dvdz = (0.25 * (V_(1) + V_(-sJ + 1) - V_(-1) - V_(-sJ - 1))) / dz;
+    const double dwdx = (0.25 * (W_(sI) + W_(sI - 1) - W_(-sI) - W_(-sI - 1))) / dx;
+    const double dwdy = (0.25 * (W_(sJ) + W_(sJ - 1) - W_(-sJ) - W_(-sJ - 1))) / dy;
+    const double dwdz = (W_(0) - W_(-1)) / dz;
+#undef U_
+#undef V_
+#undef W_
+    const double g2xx = dudx * dudx + dudy * dvdx + dudz * dwdx;
+    const double g2yy = dvdx * dudy + dvdy * dvdy + dvdz * dwdy;
+    const double g2zz = dwdx * dudz + dwdy * dvdz + dwdz * dwdz;
+    const double g2xy = dudx * dudy + dudy * dvdy + dudz * dwdy;
+    const double g2yx = dvdx * dudx + dvdy * dvdx + dvdz * dwdx;
+    const double g2xz = dudx * dudz + dudy * dvdz + dudz * dwdz;
+    const double g2zx = dwdx * dudx + dwdy * dvdx + dwdz * dudz;
+    const double g2yz = dvdx * dudz + dvdy * dvdz + dvdz * dwdz;
+    const double g2zy = dwdx * dudy + dwdy * dvdy + dwdz * dudy;
+    const double tr = (g2xx + g2yy + g2zz) / 3.0;
+    const double sdxx = g2xx - tr, sdyy = g2yy - tr, sdzz = g2zz - tr;
+    const double sdxy = 0.5 * (g2xy + g2yx);
+    const double sdxz = 0.5 * (g2xz + g2zx);
+    const double sdyz = 0.5 * (g2yz + g2zy);
+    const double sdsd = sdxx * sdxx + sdyy * sdyy + sdzz * sdzz +
+                        2.0 * (sdxy * sdxy + sdxz * sdxz + sdyz * sdyz);
+    const double sxy = 0.5 * (dudy + dvdx);
+    const double sxz = 0.5 * (dudz + dwdx);
+    const double syz = 0.5 * (dvdz + dwdy);
+    const double ss = dudx * dudx + dvdy * dvdy + dwdz * dwdz +
+                      2.0 * (sxy * sxy + sxz * sxz + syz * syz);
+    double nut = 0.0;
+    if (sdsd > 1.0e-8) {
+      const double sdsd15 = pow(sdsd, 1.5);
+      const double denom = pow(fabs(ss), 2.5) + pow(sdsd, 1.25);
+      nut = ls * ls * sdsd15 / denom;
+    }
+    vis[id] = c.rrey + nut;
+  }
+}
+
+// vis = 1/Re on real cells (kernels.py:442-449)
+__global__ void k_fill_real(double* f, Geo g, double val) {
+  const long tot = (long)g.n * g.n * g.n;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
+       t += (long)gridDim.x * blockDim.x) {
+    const int k = NPL + (int)(t % g.n);
+    const int j = NPL + (int)((t / g.n) % g.n);
+    const int i = NPL + (int)(t / ((long)g.n * g.n));
+    f[g.at(i, j, k)] = val;
+  }
+}
+
+int launch_wale(const wf_case& c, cudaStream_t s) {
+  Geo g = geo_of(c.n);
+  const long tot = (long)c.n * c.n * c.n;
+  if (c.sgs) {
+    k_wale<<<nblocks(tot), TPB, 0, s>>>(c, g);
+    WF_CKL("k_wale");
+    FillReq r{c.fld[WF_VIS], FILL_VIS, c.rrey};
+    return launch_fills(&r, 1, c.n, s);
+  }
+  k_fill_real<<<nblocks(tot), TPB, 0, s>>>(c.fld[WF_VIS], g, c.rrey);
+  WF_CKL("k_fill_real");
+  return WF_OK;
+}
+
+// --------------------------------------------------------------------------
+// convection (kernels.py:53-168) and diffusion (kernels.py:177-225)
+// --------------------------------------------------------------------------
+// 4th-order interpolation I at `id` along stride s (kernels.py:31-46)
+__device__ __forceinline__ double I4(const double* f, long id, long s) {
+  return (-LD(f, id + s) + 9.0 * LD(f, id) + 9.0 * LD(f, id - s) - LD(f, id - 2 * s)) / 16.0;
+}
+
+// op-range dims (solver.py:99-110): the component's own axis is n-1 long
+__device__ __forceinline__ void op_dims(int comp, int n, int& ni, int& nj, int& nk) {
+  ni = nj = nk = n;
+  if (comp == 0) ni = n - 1;
+  if (comp == 1) nj = n - 1;
+  if (comp == 2) nk = n - 1;
+}
+
+template <int COMP>
+__global__ void __launch_bounds__(TPB) k_conv(const wf_case c, Geo g, double alpha,
+                                             const double* __restrict__ dtp) {
+  const double* u = c.fld[WF_U];
+  const double* v = c.fld[WF_V];
+  const double* w = c.fld[WF_W];
+  const double* oo = c.fld[WF_UOO + COMP];
+  double* star = c.fld[WF_USTAR + COMP];
+  const double dx = c.dx, dy = c.dy, dz = c.dz;
+  const double dt = *dtp;
+  const long X = g.sI, Y = g.sJ, Z = 1;
+  int ni, nj, nk;
+  op_dims(COMP, g.n, ni, nj, nk);
+  const long tot = (long)ni * nj * nk;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
+       t += (long)gridDim.x * blockDim.x) {
+    const int k = NPL + (int)(t % nk);
+    const int j = NPL + (int)((t / nk) % nj);
+    const int i = NPL + (int)(t / ((long)nk * nj));
+    const long id = g.at(i, j, k);
+    double tot3;
+    if (COMP == 0) {
+      double a;
+      a = I4(u, id + 2 * X, X); const double sp2 = a * a;
+      a = I4(u, id + X, X); const double sp1 = a * a;
+      a = I4(u, id, X); const double sn = a * a;
+      a = I4(u, id - X, X); const double sm1 = a * a;
+      const double du2dx = (-sp2 + 27.0 * sp1 - 27.0 * sn + sm1) / (24.0 * dx);
+      double p1 = I4(u, id + 2 * Y, Y) * I4(v, id + X + Y, X);
+      double p0 = I4(u, id + Y, Y) * I4(v, id + X, X);
+      double m1 = I4(u, id, Y) * I4(v, id + X - Y, X);
+      double m2 = I4(u, id - Y, Y) * I4(v, id + X - 2 * Y, X);
+      const double duvdy = (-p1 + 27.0 * p0 - 27.0 * m1 + m2) / (24.0 * dy);
+      p1 = I4(u, id + 2 * Z, Z) * I4(w, id + X + Z, X);
+      p0 = I4(u, id + Z, Z) * I4(w, id + X, X);
+      m1 = I4(u, id, Z) * I4(w, id + X - Z, X);
+      m2 = I4(u, id - Z, Z) * I4(w, id + X - 2 * Z, X);
+      const double duwdz = (-p1 + 27.0 * p0 - 27.0 * m1 + m2) / (24.0 * dz);
+      tot3 = du2dx + duvdy + duwdz;
+    } else if (COMP == 1) {
+      double a;
+      a = I4(v, id + 2 * Y, Y); const double sp2 = a * a;
+      a = I4(v, id + Y, Y); const double sp1 = a * a;
+      a = I4(v, id, Y); const double sn = a * a;
+      a = I4(v, id - Y, Y); const double sm1 = a * a;
+      const double dv2dy = (-sp2 + 27.0 * sp1 - 27.0 * sn + sm1) / (24.0 * dy);
+      double p1 = I4(v, id + 2 * X, X) * I4(u, id + X + Y, Y);
+      double p0 = I4(v, id + X, X) * I4(u, id + Y, Y);
+      double m1 = I4(v, id, X) * I4(u, id - X + Y, Y);
+      double m2 = I4(v, id - X, X) * I4(u, id - 2 * X + Y, Y);
+      const double duvdx = (-p1 + 27.0 * p0 - 27.0 * m1 + m2) / (24.0 * dx);
+      p1 = I4(v, id + 2 * Z, Z) * I4(w, id + Y + Z, Y);
+      p0 = I4(v, id + Z, Z) * I4(w, id + Y, Y);
+      m1 = I4(v, id, Z) * I4(w, id + Y - Z, Y);
+      m2 = I4(v, id - Z, Z) * I4(w, id + Y - 2 * Z, Y);
+      const double dvwdz = (-p1 + 27.0 * p0 - 27.0 * m1 + m2) / (24.0 * dz);
+      tot3 = duvdx + dv2dy + dvwdz;
+    } else {
+      double a;
+      a = I4(w, id + 2 * Z, Z); const double sp2 = a * a;
+      a = I4(w, id + Z, Z); const double sp1 = a * a;
+      a = I4(w, id, Z); const double sn = a * a;
+      a = I4(w, id - Z, Z); const double sm1 = a * a;
+      const double dw2dz = (-sp2 + 27.0 * sp1 - 27.0 * sn + sm1) / (24.0 * dz);
+      double p1 = I4(w, id + 2 * X, X) * I4(u, id + X + Z, Z);
+      double p0 = I4(w, id + X, X) * I4(u, id + Z, Z);
+      double m1 = I4(w, id, X) * I4(u, id - X + Z, Z);
+      double m2 = I4(w, id - X, X) * I4(u, id - 2 * X + Z, Z);
+      const double duwdx = (-p1 + 27.0 * p0 - 27.0 * m1 + m2) / (24.0 * dx);
+      p1 = I4(w, id + 2 * Y, Y) * I4(v, id + Y + Z, Z);
+      p0 = I4(w, id + Y, Y) * I4(v, id + Z, Z);
+      m1 = I4(w, id, Y) * I4(v, id - Y + Z, Z);
+      m2 = I4(w, id - Y, Y) * I4(v, id - 2 * Y + Z, Z);
+      const double dvwdy = (-p1 + 27.0 * p0 - 27.0 * m1 + m2) / (24.0 * dy);
+      tot3 = duwdx + dvwdy + dw2dz;
+    }
+    star[id] = LD(oo, id) - dt * alpha * tot3;
+  }
+}
+
+__device__ __forceinline__ double lap1(const double* f, long id, long s, double d) {
+  return (-LD(f, id + 2 * s) + 16.0 * LD(f, id + s) - 30.0 * LD(f, id) +
+          16.0 * LD(f, id - s) - LD(f, id - 2 * s)) /
+         (12.0 * d * d);
+}
+
+template <int COMP>
+__global__ void __launch_bounds__(TPB) k_diff(const wf_case c, Geo g, double alpha,
+                                             const double* __restrict__ dtp) {
+  const double* f = c.fld[WF_U + COMP];
+  const double* vis = c.fld[WF_VIS];
+  double* star = c.fld[WF_USTAR + COMP];
+  const double dt = *dtp;
+  const long vofs = COMP == 0 ? 0 : (COMP == 1 ? g.sJ : 1);
+  int ni, nj, nk;
+  op_dims(COMP, g.n, ni, nj, nk);
+  const long tot = (long)ni * nj * nk;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
+       t += (long)gridDim.x * blockDim.x) {
+    const int k = NPL + (int)(t % nk);
+    const int j = NPL + (int)((t / nk) % nj);
+    const int i = NPL + (int)(t / ((long)nk * nj));
+    const long id = g.at(i, j, k);
+    const double l4 = lap1(f, id, g.sI, c.dx) + lap1(f, id, g.sJ, c.dy) + lap1(f, id, 1, c.dz);
+    const double diff = LD(vis, id + vofs) * l4;
+    star[id] = star[id] + dt * alpha * diff;
+  }
+}
+
+int launch_conv(const wf_case& c, int comp, double alpha, const double* dt,
+                cudaStream_t s) {
+  Geo g = geo_of(c.n);
+  const long tot = (long)c.n * c.n * (c.n - 1);
+  const int nb = nblocks(tot);
+  if (comp == 0) k_conv<0><<<nb, TPB, 0, s>>>(c, g, alpha, dt);
+  else if (comp == 1) k_conv<1><<<nb, TPB, 0, s>>>(c, g, alpha, dt);
+  else if (comp == 2) k_conv<2><<<nb, TPB, 0, s>>>(c, g, alpha, dt);
+  else return fail(WF_EINVAL, "conv: comp must be 0, 1 or 2");
+  WF_CKL("k_conv");
+  return WF_OK;
+}
+
+int launch_diff(const wf_case& c, int comp, double alpha, const double* dt,
+                cudaStream_t s) {
+  Geo g = geo_of(c.n);
+  const long tot = (long)c.n * c.n * (c.n - 1);
+  const int nb = nblocks(tot);
+  if (comp == 0) k_diff<0><<<nb, TPB, 0, s>>>(c, g, alpha, dt);
+  else if (comp == 1) k_diff<1><<<nb, TPB, 0, s>>>(c, g, alpha, dt);
+  else if (comp == 2) k_diff<2><<<nb, TPB, 0, s>>>(c, g, alpha, dt);
+  else return fail(WF_EINVAL, "diff: comp must be 0, 1 or 2");
+  WF_CKL("k_diff");
+  return WF_OK;
+}
+
+// --------------------------------------------------------------------------
+// calvel (kernels.py:232-264): the three components in one launch
+// --------------------------------------------------------------------------
+__global__ void __launch_bounds__(TPB) k_calvel(const wf_case c, Geo g, double alpha,
+                                               const double* __restrict__ dtp) {
+  const double* p = c.fld[WF_P];
+  const double dt = *dtp;
+  const long tot = (long)g.n * g.n * g.n;
+  const int hi = NPL + g.n - 1;  // last real index; the component's own axis stops before it
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
+       t += (long)gridDim.x * blockDim.x) {
+    const int k = NPL + (int)(t % g.n);
+    const int j = NPL + (int)((t / g.n) % g.n);
+    const int i = NPL + (int)(t / ((long)g.n * g.n));
+    const long id = g.at(i, j, k);
+    const double p0 = LD(p, id);
+    if (i < hi)
+      c.fld[WF_U][id] = LD(c.fld[WF_USTAR], id) - dt * alpha * (LD(p, id + g.sI) - p0) / c.dx;
+    if (j < hi)
+      c.fld[WF_V][id] = LD(c.fld[WF_VSTAR], id) - dt * alpha * (LD(p, id + g.sJ) - p0) / c.dy;
+    if (k < hi)
+      c.fld[WF_W][id] = LD(c.fld[WF_WSTAR], id) - dt * alpha * (LD(p, id + 1) - p0) / c.dz;
+  }
+}
+
+int launch_calvel(const wf_case& c, double alpha, const double* dt, cudaStream_t s) {
+  Geo g = geo_of(c.n);
+  k_calvel<<<nblocks((long)c.n * c.n * c.n), TPB, 0, s>>>(c, g, alpha, dt);
+  WF_CKL("k_calvel");
+  return WF_OK;
+}
+
+// --------------------------------------------------------------------------
+// calmas (kernels.py:271-289) + one iteration of the projection control
+// (solver.py:185-209), decided by the last block on the device
+// --------------------------------------------------------------------------
+__global__ void __launch_bounds__(TPB) k_calmas(const wf_case c, Geo g,
+                                               unsigned long long h_if,
+                                               unsigned long long h_loop) {
+  __shared__ double sm[32];
+  const double* u = c.fld[WF_U];
+  const double* v = c.fld[WF_V];
+  const double* w = c.fld[WF_W];
+  double* su = c.fld[WF_SU];
+  wf_scalars* sc = c.sc;
+  const double dt = sc->dt;
+  const double dx = c.dx, dy = c.dy, dz = c.dz;
+  double mloc = 0.0;
+  const long tot = (long)g.n * g.n * g.n;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
+       t += (long)gridDim.x * blockDim.x) {
+    const int k = NPL + (int)(t % g.n);
+    const int j = NPL + (int)((t / g.n) % g.n);
+    const int i = NPL + (int)(t / ((long)g.n * g.n));
+    const long id = g.at(i, j, k);
+    const long X = g.sI, Y = g.sJ;
+    const double dudx = (-LD(u, id + X) + 27.0 * LD(u, id) - 27.0 * LD(u, id - X) +
+                         LD(u, id - 2 * X)) / (24.0 * dx);
+    const double dvdy = (-LD(v, id + Y) + 27.0 * LD(v, id) - 27.0 * LD(v, id - Y) +
+                         LD(v, id - 2 * Y)) / (24.0 * dy);
+    const double dwdz = (-LD(w, id + 1) + 27.0 * LD(w, id) - 27.0 * LD(w, id - 1) +
+                         LD(w, id - 2)) / (24.0 * dz);
+    const double fact = dudx + dvdy + dwdz;
+    su[id] = fact / dt;
+    mloc = fmax(mloc, fabs(fact * dx * dy * dz));
+  }
+  mloc = block_max(mloc, sm);
+  if (threadIdx.x == 0) atomicMax(&sc->red[4], dbits(mloc));
+  if (!last_block(&sc->ticket)) return;
+  if (threadIdx.x != 0) return;
+  const double rmax = bitsd(atomicAdd(&sc->red[4], 0ull));
+  sc->red[4] = 0ull;
+  sc->rmax = rmax;
+  const int it = ++sc->iters;
+  if (it <= 32) sc->rmax_trace[it - 1] = rmax;
+  const bool conv = (it > 1) && (rmax < c.eps);
+  const bool div = !conv && (rmax > 10.0);
+  const bool run = !conv && !div;
+  if (div) sc->status = WF_ST_DIVERGED;
+  if (run && it >= c.maxcy && sc->status == WF_ST_OK) sc->status = WF_ST_NOT_CONVERGED;
+  const int more = (run && it < c.maxcy) ? 1 : 0;
+  sc->loop = (run ? 2 : 0) | more;
+  if (h_if) cudaGraphSetConditional((cudaGraphConditionalHandle)h_if, run ? 1u : 0u);
+  if (h_loop) cudaGraphSetConditional((cudaGraphConditionalHandle)h_loop, (unsigned)more);
+}
+
+int launch_calmas(const wf_case& c, unsigned long long h_if, unsigned long long h_loop,
+                  cudaStream_t s) {
+  Geo g = geo_of(c.n);
+  k_calmas<<<nblocks((long)c.n * c.n * c.n, TPB, 148 * 4), TPB, 0, s>>>(c, g, h_if, h_loop);
+  WF_CKL("k_calmas");
+  return WF_OK;
+}
+
+// --------------------------------------------------------------------------
+// p += pp over real cells plus one ring (kernels.py:405-414)
+// --------------------------------------------------------------------------
+__global__ void k_add_ring(double* p, const double* pp, Geo g) {
+  const int m = g.n + 2;
+  const long tot = (long)m * m * m;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
+       t += (long)gridDim.x * blockDim.x) {
+    const int k = NPL - 1 + (int)(t % m);
+    const int j = NPL - 1 + (int)((t / m) % m);
+    const int i = NPL - 1 + (int)(t / ((long)m * m));
+    const long id = g.at(i, j, k);
+    p[id] = p[id] + pp[id];
+  }
+}
+
+int launch_add_ring(double* p, const double* pp, int n, cudaStream_t s) {
+  Geo g = geo_of(n);
+  k_add_ring<<<nblocks((long)(n + 2) * (n + 2) * (n + 2)), TPB, 0, s>>>(p, pp, g);
+  WF_CKL("k_add_ring");
+  return WF_OK;
+}
+
+}  // namespace wf

@@ -1,0 +1,358 @@
+// One FlowSolver.step() (reference solver.py:217-271) on the device, the
+// C ABI entry points, and error plumbing.
+//
+// Step layout (launch order follows solver.py exactly):
+//   prologue : checkdt -> uoo/voo/woo copy -> WALE + vis fill ->
+//              2 x RK stage (fill+conv per component, fill+diff per
+//              component, calvel(0.5) after stage 1) -> calvel(1.0)
+//   loop     : calmas + control  [if run] MG solve, p += pp, pbound,
+//              calvel(1.0)  -- repeated while the control says so
+//   epilogue : fill u, v, w
+// In graph mode the loop is a conditional WHILE node whose body holds the
+// calmas kernel and a conditional IF node for the multigrid part; the
+// calmas kernel's last block sets both conditions on the device, so a
+// whole step is one graph launch with no host round trip.
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "wf_internal.h"
+
+namespace wf {
+
+static thread_local std::string g_err;
+
+void set_error(const std::string& msg) { g_err = msg; }
+int fail(int code, const std::string& msg) {
+  set_error(msg);
+  return code;
+}
+int cuda_fail(cudaError_t e, const char* what) {
+  set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return WF_ECUDA;
+}
+
+int validate_case(const wf_case& c) {
+  if (c.n < 4) return fail(WF_EINVAL, "n must be >= 4");
+  if (c.nlev < 1 || c.nlev > WF_MAX_LEVELS) return fail(WF_EINVAL, "mg_levels out of range");
+  if (c.n % (1 << (c.nlev - 1)) != 0)
+    return fail(WF_EINVAL, "n must be divisible by 2**(mg_levels-1)");
+  for (int f = 0; f < WF_NFIELDS; ++f)
+    if (!c.fld[f]) return fail(WF_EINVAL, "null field pointer");
+  if (!c.sc) return fail(WF_EINVAL, "null scalar block");
+  for (int l = 1; l < c.nlev; ++l)
+    if (!c.mg_phi[l] || !c.mg_rhs[l]) return fail(WF_EINVAL, "missing multigrid level buffer");
+  if (c.mg_fp32 && (!c.mg_phi[0] || !c.mg_rhs[0]))
+    return fail(WF_EINVAL, "mixed precision needs FP32 level-0 buffers");
+  if (c.maxcy < 1 || c.maxcy > 32) return fail(WF_EINVAL, "max_outer_iters must be 1..32");
+  if (c.dx <= 0 || c.dy <= 0 || c.dz <= 0) return fail(WF_EINVAL, "cell sizes must be > 0");
+  if (c.n_pre < 0 || c.n_post < 0 || c.n_coarse < 0 || c.n_vcycles < 0)
+    return fail(WF_EINVAL, "negative sweep count");
+  return WF_OK;
+}
+
+static int fill_comp(const wf_case& c, int comp, cudaStream_t s) {
+  FillReq r{c.fld[WF_U + comp], comp == 0 ? FILL_U : (comp == 1 ? FILL_V : FILL_W), c.ulid};
+  return launch_fills(&r, 1, c.n, s);
+}
+
+static int step_prologue(const wf_case& c, cudaStream_t s) {
+  WF_TRY(launch_checkdt(c, s));
+  WF_TRY(launch_copy_oo(c, s));
+  WF_TRY(launch_wale(c, s));
+  const double* dt = &c.sc->dt;
+  const double alfark[2] = {0.5, 1.0};  // solver.py:26
+  for (int st = 0; st < 2; ++st) {
+    for (int comp = 0; comp < 3; ++comp) {
+      WF_TRY(fill_comp(c, comp, s));
+      WF_TRY(launch_conv(c, comp, alfark[st], dt, s));
+    }
+    for (int comp = 0; comp < 3; ++comp) {
+      WF_TRY(fill_comp(c, comp, s));
+      WF_TRY(launch_diff(c, comp, alfark[st], dt, s));
+    }
+    if (st == 0) WF_TRY(launch_calvel(c, alfark[st], dt, s));
+  }
+  return launch_calvel(c, 1.0, dt, s);
+}
+
+static int step_mg_part(const wf_case& c, cudaStream_t s) {
+  WF_TRY(mg_solve(c, s));
+  WF_TRY(launch_add_ring(c.fld[WF_P], c.fld[WF_PP], c.n, s));
+  FillReq r{c.fld[WF_P], FILL_PBOUND, 0.0};
+  WF_TRY(launch_fills(&r, 1, c.n, s));
+  return launch_calvel(c, 1.0, &c.sc->dt, s);
+}
+
+static int step_epilogue(const wf_case& c, cudaStream_t s) {
+  FillReq r[3] = {{c.fld[WF_U], FILL_U, c.ulid}, {c.fld[WF_V], FILL_V, 0.0},
+                  {c.fld[WF_W], FILL_W, 0.0}};
+  return launch_fills(r, 3, c.n, s);
+}
+
+}  // namespace wf
+
+using namespace wf;
+
+struct wf_stepper {
+  wf_case c;
+  int mode;
+  cudaGraph_t graph;
+  cudaGraphExec_t exec;
+  int32_t* hflag;  // pinned, host-loop mode
+};
+
+static int build_graph(wf_stepper* st) {
+  const wf_case& c = st->c;
+  cudaStream_t cap;
+  WF_CK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+  int rc = WF_OK;
+  cudaGraph_t g = nullptr;
+  do {
+    if (cudaGraphCreate(&g, 0) != cudaSuccess) { rc = cuda_fail(cudaGetLastError(), "cudaGraphCreate"); break; }
+    cudaGraphConditionalHandle h_loop;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&h_loop, g, 1, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) { rc = cuda_fail(e, "cudaGraphConditionalHandleCreate(loop)"); break; }
+    e = cudaStreamBeginCaptureToGraph(cap, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) { rc = cuda_fail(e, "cudaStreamBeginCaptureToGraph"); break; }
+    rc = step_prologue(c, cap);
+    cudaGraphNode_t wnode = nullptr;
+    cudaGraph_t wbody = nullptr;
+    if (rc == WF_OK) {
+      cudaStreamCaptureStatus cst;
+      const cudaGraphNode_t* deps = nullptr;
+      size_t ndeps = 0;
+      e = cudaStreamGetCaptureInfo(cap, &cst, nullptr, nullptr, &deps, &ndeps);
+      if (e != cudaSuccess) rc = cuda_fail(e, "cudaStreamGetCaptureInfo");
+      if (rc == WF_OK) {
+        cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+        cp.conditional.handle = h_loop;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        e = cudaGraphAddNode(&wnode, g, deps, ndeps, &cp);
+        if (e != cudaSuccess) rc = cuda_fail(e, "cudaGraphAddNode(while)");
+        else wbody = cp.conditional.phGraph_out[0];
+      }
+      if (rc == WF_OK) {
+        e = cudaStreamUpdateCaptureDependencies(cap, &wnode, 1, cudaStreamSetCaptureDependencies);
+        if (e != cudaSuccess) rc = cuda_fail(e, "cudaStreamUpdateCaptureDependencies");
+      }
+      if (rc == WF_OK) rc = step_epilogue(c, cap);
+    }
+    cudaGraph_t gout = nullptr;
+    e = cudaStreamEndCapture(cap, &gout);
+    if (rc == WF_OK && e != cudaSuccess) rc = cuda_fail(e, "cudaStreamEndCapture(step)");
+    if (rc != WF_OK) break;
+
+    // while body: calmas + control, then IF(run) multigrid part
+    cudaGraphConditionalHandle h_if;
+    e = cudaGraphConditionalHandleCreate(&h_if, wbody, 0, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) { rc = cuda_fail(e, "cudaGraphConditionalHandleCreate(if)"); break; }
+    e = cudaStreamBeginCaptureToGraph(cap, wbody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) { rc = cuda_fail(e, "cudaStreamBeginCaptureToGraph(while)"); break; }
+    rc = launch_calmas(c, (unsigned long long)h_if, (unsigned long long)h_loop, cap);
+    cudaGraph_t ibody = nullptr;
+    if (rc == WF_OK) {
+      cudaStreamCaptureStatus cst;
+      const cudaGraphNode_t* deps = nullptr;
+      size_t ndeps = 0;
+      e = cudaStreamGetCaptureInfo(cap, &cst, nullptr, nullptr, &deps, &ndeps);
+      if (e != cudaSuccess) rc = cuda_fail(e, "cudaStreamGetCaptureInfo(while)");
+      cudaGraphNode_t inode = nullptr;
+      if (rc == WF_OK) {
+        cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+        cp.conditional.handle = h_if;
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        e = cudaGraphAddNode(&inode, wbody, deps, ndeps, &cp);
+        if (e != cudaSuccess) rc = cuda_fail(e, "cudaGraphAddNode(if)");
+        else ibody = cp.conditional.phGraph_out[0];
+      }
+      if (rc == WF_OK) {
+        e = cudaStreamUpdateCaptureDependencies(cap, &inode, 1, cudaStreamSetCaptureDependencies);
+        if (e != cudaSuccess) rc = cuda_fail(e, "cudaStreamUpdateCaptureDependencies(while)");
+      }
+    }
+    e = cudaStreamEndCapture(cap, &gout);
+    if (rc == WF_OK && e != cudaSuccess) rc = cuda_fail(e, "cudaStreamEndCapture(while)");
+    if (rc != WF_OK) break;
+
+    e = cudaStreamBeginCaptureToGraph(cap, ibody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) { rc = cuda_fail(e, "cudaStreamBeginCaptureToGraph(if)"); break; }
+    rc = step_mg_part(c, cap);
+    e = cudaStreamEndCapture(cap, &gout);
+    if (rc == WF_OK && e != cudaSuccess) rc = cuda_fail(e, "cudaStreamEndCapture(if)");
+    if (rc != WF_OK) break;
+
+    e = cudaGraphInstantiate(&st->exec, g, 0);
+    if (e != cudaSuccess) { rc = cuda_fail(e, "cudaGraphInstantiate(step)"); break; }
+    st->graph = g;
+    g = nullptr;
+  } while (0);
+  if (g) cudaGraphDestroy(g);
+  cudaStreamDestroy(cap);
+  return rc;
+}
+
+extern "C" {
+
+int wf_version(void) { return 100; }
+
+const char* wf_last_error(void) { return g_err.c_str(); }
+
+int wf_struct_sizes(int64_t* scalars, int64_t* casebytes) {
+  if (scalars) *scalars = (int64_t)sizeof(wf_scalars);
+  if (casebytes) *casebytes = (int64_t)sizeof(wf_case);
+  return WF_OK;
+}
+
+int wf_mg_level_elems(int32_t n, int32_t nlev, int32_t level, int64_t* elems) {
+  if (!elems || level < 0 || level >= nlev || nlev > WF_MAX_LEVELS)
+    return fail(WF_EINVAL, "wf_mg_level_elems: bad level");
+  const int64_t m = (int64_t)(n >> level) + 2;
+  *elems = m * m * m;
+  return WF_OK;
+}
+
+int wf_scalars_init(wf_scalars* sc, double dt0, void* stream) {
+  return launch_scalars_init(sc, dt0, (cudaStream_t)stream);
+}
+
+int wf_init_noise(double* u, double* v, double* w, int32_t n, double amp, int32_t seed,
+                  void* stream) {
+  return launch_init_noise(u, v, w, n, amp, seed, (cudaStream_t)stream);
+}
+
+int wf_fill_initial(const wf_case* c, void* stream) {
+  if (!c) return fail(WF_EINVAL, "null case");
+  cudaStream_t s = (cudaStream_t)stream;
+  FillReq r[3] = {{c->fld[WF_U], FILL_U, c->ulid}, {c->fld[WF_V], FILL_V, 0.0},
+                  {c->fld[WF_W], FILL_W, 0.0}};
+  WF_TRY(launch_fills(r, 3, c->n, s));
+  FillReq p{c->fld[WF_P], FILL_PMIRROR, 0.0};
+  return launch_fills(&p, 1, c->n, s);
+}
+
+static int fill_one(double* f, int kind, double val, int32_t n, void* stream) {
+  FillReq r{f, kind, val};
+  return launch_fills(&r, 1, n, (cudaStream_t)stream);
+}
+int wf_fill_u(double* u, int32_t n, double ulid, void* s) { return fill_one(u, FILL_U, ulid, n, s); }
+int wf_fill_v(double* v, int32_t n, void* s) { return fill_one(v, FILL_V, 0.0, n, s); }
+int wf_fill_w(double* w, int32_t n, void* s) { return fill_one(w, FILL_W, 0.0, n, s); }
+int wf_fill_vis(double* vis, int32_t n, double rrey, void* s) {
+  return fill_one(vis, FILL_VIS, rrey, n, s);
+}
+int wf_fill_pbound(double* p, int32_t n, void* s) { return fill_one(p, FILL_PBOUND, 0.0, n, s); }
+int wf_fill_p_mirror(double* p, int32_t n, void* s) {
+  return fill_one(p, FILL_PMIRROR, 0.0, n, s);
+}
+
+int wf_conv(const wf_case* c, int32_t comp, double alpha, const double* dt, void* s) {
+  if (!c || !dt) return fail(WF_EINVAL, "null argument");
+  return launch_conv(*c, comp, alpha, dt, (cudaStream_t)s);
+}
+int wf_diff(const wf_case* c, int32_t comp, double alpha, const double* dt, void* s) {
+  if (!c || !dt) return fail(WF_EINVAL, "null argument");
+  return launch_diff(*c, comp, alpha, dt, (cudaStream_t)s);
+}
+int wf_calvel(const wf_case* c, double alpha, const double* dt, void* s) {
+  if (!c || !dt) return fail(WF_EINVAL, "null argument");
+  return launch_calvel(*c, alpha, dt, (cudaStream_t)s);
+}
+int wf_calmas(const wf_case* c, void* s) {
+  if (!c) return fail(WF_EINVAL, "null case");
+  return launch_calmas(*c, 0, 0, (cudaStream_t)s);
+}
+int wf_wale_vis(const wf_case* c, void* s) {
+  if (!c) return fail(WF_EINVAL, "null case");
+  return launch_wale(*c, (cudaStream_t)s);
+}
+int wf_checkdt(const wf_case* c, void* s) {
+  if (!c) return fail(WF_EINVAL, "null case");
+  return launch_checkdt(*c, (cudaStream_t)s);
+}
+int wf_add_ring(double* p, const double* pp, int32_t n, void* s) {
+  if (!p || !pp) return fail(WF_EINVAL, "null field");
+  return launch_add_ring(p, pp, n, (cudaStream_t)s);
+}
+
+int wf_mg_solve(const wf_case* c, void* s) {
+  if (!c) return fail(WF_EINVAL, "null case");
+  WF_TRY(validate_case(*c));
+  return mg_solve(*c, (cudaStream_t)s);
+}
+int wf_mg_vcycle(const wf_case* c, double* phi0, const double* rhs0, void* s) {
+  if (!c || !phi0 || !rhs0) return fail(WF_EINVAL, "null argument");
+  return mg_vcycle_pair(*c, phi0, rhs0, (cudaStream_t)s);
+}
+int wf_mg_relax(const wf_case* c, double* phi0, const double* rhs0, int32_t nsweeps, void* s) {
+  if (!c || !phi0 || !rhs0) return fail(WF_EINVAL, "null argument");
+  return mg_relax_pair(*c, phi0, rhs0, nsweeps, (cudaStream_t)s);
+}
+int wf_mg_residual_max(const wf_case* c, const double* phi0, const double* rhs0, double* out,
+                       void* s) {
+  if (!c || !phi0 || !rhs0 || !out) return fail(WF_EINVAL, "null argument");
+  return mg_residual_max_pair(*c, phi0, rhs0, out, (cudaStream_t)s);
+}
+int wf_mg_refill(const wf_case* c, double* phi0, void* s) {
+  if (!c || !phi0) return fail(WF_EINVAL, "null argument");
+  return mg_refill_pair(*c, phi0, (cudaStream_t)s);
+}
+
+int wf_stepper_create(const wf_case* c, int32_t mode, wf_stepper** out) {
+  if (!c || !out) return fail(WF_EINVAL, "null argument");
+  *out = nullptr;
+  WF_TRY(validate_case(*c));
+  if (mode != 0 && mode != 1) return fail(WF_EINVAL, "mode must be 0 (graph) or 1 (host loop)");
+  wf_stepper* st = new wf_stepper();
+  st->c = *c;
+  st->mode = mode;
+  st->graph = nullptr;
+  st->exec = nullptr;
+  st->hflag = nullptr;
+  int rc = WF_OK;
+  if (mode == 0) {
+    rc = build_graph(st);
+  } else {
+    cudaError_t e = cudaMallocHost((void**)&st->hflag, sizeof(int32_t));
+    if (e != cudaSuccess) rc = cuda_fail(e, "cudaMallocHost");
+  }
+  if (rc != WF_OK) {
+    wf_stepper_destroy(st);
+    return rc;
+  }
+  *out = st;
+  return WF_OK;
+}
+
+int wf_stepper_step(wf_stepper* st, void* stream) {
+  if (!st) return fail(WF_EINVAL, "null stepper");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (st->mode == 0) {
+    WF_CK(cudaGraphLaunch(st->exec, s));
+    return WF_OK;
+  }
+  const wf_case& c = st->c;
+  WF_TRY(step_prologue(c, s));
+  for (int it = 0; it < 64; ++it) {
+    WF_TRY(launch_calmas(c, 0, 0, s));
+    WF_CK(cudaMemcpyAsync(st->hflag, &c.sc->loop, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    WF_CK(cudaStreamSynchronize(s));
+    const int32_t f = *st->hflag;
+    if (f & 2) WF_TRY(step_mg_part(c, s));
+    if (!(f & 1)) break;
+  }
+  return step_epilogue(c, s);
+}
+
+int wf_stepper_destroy(wf_stepper* st) {
+  if (!st) return WF_OK;
+  if (st->exec) cudaGraphExecDestroy(st->exec);
+  if (st->graph) cudaGraphDestroy(st->graph);
+  if (st->hflag) cudaFreeHost(st->hflag);
+  delete st;
+  return WF_OK;
+}
+
+}  // extern "C"

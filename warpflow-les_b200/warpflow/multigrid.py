@@ -1,0 +1,153 @@
+"""Geometric multigrid Poisson solver (reference warpflow/multigrid.py),
+run by libwfb200's multigrid kernels.
+
+Interface kept from the reference (multigrid.py:207-337): ``levels`` with
+``phi``, ``rhs``, ``n3``, ``shape`` and the coefficient arrays ``aw ... ap``
+(exposed as read-only host views; the device kernels need none),
+``_vcycle()``, ``_relax(l, n)``, ``_refill(lev)``, ``solve(su, pp, npl)`` and
+the tunables ``n_pre``, ``n_post``, ``n_coarse``, ``n_vcycles``.
+
+``solve`` works in place: level 0 of the V-cycle is the one-ring core of
+``pp`` with ``su`` as its right-hand side, so nothing is copied in or out.
+The level-0 ``phi``/``rhs`` arrays serve the standalone harness form
+(``_vcycle`` / ``_relax(0, n)``), as in tests/test_mg.py.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _abi
+from .fields import DeviceField, cuda_device
+
+NPL_MG = 1  # one ring layer per level (reference multigrid.py:20)
+
+
+class _CoeffView:
+    """Host view of one constant coefficient array of a level
+    (reference multigrid.py:23-67: 1/d^2 on real cells, zero across
+    physical faces, ap = -sum; zero on the ring)."""
+
+    def __init__(self, lev, which):
+        self.lev, self.which = lev, which
+
+    @property
+    def shape(self):
+        return self.lev.shape
+
+    def numpy(self):
+        n = self.lev.n3[0]
+        a = np.zeros(self.lev.shape)
+        cx, cy, cz = (1.0 / (d * d) for d in self.lev.h)
+        core = {}
+        for name, c in (("aw", cx), ("ae", cx), ("as_", cy), ("an", cy),
+                        ("ab", cz), ("at", cz)):
+            core[name] = np.full((n, n, n), c)
+        core["aw"][0] = 0.0
+        core["ae"][n - 1] = 0.0
+        core["as_"][:, 0] = 0.0
+        core["an"][:, n - 1] = 0.0
+        core["ab"][:, :, 0] = 0.0
+        core["at"][:, :, n - 1] = 0.0
+        if self.which == "ap":
+            val = -(core["aw"] + core["ae"] + core["as_"] + core["an"]
+                    + core["ab"] + core["at"])
+        else:
+            val = core[self.which]
+        a[1:n + 1, 1:n + 1, 1:n + 1] = val
+        return a
+
+
+class _Level:
+    def __init__(self, n3, h, device, dtype=torch.float64):
+        self.n3 = tuple(n3)
+        self.shape = tuple(x + 2 for x in n3)
+        self.h = tuple(h)
+        self.phi = DeviceField.zeros(self.shape, device, dtype)
+        self.rhs = DeviceField.zeros(self.shape, device, dtype)
+        for name in ("aw", "ae", "as_", "an", "ab", "at", "ap"):
+            setattr(self, name, _CoeffView(self, name))
+
+
+class Multigrid:
+    def __init__(self, cfg, topo, device, dx, dy, dz):
+        self.cfg = cfg
+        self.topo = topo
+        self.device = cuda_device(device)
+        nb = topo.local_ncells
+        if len(set(nb)) != 1:
+            raise ValueError("only cubic grids are supported (got %s)" % (nb,))
+        self.dx, self.dy, self.dz = dx, dy, dz
+        self.levels = []
+        for l in range(cfg.numerics.mg_levels):
+            s = 2.0 ** l
+            self.levels.append(_Level(tuple(x >> l for x in nb),
+                                      (dx * s, dy * s, dz * s), self.device))
+        self.n_pre = 6       # multigrid.py:257-260
+        self.n_post = 6
+        self.n_coarse = 300
+        self.n_vcycles = 4
+        self._sc = torch.zeros(ctypes.sizeof(_abi.WfScalars), dtype=torch.uint8,
+                               device=self.device)
+        self._out = torch.zeros(1, dtype=torch.float64, device=self.device)
+        _abi.call("wf_scalars_init", self._sc.data_ptr(), 0.0, self._stream())
+
+    def _stream(self):
+        return ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def case(self, su=None, pp=None, levels=None) -> _abi.WfCase:
+        """The wf_case the multigrid entry points read (levels >= 1 buffers,
+        sweep counts, spacing); ``su``/``pp`` are set for ``solve``."""
+        levels = self.levels if levels is None else levels
+        c = _abi.WfCase()
+        c.n = levels[0].n3[0]
+        c.nlev = len(levels)
+        c.maxcy = 1
+        c.n_pre, c.n_post = self.n_pre, self.n_post
+        c.n_coarse, c.n_vcycles = self.n_coarse, self.n_vcycles
+        c.dx, c.dy, c.dz = levels[0].h
+        for l in range(1, len(levels)):
+            c.mg_phi[l] = levels[l].phi.ptr
+            c.mg_rhs[l] = levels[l].rhs.ptr
+        if su is not None:
+            c.fld[_abi.FIELD_NAMES.index("su")] = su.ptr
+        if pp is not None:
+            c.fld[_abi.FIELD_NAMES.index("pp")] = pp.ptr
+        c.sc = self._sc.data_ptr()
+        return c
+
+    def _refill(self, lev):
+        c = self.case(levels=[lev])
+        _abi.call("wf_mg_refill", ctypes.byref(c), lev.phi.ptr, self._stream())
+
+    def _relax(self, l, nsweeps):
+        lev = self.levels[l]
+        c = self.case(levels=[lev])
+        _abi.call("wf_mg_relax", ctypes.byref(c), lev.phi.ptr, lev.rhs.ptr,
+                  int(nsweeps), self._stream())
+
+    def _vcycle(self):
+        lev0 = self.levels[0]
+        c = self.case()
+        _abi.call("wf_mg_vcycle", ctypes.byref(c), lev0.phi.ptr, lev0.rhs.ptr,
+                  self._stream())
+
+    def residual_max(self, l=0):
+        """max |rhs - A phi| of a level (reference tests/test_mg.py:16-32)."""
+        lev = self.levels[l]
+        c = self.case(levels=[lev])
+        _abi.call("wf_mg_residual_max", ctypes.byref(c), lev.phi.ptr, lev.rhs.ptr,
+                  self._out.data_ptr(), self._stream())
+        return float(self._out.item())
+
+    def solve(self, su3, pp3, npl):
+        """A pp = su with 4 V-cycles from zero (reference multigrid.py:324-337)."""
+        if npl != 3:
+            raise ValueError("solve expects 3-ghost fields")
+        c = self.case(su=su3, pp=pp3)
+        for i, name in enumerate(_abi.FIELD_NAMES):
+            if not c.fld[i]:
+                c.fld[i] = su3.ptr  # unused slots must be non-null for validation
+        _abi.call("wf_mg_solve", ctypes.byref(c), self._stream())

@@ -1,0 +1,201 @@
+"""Time-marching flow solver (reference warpflow/solver.py), B200 build.
+
+``FlowSolver.step()`` is one launch of a CUDA graph built once per solver
+by libwfb200 (``wf_stepper_*``): dt control, WALE, both Heun RK2 stages,
+and the projection loop all run on the device, and the loop's
+data-dependent exit is a conditional graph node set by the divergence
+kernel.  The host reads one small scalar block per step (the reference
+makes five or more blocking readbacks, solver.py:119,133,175).
+
+Public interface as the reference (solver.py:29-271): constructor
+``FlowSolver(cfg, topo, device)``, ``step() -> {ctime, dt, rmax, iters,
+cfl}``, the field dict ``f`` (13 names), ``ncells``, ``dx/dy/dz``, ``rey``,
+``dt``, ``ctime``, ``itime``, ``rmax``, ``cfl``, ``outer_iters``, ``bnd``,
+``ulid``, ``mg``, ``cfg``, ``topo``; same exception messages.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import torch
+
+from . import _abi
+from .bcs import BoundaryKernels
+from .fields import DeviceField, cuda_device
+from .multigrid import Multigrid
+from .topology import NPL
+
+ALFARK = (0.5, 1.0)  # Heun RK2 stage coefficients (reference solver.py:26)
+
+STEP_MODES = {"graph": 0, "host": 1}
+
+
+class FlowSolver:
+    def __init__(self, cfg, topo, device, step_mode=None):
+        self.cfg = cfg
+        self.topo = topo
+        dev = cuda_device(device)
+        self.device = dev
+        ni, nj, nk = topo.local_ncells
+        if not (ni == nj == nk):
+            raise ValueError("only cubic grids are supported (got %s)" % ((ni, nj, nk),))
+        self.ncells = (ni, nj, nk)
+        self.n = ni
+        self.dx = cfg.domain.lx / cfg.grid.nx
+        self.dy = cfg.domain.ly / cfg.grid.ny
+        self.dz = cfg.domain.lz / cfg.grid.nz
+        self.rey = 1.0 / cfg.physics.reynolds
+
+        shape = (ni + 2 * NPL,) * 3
+        self.f = {name: DeviceField.zeros(shape, dev) for name in _abi.FIELD_NAMES}
+
+        b = cfg.boundaries
+        self.bnd = {"west": b.west, "east": b.east, "south": b.south,
+                    "north": b.north, "bottom": b.bottom, "top": b.top}
+        self.bcs = BoundaryKernels(self.bnd, dev)
+        self.ulid = b.lid_velocity
+        self.mg = Multigrid(cfg, topo, dev, self.dx, self.dy, self.dz)
+        self.mixed = cfg.numerics.mg_precision == "mixed"
+        self._mg32 = []
+        if self.mixed:
+            for lev in self.mg.levels:
+                shp = lev.shape
+                self._mg32.append((DeviceField.zeros(shp, dev, torch.float32),
+                                   DeviceField.zeros(shp, dev, torch.float32)))
+
+        nsc = ctypes.sizeof(_abi.WfScalars)
+        self._sc = torch.zeros(nsc, dtype=torch.uint8, device=dev)
+        self._sc_host = torch.zeros(nsc, dtype=torch.uint8, pin_memory=True)
+        self._sc_view = _abi.WfScalars.from_address(self._sc_host.data_ptr())
+
+        self._dt = cfg.time.dt_init
+        self._ctime = 0.0
+        self.itime = 0
+        self.rmax = 0.0
+        self.cfl = 0.0
+        self.outer_iters = 0
+        self.rmax_trace = []
+
+        s = self._stream()
+        _abi.call("wf_scalars_init", self._sc.data_ptr(), float(self._dt), s)
+        amp = cfg.initial.noise if cfg.initial.type == "rest" else 0.0
+        if amp > 0.0:
+            _abi.call("wf_init_noise", self.f["u"].ptr, self.f["v"].ptr, self.f["w"].ptr,
+                      ni, float(amp), 1, s)
+        self.f["vis"].fill_(self.rey)
+        self.case = self._make_case()
+        _abi.call("wf_fill_initial", ctypes.byref(self.case), s)
+
+        mode = step_mode or os.environ.get("WF_STEP_MODE", "graph")
+        if mode not in STEP_MODES:
+            raise ValueError("step_mode must be one of %s" % sorted(STEP_MODES))
+        self.step_mode = mode
+        self._stepper = ctypes.c_void_p()
+        _abi.call("wf_stepper_create", ctypes.byref(self.case), STEP_MODES[mode],
+                  ctypes.byref(self._stepper))
+
+    # ------------------------------------------------------------------ #
+    def _stream(self):
+        return ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def _make_case(self) -> _abi.WfCase:
+        cfg = self.cfg
+        c = self.mg.case()
+        c.sgs = 1 if cfg.physics.sgs_enabled else 0
+        c.variable_dt = 1 if cfg.time.variable_dt else 0
+        c.maxcy = int(cfg.numerics.max_outer_iters)
+        c.mg_fp32 = 1 if self.mixed else 0
+        c.dx, c.dy, c.dz = self.dx, self.dy, self.dz
+        c.rrey = self.rey
+        c.cw = float(cfg.physics.sgs_cw)
+        c.ulid = float(self.ulid)
+        c.dt_growth = float(cfg.time.dt_growth)
+        c.safety = float(cfg.time.safety_factor)
+        c.eps = float(cfg.numerics.div_tolerance)
+        for i, name in enumerate(_abi.FIELD_NAMES):
+            c.fld[i] = self.f[name].ptr
+        if self.mixed:
+            for l, (phi32, rhs32) in enumerate(self._mg32):
+                c.mg_phi[l] = phi32.ptr
+                c.mg_rhs[l] = rhs32.ptr
+        c.sc = self._sc.data_ptr()
+        return c
+
+    def _pull_scalars(self):
+        self._sc_host.copy_(self._sc, non_blocking=True)
+        torch.cuda.current_stream(self.device).synchronize()
+        return self._sc_view
+
+    def _push_scalar(self, name, value):
+        sc = self._pull_scalars()
+        setattr(sc, name, value)
+        self._sc.copy_(self._sc_host, non_blocking=True)
+        torch.cuda.current_stream(self.device).synchronize()
+
+    @property
+    def dt(self):
+        return self._dt
+
+    @dt.setter
+    def dt(self, value):
+        self._dt = float(value)
+        self._push_scalar("dt", self._dt)
+
+    @property
+    def ctime(self):
+        return self._ctime
+
+    @ctime.setter
+    def ctime(self, value):
+        self._ctime = float(value)
+        self._push_scalar("ctime", self._ctime)
+
+    # ------------------------------------------------------------------ #
+    def fill_bc(self, name, alfabc=0):
+        """One boundu/boundv/boundw call (reference solver.py:88-97)."""
+        n = self.n
+        if name == "u":
+            self.bcs.apply_u(self.f["u"], n, self.ulid, alfabc)
+        elif name == "v":
+            self.bcs.apply_v(self.f["v"], n, alfabc)
+        elif name == "w":
+            self.bcs.apply_w(self.f["w"], n, alfabc)
+
+    def step(self):
+        """One time step (reference solver.py:217-271)."""
+        _abi.call("wf_stepper_step", self._stepper, self._stream())
+        sc = self._pull_scalars()
+        self.itime = int(sc.itime)
+        self._dt = float(sc.dt)
+        self._ctime = float(sc.ctime)
+        self.rmax = float(sc.rmax)
+        self.cfl = float(sc.cfl)
+        self.outer_iters = int(sc.iters)
+        self.rmax_trace = [float(sc.rmax_trace[i])
+                           for i in range(min(self.outer_iters, 32))]
+        st = int(sc.status)
+        if st == _abi.ST_DT_COLLAPSE:
+            raise RuntimeError("time step collapsed (dtmax = %.3e)" % sc.dtmax)
+        if st == _abi.ST_DIVERGED:
+            raise RuntimeError("projection diverged: rmax = %.6e at itime %d"
+                               % (self.rmax, self.itime))
+        if st == _abi.ST_NOT_CONVERGED:
+            if self.topo.rank == 0:
+                print("warning: projection did not converge, rmax = %.6e after %d "
+                      "iterations" % (self.rmax, self.cfg.numerics.max_outer_iters),
+                      flush=True)
+            self._push_scalar("status", _abi.ST_OK)
+        return {"ctime": self._ctime, "dt": self._dt, "rmax": self.rmax,
+                "iters": self.outer_iters, "cfl": self.cfl}
+
+    def close(self):
+        if getattr(self, "_stepper", None):
+            _abi.load().wf_stepper_destroy(self._stepper)
+            self._stepper = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
