@@ -1,0 +1,350 @@
+"""Benchmark: lid-driven cavity LES steps on B200 (warpflow B200 build).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--n 80] [--precision fp64|mixed]
+
+Workload (N=1): the 80^3 cavity of cases/cavity_serial.yaml -- Re 400,
+WALE, seeded 1 % noise, variable dt (x1.1 from 3e-4, capped at 0.8 dtmax),
+3-level RBGS multigrid 6/6/300, 4 V-cycles, div_tolerance 1e-6.  One step
+is one FlowSolver.step().  Under torchrun each rank advances its own
+independent replica of the case on its GPU (the case does not shard;
+weak scaling), timing is the max over ranks.
+
+Prints one JSON line (rank 0).  ``value`` is Mcell-steps/s from CUDA
+events around each step's graph launch with the state resident in HBM;
+the L2 (126 MB) is flushed between timed steps by writing a 512 MB buffer
+(the 80^3 working set, ~70 MB, would otherwise stay L2-resident).
+``e2e`` is the same metric through the public API with the state coming
+from and going back to pinned host buffers every step.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import io
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "warpflow-les_b200"))
+sys.path.insert(0, ROOT)
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+
+
+def case_raw(n, levels, precision, seed_noise=0.01):
+    return {
+        "case": "cavity_serial_%d" % n,
+        "domain": {"lx": 1.0, "ly": 1.0, "lz": 1.0},
+        "grid": {"nx": n, "ny": n, "nz": n},
+        "physics": {"reynolds": 400, "sgs": {"enabled": True, "model": "wale", "cw": 0.46}},
+        "initial": {"type": "rest", "noise": seed_noise},
+        "boundaries": {"west": "wall", "east": "wall", "south": "slip", "north": "slip",
+                       "bottom": "wall", "top": "moving_lid", "lid_velocity": 1.0},
+        "numerics": {"mg_levels": levels, "max_outer_iters": 30, "div_tolerance": 1.0e-6,
+                     "mg_precision": precision},
+        "time": {"n_steps": 1000, "variable_dt": True, "dt_init": 3.0e-4,
+                 "safety_factor": 0.8, "dt_growth": 1.1},
+        "mpi": {"domains": [1, 1, 1]},
+    }
+
+
+# ---------------------------------------------------------------------------
+# algorithmic byte model of one step (reference passes, one read of each
+# distinct input and one write of each output per pass over the N^3 cells)
+# ---------------------------------------------------------------------------
+def vcycle_words(levels, n_pre=6, n_post=6, n_coarse=300):
+    """Words per fine cell of one V-cycle: RBGS sweeps (phi, rhs -> phi),
+    restriction (+ coarse phi zeroing) and prolongation."""
+    L = levels
+    w = 0.0
+    for l in range(L):
+        sweeps = (n_pre + n_post) if l < L - 1 else n_coarse
+        w += sweeps * 3.0 / 8 ** l
+    for l in range(1, L):
+        w += 2.0 / 8 ** (l - 1) + 2.0 / 8 ** l      # restrict l-1 -> l
+        w += 1.0 / 8 ** l + 2.0 / 8 ** (l - 1)      # prolong l -> l-1
+    return w
+
+
+def step_bytes(n, iters, nmg, levels, mg_word=8):
+    """Bytes per step: fixed 89 words (dt reduce 7, copies 6, WALE 4, two RK
+    stages 54, two calvels 18), 4 per divergence pass, and per multigrid
+    solve the solve (6 + 4 V-cycles) plus p += pp (3) and calvel (9)."""
+    v = vcycle_words(levels)
+    fixed = 89 + 4 * iters + 12 * nmg
+    mg = nmg * (6 + 4 * v)
+    return n ** 3 * (8.0 * fixed + mg_word * mg)
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = list(csv.reader(io.StringIO(open(self.path).read())))
+        os.unlink(self.path)
+        sm, mx, pw, reasons = [], None, [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                pw.append(float(r[3]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, r[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "power_w_max": max(pw) if pw else None, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return PEAKS_FALLBACK["hbm_gbs"], "fallback"
+
+
+# ---------------------------------------------------------------------------
+def run_oracle(n, levels, steps, warmup):
+    """The reference algorithm on the host cores (NumPy FP64 oracle port;
+    the reference's Warp CPU path cannot run here: warp-lang is not
+    installed)."""
+    from oracle import wf_oracle as O
+    from warpflow.config import case_from_dict
+    cfg = case_from_dict(case_raw(n, levels, "fp64"))
+    sol = O.OracleSolver(cfg)
+    for _ in range(warmup):
+        sol.step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        sol.step()
+    dt = time.perf_counter() - t0
+    return n ** 3 * steps / dt / 1e6, dt
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=80)
+    ap.add_argument("--levels", type=int, default=3)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    K, W = args.steps, max(3, args.warmup)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    metric = "Mcell-steps/s (80^3 cavity step, FP64, div<=1e-6)"
+    cfg_desc = {"workload": "lid-driven cavity %d^3, Re 400, WALE, variable dt, "
+                            "3-level RBGS multigrid 6/6/300 x4 V-cycles" % args.n,
+                "n": args.n, "mg_levels": args.levels, "mg_precision": args.precision,
+                "replicas": world, "l2": "flushed between timed steps (512 MB write)"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        ks = min(K, 6)
+        val, dt = run_oracle(args.n, args.levels, ks, 1)
+        line = {"impl": "reference", "metric": metric, "value": round(val, 4),
+                "unit": "Mcell-steps/s", "n_gpus": args.gpus, "steps": ks, "warmup": 1,
+                "ms_per_step": round(1e3 * dt / ks, 2), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded hash noise, reference init_noise)",
+                "config": cfg_desc,
+                "cpu_baseline": {"value": round(val, 4), "unit": "Mcell-steps/s", "cores": 1,
+                                 "kind": "port",
+                                 "sample": "%d steps of the %d^3 cavity after 1 warm-up step "
+                                           "(NumPy FP64 oracle; the reference's Warp CPU path "
+                                           "is unavailable: warp-lang not installed)"
+                                           % (ks, args.n)},
+                "e2e": {"value": round(val, 4), "unit": "Mcell-steps/s",
+                        "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from warpflow import FlowSolver, build_topology
+    from warpflow.config import case_from_dict
+
+    cfg = case_from_dict(case_raw(args.n, args.levels, args.precision))
+    sol = FlowSolver(cfg, build_topology(cfg), dev)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    counts = sol.launch_counts()
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    # ---- warm-up ----------------------------------------------------------
+    for _ in range(W):
+        sol.step()
+    torch.cuda.synchronize()
+
+    # ---- timed region -----------------------------------------------------
+    sampler = ClockSampler(local)
+    sampler.start()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    iters, nmgs = [], []
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(K):
+        flush.zero_()
+        starts[k].record()
+        sol.launch_step()
+        ends[k].record()
+        sol.finish_step()
+        iters.append(sol.outer_iters)
+        nmgs.append(sol.last_nmg)
+    torch.cuda.synchronize()
+    barrier()
+    wall = time.perf_counter() - t0
+    clocks = sampler.stop()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    dev_s = sum(step_ms) / 1e3
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([dev_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_s = float(t.item())
+    value = world * args.n ** 3 * K / dev_s / 1e6
+    launches = sum(counts[0] + counts[3] + it * counts[1] + m * counts[2]
+                   for it, m in zip(iters, nmgs))
+
+    # ---- roofline (algorithmic bytes of the measured iterations) ------------
+    mg_word = 4 if args.precision == "mixed" else 8
+    bytes_tot = sum(step_bytes(args.n, it, m, args.levels, mg_word)
+                    for it, m in zip(iters, nmgs))
+    peak, peak_kind = load_peaks()
+    achieved = bytes_tot / (sum(step_ms) / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "whole step (one CUDA graph launch)",
+                "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind,
+                "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "traffic": None,
+                "alg_bytes_per_step": round(bytes_tot / K),
+                "note": "achieved = algorithmic bytes of the reference passes (measured "
+                        "iters per step) / device step time; frac of measured copy peak"}
+
+    # ---- end to end through the public API with host buffers ---------------
+    e2e = None
+    if not args.no_e2e:
+        state_in = ("u", "v", "w", "p", "vis")
+        state_out = ("u", "v", "w", "p")
+        host = {k: torch.empty(sol.f[k].shape, dtype=torch.float64, pin_memory=True)
+                for k in state_in}
+        for k in state_in:
+            host[k].copy_(sol.f[k].t)
+        outs = {k: torch.empty(sol.f[k].shape, dtype=torch.float64, pin_memory=True)
+                for k in state_out}
+        ke = max(10, K // 3)
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(ke):
+            for k in state_in:
+                sol.f[k].t.copy_(host[k], non_blocking=True)
+            sol.step()
+            for k in state_out:
+                outs[k].copy_(sol.f[k].t, non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+            for k in state_in:
+                if k in outs:
+                    host[k], outs[k] = outs[k], host[k]
+        torch.cuda.synchronize()
+        barrier()
+        te = time.perf_counter() - t0
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([te], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            te = float(t.item())
+        nb = sol.f["u"].t.numel() * 8
+        e2e = {"value": round(world * args.n ** 3 * ke / te / 1e6, 2),
+               "unit": "Mcell-steps/s", "steps": ke,
+               "h2d_bytes_per_step": nb * len(state_in),
+               "d2h_bytes_per_step": nb * len(state_out) + 4 * 8,
+               "api": "FlowSolver.step() with u,v,w,p,vis uploaded from and u,v,w,p "
+                      "downloaded to pinned host memory every step; wall clock"}
+
+    # ---- CPU baseline (oracle port on the host cores) -----------------------
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        cval, cdt = run_oracle(args.n, args.levels, 2, 0)
+        cpu = {"value": round(cval, 4), "unit": "Mcell-steps/s", "cores": 1, "kind": "port",
+               "sample": "first 2 steps of the %d^3 cavity (NumPy FP64 oracle, %.1f s); the "
+                         "reference's Warp CPU path is unavailable here" % (args.n, cdt)}
+
+    if rank == 0:
+        line = {"metric": metric, "value": round(value, 2), "unit": "Mcell-steps/s",
+                "n_gpus": world, "steps": K, "warmup": W,
+                "ms_per_step": round(sum(step_ms) / K, 4), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded hash noise, reference init_noise)",
+                "config": cfg_desc, "iters_mean": round(sum(iters) / K, 3),
+                "wall_s": round(wall, 3), "gpu_launches": int(launches),
+                "launches_per_step": round(launches / K, 1),
+                "clocks": clocks, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e}
+        print(json.dumps(line), flush=True)
+    sol.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -80,7 +80,7 @@ typedef struct wf_scalars {
   int32_t status;     /* wf_status */
   int32_t loop;       /* device loop flag of the projection */
   uint32_t ticket;    /* last-block-done counter */
-  int32_t pad;
+  int32_t nmg;        /* multigrid solves run in the last step */
 } wf_scalars;
 
 /* One cavity case: geometry, physics, numerics and the caller's buffers. */
@@ -180,6 +180,9 @@ typedef struct wf_stepper wf_stepper;
 WF_API int wf_stepper_create(const wf_case* c, int32_t mode, wf_stepper** out);
 /* One FlowSolver.step(): enqueue the step on `stream`.  No host sync. */
 WF_API int wf_stepper_step(wf_stepper* s, void* stream);
+/* kernel launches per part of the step: prologue, one projection-loop
+ * pass (calmas), one multigrid part, epilogue */
+WF_API int wf_stepper_launch_counts(const wf_stepper* s, int32_t counts[4]);
 WF_API int wf_stepper_destroy(wf_stepper* s);
 
 #ifdef __cplusplus

@@ -5,13 +5,20 @@
 
 namespace wf {
 
-// bit patterns of non-negative doubles order like the doubles themselves,
-// so max/min reductions of |x| and of positive values are integer atomics
 __device__ __forceinline__ unsigned long long dbits(double x) {
   return (unsigned long long)__double_as_longlong(x);
 }
 __device__ __forceinline__ double bitsd(unsigned long long b) {
   return __longlong_as_double((long long)b);
+}
+// order-preserving key: okey(a) < okey(b) as unsigned iff a < b as doubles
+// (any sign), so device-wide max/min reductions are integer atomics
+__device__ __forceinline__ unsigned long long okey(double x) {
+  const unsigned long long b = dbits(x);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double okey_inv(unsigned long long k) {
+  return bitsd((k >> 63) ? (k & 0x7fffffffffffffffull) : ~k);
 }
 
 __device__ __forceinline__ double warp_max(double v) {

@@ -21,8 +21,11 @@ int cuda_fail(cudaError_t e, const char* what);
     if (_e != cudaSuccess) return ::wf::cuda_fail(_e, #expr);        \
   } while (0)
 
+// every kernel launch is followed by WF_CKL, which also counts it
+extern thread_local long g_launches;
 #define WF_CKL(what)                                                 \
   do {                                                               \
+    ++::wf::g_launches;                                              \
     cudaError_t _e = cudaGetLastError();                             \
     if (_e != cudaSuccess) return ::wf::cuda_fail(_e, what);         \
   } while (0)

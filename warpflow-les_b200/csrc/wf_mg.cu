@@ -250,11 +250,11 @@ __global__ void k_resmax(const Lvl<double> L, double* out, unsigned int* ticket,
     m = fmax(m, fabs(r));
   }
   m = block_max(m, sm);
-  if (threadIdx.x == 0) atomicMax(acc, dbits(m));
+  if (threadIdx.x == 0) atomicMax(acc, okey(m));
   if (!last_block(ticket)) return;
   if (threadIdx.x == 0) {
-    *out = bitsd(atomicAdd(acc, 0ull));
-    *acc = 0ull;
+    *out = okey_inv(atomicAdd(acc, 0ull));
+    *acc = okey(0.0);
   }
 }
 
@@ -279,12 +279,8 @@ static int relax(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
   if (nsweeps <= 0) return WF_OK;
   const size_t sb = smem_bytes<T>(L.n);
   if (sb <= SMEM_CAP) {
-    static bool attr_set = false;
-    if (!attr_set) {
-      WF_CK(cudaFuncSetAttribute(k_relax_smem<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)SMEM_CAP));
-      attr_set = true;
-    }
+    WF_CK(cudaFuncSetAttribute(k_relax_smem<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)SMEM_CAP));
     const int n3 = L.n * L.n * L.n;
     int tpb = 1024;
     if (n3 / 2 < 1024) tpb = std::max(32, ((n3 / 2 + 31) / 32) * 32);
@@ -296,9 +292,10 @@ static int relax(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
   const int nb = mg_blocks(half);
   for (int sw = 0; sw < nsweeps; ++sw) {
     k_rbgs<T><<<nb, MG_TPB, 0, s>>>(L, 0);
+    WF_CKL("k_rbgs");
     k_rbgs<T><<<nb, MG_TPB, 0, s>>>(L, 1);
+    WF_CKL("k_rbgs");
   }
-  WF_CKL("k_rbgs");
   return WF_OK;
 }
 

@@ -51,16 +51,16 @@ __global__ void k_scalars_init(wf_scalars* sc, double dt0) {
   sc->umax = sc->vmax = sc->wmax = 0.0;
   sc->dtvisc = 0.0;
   for (int i = 0; i < 32; ++i) sc->rmax_trace[i] = 0.0;
-  sc->red[0] = sc->red[1] = sc->red[2] = 0ull;
-  sc->red[3] = dbits(1.0e10);  // solver.py:127 initialiser of the min
-  sc->red[4] = 0ull;
-  sc->red[5] = 0ull;
+  sc->red[0] = sc->red[1] = sc->red[2] = okey(0.0);
+  sc->red[3] = okey(1.0e10);  // solver.py:127 initialiser of the min
+  sc->red[4] = okey(0.0);
+  sc->red[5] = okey(0.0);
   sc->itime = 0;
   sc->iters = 0;
   sc->status = WF_ST_OK;
   sc->loop = 0;
   sc->ticket = 0u;
-  sc->pad = 0;
+  sc->nmg = 0;
 }
 
 int launch_scalars_init(wf_scalars* sc, double dt0, cudaStream_t s) {
@@ -141,19 +141,19 @@ __global__ void __launch_bounds__(TPB) k_checkdt(const wf_case c, Geo g) {
   mdt = block_min(mdt, sm, 1.0e10);
   wf_scalars* sc = c.sc;
   if (threadIdx.x == 0) {
-    atomicMax(&sc->red[0], dbits(mu));
-    atomicMax(&sc->red[1], dbits(mv));
-    atomicMax(&sc->red[2], dbits(mw));
-    atomicMin(&sc->red[3], dbits(mdt));
+    atomicMax(&sc->red[0], okey(mu));
+    atomicMax(&sc->red[1], okey(mv));
+    atomicMax(&sc->red[2], okey(mw));
+    atomicMin(&sc->red[3], okey(mdt));
   }
   if (!last_block(&sc->ticket)) return;
   if (threadIdx.x != 0) return;
-  const double umax = bitsd(atomicAdd(&sc->red[0], 0ull));
-  const double vmax = bitsd(atomicAdd(&sc->red[1], 0ull));
-  const double wmax = bitsd(atomicAdd(&sc->red[2], 0ull));
-  const double dtvisc = bitsd(atomicAdd(&sc->red[3], 0ull));
-  sc->red[0] = sc->red[1] = sc->red[2] = 0ull;
-  sc->red[3] = dbits(1.0e10);
+  const double umax = okey_inv(atomicAdd(&sc->red[0], 0ull));
+  const double vmax = okey_inv(atomicAdd(&sc->red[1], 0ull));
+  const double wmax = okey_inv(atomicAdd(&sc->red[2], 0ull));
+  const double dtvisc = okey_inv(atomicAdd(&sc->red[3], 0ull));
+  sc->red[0] = sc->red[1] = sc->red[2] = okey(0.0);
+  sc->red[3] = okey(1.0e10);
   const double big = 1.0e10;
   double dtcfl = big;
   if (umax > 0.0) dtcfl = fmin(dtcfl, dx / umax);
@@ -167,6 +167,7 @@ __global__ void __launch_bounds__(TPB) k_checkdt(const wf_case c, Geo g) {
   sc->dtmax = dtmax;
   sc->itime += 1;
   sc->iters = 0;
+  sc->nmg = 0;
   if (dtmax <= 0.0 || !(dtmax < big)) sc->status = WF_ST_DT_COLLAPSE;
   const double dt_old = sc->dt;
   sc->cfl = dt_old / dtmax;
@@ -528,11 +529,11 @@ __global__ void __launch_bounds__(TPB) k_calmas(const wf_case c, Geo g,
     mloc = fmax(mloc, fabs(fact * dx * dy * dz));
   }
   mloc = block_max(mloc, sm);
-  if (threadIdx.x == 0) atomicMax(&sc->red[4], dbits(mloc));
+  if (threadIdx.x == 0) atomicMax(&sc->red[4], okey(mloc));
   if (!last_block(&sc->ticket)) return;
   if (threadIdx.x != 0) return;
-  const double rmax = bitsd(atomicAdd(&sc->red[4], 0ull));
-  sc->red[4] = 0ull;
+  const double rmax = okey_inv(atomicAdd(&sc->red[4], 0ull));
+  sc->red[4] = okey(0.0);
   sc->rmax = rmax;
   const int it = ++sc->iters;
   if (it <= 32) sc->rmax_trace[it - 1] = rmax;
@@ -540,6 +541,7 @@ __global__ void __launch_bounds__(TPB) k_calmas(const wf_case c, Geo g,
   const bool div = !conv && (rmax > 10.0);
   const bool run = !conv && !div;
   if (div) sc->status = WF_ST_DIVERGED;
+  if (run) sc->nmg += 1;
   if (run && it >= c.maxcy && sc->status == WF_ST_OK) sc->status = WF_ST_NOT_CONVERGED;
   const int more = (run && it < c.maxcy) ? 1 : 0;
   sc->loop = (run ? 2 : 0) | more;

@@ -21,6 +21,7 @@
 namespace wf {
 
 static thread_local std::string g_err;
+thread_local long g_launches = 0;
 
 void set_error(const std::string& msg) { g_err = msg; }
 int fail(int code, const std::string& msg) {
@@ -97,6 +98,7 @@ using namespace wf;
 struct wf_stepper {
   wf_case c;
   int mode;
+  int32_t counts[4];  // launches: prologue, calmas pass, multigrid part, epilogue
   cudaGraph_t graph;
   cudaGraphExec_t exec;
   int32_t* hflag;  // pinned, host-loop mode
@@ -115,7 +117,9 @@ static int build_graph(wf_stepper* st) {
     if (e != cudaSuccess) { rc = cuda_fail(e, "cudaGraphConditionalHandleCreate(loop)"); break; }
     e = cudaStreamBeginCaptureToGraph(cap, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) { rc = cuda_fail(e, "cudaStreamBeginCaptureToGraph"); break; }
+    long l0 = g_launches;
     rc = step_prologue(c, cap);
+    st->counts[0] = (int32_t)(g_launches - l0);
     cudaGraphNode_t wnode = nullptr;
     cudaGraph_t wbody = nullptr;
     if (rc == WF_OK) {
@@ -137,7 +141,9 @@ static int build_graph(wf_stepper* st) {
         e = cudaStreamUpdateCaptureDependencies(cap, &wnode, 1, cudaStreamSetCaptureDependencies);
         if (e != cudaSuccess) rc = cuda_fail(e, "cudaStreamUpdateCaptureDependencies");
       }
+      l0 = g_launches;
       if (rc == WF_OK) rc = step_epilogue(c, cap);
+      st->counts[3] = (int32_t)(g_launches - l0);
     }
     cudaGraph_t gout = nullptr;
     e = cudaStreamEndCapture(cap, &gout);
@@ -150,7 +156,9 @@ static int build_graph(wf_stepper* st) {
     if (e != cudaSuccess) { rc = cuda_fail(e, "cudaGraphConditionalHandleCreate(if)"); break; }
     e = cudaStreamBeginCaptureToGraph(cap, wbody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) { rc = cuda_fail(e, "cudaStreamBeginCaptureToGraph(while)"); break; }
+    l0 = g_launches;
     rc = launch_calmas(c, (unsigned long long)h_if, (unsigned long long)h_loop, cap);
+    st->counts[1] = (int32_t)(g_launches - l0);
     cudaGraph_t ibody = nullptr;
     if (rc == WF_OK) {
       cudaStreamCaptureStatus cst;
@@ -179,7 +187,9 @@ static int build_graph(wf_stepper* st) {
 
     e = cudaStreamBeginCaptureToGraph(cap, ibody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) { rc = cuda_fail(e, "cudaStreamBeginCaptureToGraph(if)"); break; }
+    l0 = g_launches;
     rc = step_mg_part(c, cap);
+    st->counts[2] = (int32_t)(g_launches - l0);
     e = cudaStreamEndCapture(cap, &gout);
     if (rc == WF_OK && e != cudaSuccess) rc = cuda_fail(e, "cudaStreamEndCapture(if)");
     if (rc != WF_OK) break;
@@ -311,6 +321,7 @@ int wf_stepper_create(const wf_case* c, int32_t mode, wf_stepper** out) {
   st->graph = nullptr;
   st->exec = nullptr;
   st->hflag = nullptr;
+  for (int i = 0; i < 4; ++i) st->counts[i] = 0;
   int rc = WF_OK;
   if (mode == 0) {
     rc = build_graph(st);
@@ -334,16 +345,33 @@ int wf_stepper_step(wf_stepper* st, void* stream) {
     return WF_OK;
   }
   const wf_case& c = st->c;
+  long l0 = g_launches;
   WF_TRY(step_prologue(c, s));
+  st->counts[0] = (int32_t)(g_launches - l0);
   for (int it = 0; it < 64; ++it) {
+    l0 = g_launches;
     WF_TRY(launch_calmas(c, 0, 0, s));
+    st->counts[1] = (int32_t)(g_launches - l0);
     WF_CK(cudaMemcpyAsync(st->hflag, &c.sc->loop, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     WF_CK(cudaStreamSynchronize(s));
     const int32_t f = *st->hflag;
-    if (f & 2) WF_TRY(step_mg_part(c, s));
+    if (f & 2) {
+      l0 = g_launches;
+      WF_TRY(step_mg_part(c, s));
+      st->counts[2] = (int32_t)(g_launches - l0);
+    }
     if (!(f & 1)) break;
   }
-  return step_epilogue(c, s);
+  l0 = g_launches;
+  WF_TRY(step_epilogue(c, s));
+  st->counts[3] = (int32_t)(g_launches - l0);
+  return WF_OK;
+}
+
+int wf_stepper_launch_counts(const wf_stepper* st, int32_t counts[4]) {
+  if (!st || !counts) return fail(WF_EINVAL, "null argument");
+  for (int i = 0; i < 4; ++i) counts[i] = st->counts[i];
+  return WF_OK;
 }
 
 int wf_stepper_destroy(wf_stepper* st) {

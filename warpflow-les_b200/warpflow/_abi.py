@@ -37,7 +37,7 @@ class WfScalars(ctypes.Structure):
         ("status", ctypes.c_int32),
         ("loop", ctypes.c_int32),
         ("ticket", ctypes.c_uint32),
-        ("pad", ctypes.c_int32),
+        ("nmg", ctypes.c_int32),
     ]
 
 
@@ -104,6 +104,7 @@ SIGNATURES = {
     "wf_stepper_create": (_I32, [_CP, _I32, ctypes.POINTER(_VP)]),
     "wf_stepper_step": (_I32, [_VP, _VP]),
     "wf_stepper_destroy": (_I32, [_VP]),
+    "wf_stepper_launch_counts": (_I32, [_VP, ctypes.POINTER(_I32)]),
 }
 
 _lib = None

@@ -164,8 +164,25 @@ class FlowSolver:
 
     def step(self):
         """One time step (reference solver.py:217-271)."""
+        self.launch_step()
+        return self.finish_step()
+
+    def launch_step(self):
+        """Enqueue one step on the current stream without waiting."""
         _abi.call("wf_stepper_step", self._stepper, self._stream())
+
+    def launch_counts(self):
+        """Kernel launches of (prologue, calmas pass, multigrid part,
+        epilogue) of this solver's step."""
+        arr = (ctypes.c_int32 * 4)()
+        _abi.call("wf_stepper_launch_counts", self._stepper, arr)
+        return tuple(arr)
+
+    def finish_step(self):
+        """Wait for the enqueued step, update the host-side scalars and raise
+        the reference's errors."""
         sc = self._pull_scalars()
+        self.last_nmg = int(sc.nmg)
         self.itime = int(sc.itime)
         self._dt = float(sc.dt)
         self._ctime = float(sc.ctime)
