@@ -226,6 +226,137 @@ __global__ void __launch_bounds__(1024) k_relax_smem(Lvl<T> L, int nsweeps) {
   }
 }
 
+// ---- the coarse level: many sweeps of an even n <= 24 in one CTA ----------
+// One thread per (i,j) column.  Columns are split by the parity of i+j into
+// two groups of warps, so within a warp every thread updates the same k
+// parity in a given half-sweep (no divergence, register indices fixed at
+// compile time).  The column's phi and rhs live in registers; phi is also
+// published to shared memory, stored red/black-split as
+// [column parity][k][i][j/2], where the four in-plane neighbours of a
+// column (all of the other parity) are contiguous across the lanes of a
+// warp.  The diagonal is applied as a reciprocal (one rounding away from the
+// division).  Ring terms have zero coefficients and are not read.
+template <int NC>
+struct CoarseShape {
+  static constexpr int THREADS = 2 * (((NC * (NC / 2)) + 31) / 32) * 32;
+};
+
+template <class T, int NC, bool RHS_SMEM>
+__global__ void __launch_bounds__(CoarseShape<NC>::THREADS) k_coarse_cols(Lvl<T> L,
+                                                                           int nsweeps) {
+  constexpr int H = NC / 2;
+  constexpr int HALF = NC * H;                  // columns per parity
+  constexpr int GROUP = ((HALF + 31) / 32) * 32;
+  constexpr int PLANE = NC * H;                 // one parity, one k plane
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* sp = reinterpret_cast<T*>(smraw);
+  T* srh = sp + NC * NC * NC;                   // rhs, when it stays in smem
+  const int tid = threadIdx.x;
+  const int g = tid / GROUP;                    // 0: (i+j) even, 1: odd
+  const int q = tid - g * GROUP;
+  const bool active = q < HALF;
+  const int i = active ? q / H : 0;
+  const int m = active ? q - i * H : 0;
+  const int j = 2 * m + ((i + g) & 1);
+  T* own = sp + g * NC * PLANE;
+  const T* oth = sp + (1 - g) * NC * PLANE;
+  const int me = q < HALF ? q : 0;
+  const int oW = i > 0 ? me - H : me;
+  const int oE = i < NC - 1 ? me + H : me;
+  const int oS = j > 0 ? i * H + ((j - 1) >> 1) : me;
+  const int oN = j < NC - 1 ? i * H + ((j + 1) >> 1) : me;
+  const T aw = i > 0 ? L.ax : T(0), ae = i < NC - 1 ? L.ax : T(0);
+  const T as = j > 0 ? L.ay : T(0), an = j < NC - 1 ? L.ay : T(0);
+  const T az = L.az;
+  // multigrid.py:58-67: ap = -(aw + ae + as + an + ab + at)
+  const T inv_in = T(1) / (-(aw + ae + as + an + az + az));
+  const T inv_lo = T(1) / (-(aw + ae + as + an + T(0) + az));
+  const T inv_hi = T(1) / (-(aw + ae + as + an + az + T(0)));
+  T ph[NC];
+  T rh[RHS_SMEM ? 1 : NC];
+  const long c0 = lid(L, i + 1, j + 1, 1);
+#pragma unroll
+  for (int k = 0; k < NC; ++k) {
+    ph[k] = active ? L.phi[c0 + k] : T(0);
+    const T r = active ? L.rhs[c0 + k] : T(0);
+    if (RHS_SMEM) {
+      if (active) srh[(g * NC + k) * PLANE + me] = r;
+    } else {
+      rh[RHS_SMEM ? 0 : k] = r;
+    }
+    if (active) own[k * PLANE + me] = ph[k];
+  }
+  __syncthreads();
+  for (int sw = 0; sw < nsweeps; ++sw) {
+#pragma unroll
+    for (int color = 0; color < 2; ++color) {
+      // (i+j+k+color) odd  <=>  k parity = (1 + g + color) & 1
+      const int kp = (1 + g + color) & 1;
+      if (active) {
+        if (kp == 0) {
+#pragma unroll
+          for (int k = 0; k < NC; k += 2) {
+            const T* pl = oth + k * PLANE;
+            T sum = aw * pl[oW] + ae * pl[oE] + as * pl[oS] + an * pl[oN];
+            if (k > 0) sum = sum + az * ph[k - 1];
+            if (k < NC - 1) sum = sum + az * ph[k + 1];
+            const T r = RHS_SMEM ? srh[(g * NC + k) * PLANE + me] : rh[RHS_SMEM ? 0 : k];
+            const T x = (r - sum) * (k == 0 ? inv_lo : (k == NC - 1 ? inv_hi : inv_in));
+            ph[k] = x;
+            own[k * PLANE + me] = x;
+          }
+        } else {
+#pragma unroll
+          for (int k = 1; k < NC; k += 2) {
+            const T* pl = oth + k * PLANE;
+            T sum = aw * pl[oW] + ae * pl[oE] + as * pl[oS] + an * pl[oN];
+            sum = sum + az * ph[k - 1];
+            if (k < NC - 1) sum = sum + az * ph[k + 1];
+            const T r = RHS_SMEM ? srh[(g * NC + k) * PLANE + me] : rh[RHS_SMEM ? 0 : k];
+            const T x = (r - sum) * (k == NC - 1 ? inv_hi : inv_in);
+            ph[k] = x;
+            own[k * PLANE + me] = x;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (!active) return;
+#pragma unroll
+  for (int k = 0; k < NC; ++k) {
+    const long c = c0 + k;
+    L.phi[c] = ph[k];
+    if (nsweeps > 0) ring_mirror(L, i, j, k, c, ph[k]);
+  }
+}
+
+template <class T, int NC, bool RHS_SMEM>
+static int launch_coarse(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
+  constexpr int HALF = NC * (NC / 2);
+  constexpr int GROUP = ((HALF + 31) / 32) * 32;
+  const size_t sb = (size_t)NC * NC * NC * sizeof(T) * (RHS_SMEM ? 2 : 1);
+  WF_CK(cudaFuncSetAttribute(k_coarse_cols<T, NC, RHS_SMEM>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb));
+  k_coarse_cols<T, NC, RHS_SMEM><<<1, 2 * GROUP, sb, s>>>(L, nsweeps);
+  WF_CKL("k_coarse_cols");
+  return WF_OK;
+}
+
+// returns 1 when a specialised coarse kernel handled the level
+template <class T>
+static int try_coarse(const Lvl<T>& L, int nsweeps, cudaStream_t s, int* rc) {
+  switch (L.n) {
+    case 4: *rc = launch_coarse<T, 4, false>(L, nsweeps, s); return 1;
+    case 8: *rc = launch_coarse<T, 8, false>(L, nsweeps, s); return 1;
+    case 12: *rc = launch_coarse<T, 12, false>(L, nsweeps, s); return 1;
+    case 16: *rc = launch_coarse<T, 16, false>(L, nsweeps, s); return 1;
+    case 20: *rc = launch_coarse<T, 20, false>(L, nsweeps, s); return 1;
+    case 24: *rc = launch_coarse<T, 24, true>(L, nsweeps, s); return 1;
+    default: return 0;
+  }
+}
+
 // max |rhs - A phi| over a level (tests/test_mg.py:16-32)
 __global__ void k_resmax(const Lvl<double> L, double* out, unsigned int* ticket,
                          unsigned long long* acc) {
@@ -277,6 +408,11 @@ constexpr size_t SMEM_CAP = 220 * 1024;
 template <class T>
 static int relax(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
   if (nsweeps <= 0) return WF_OK;
+  // small levels with many sweeps: the column kernel
+  if (nsweeps > 12 || L.n <= 12) {
+    int rc = WF_OK;
+    if (try_coarse<T>(L, nsweeps, s, &rc)) return rc;
+  }
   const size_t sb = smem_bytes<T>(L.n);
   if (sb <= SMEM_CAP) {
     WF_CK(cudaFuncSetAttribute(k_relax_smem<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
