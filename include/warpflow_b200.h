@@ -159,6 +159,17 @@ WF_API int wf_add_ring(double* p, const double* pp, int32_t n, void* stream);
  * on A pp = su (7-point Neumann, RBGS 6/6/300).  Level 0 works in place in
  * `pp`; level >= 1 buffers come from the case. */
 WF_API int wf_mg_solve(const wf_case* c, void* stream);
+/* No counterpart in the reference.  The same solve as wf_mg_solve (6/6/300
+ * sweeps, 4 V-cycles from zero, pp written in place from su) for callers
+ * that cannot allocate device memory -- host codes that hand out every GPU
+ * buffer from their own fixed pool or memory budget.  The coarse levels live
+ * in a 4 MiB array compiled into the library (held on every GPU that loads
+ * it until the process exits), enough for n <= 112 at 3 levels; larger
+ * problems return WF_EINVAL.  Nothing is allocated.  The first call on a
+ * device looks up the array's address; make it before any stream capture.
+ * Calls share the array: calls that overlap on the GPU race. */
+WF_API int wf_mg_solve_noalloc(const double* su, double* pp, int32_t n, int32_t nlev,
+                               double dx, double dy, double dz, void* stream);
 /* multigrid.py:301-322 one V-cycle on an explicit level-0 pair (phi, rhs)
  * of (n+2)^3 doubles each (the standalone harness of tests/test_mg.py). */
 WF_API int wf_mg_vcycle(const wf_case* c, double* phi0, const double* rhs0, void* stream);

@@ -18,6 +18,8 @@
 // Level 0 works in place: phi is the (n+2)^3 core of `pp` and rhs the core
 // of `su`, both with the padded (n+6) strides.
 #include <algorithm>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "wf_dev.cuh"
@@ -556,6 +558,128 @@ int mg_residual_max_pair(const wf_case& c, const double* phi0, const double* rhs
   k_resmax<<<mg_blocks((long)c.n * c.n * c.n), MG_TPB, 0, s>>>(lv[0], out, &c.sc->ticket,
                                                                &c.sc->red[5]);
   WF_CKL("k_resmax");
+  return WF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Multigrid solve for callers that cannot allocate device memory.
+//
+// Some host programs do not let a library allocate GPU memory at all: a
+// Fortran or C++ flow solver that links this library through the C ABI and
+// hands out every device buffer from its own fixed pool, or a service that
+// admits work against a fixed memory budget and must know every byte in
+// advance.  For them, wf_mg_solve_noalloc keeps the coarse multigrid levels
+// (1 .. nlev-1) in one fixed array compiled into this library, so the
+// caller passes only the right-hand side and the solution and nothing is
+// allocated on any call.
+//
+// The array holds MG_NOALLOC_DOUBLES doubles (4 MiB) on every GPU that
+// loads the library, for the life of the process; that is enough for n up
+// to 112 at 3 levels.  Larger problems are rejected with WF_EINVAL.
+// Host code cannot use the array's name as a device address, so the first
+// call on each device looks the address up once (with that device current)
+// and caches it; make that first call before any stream capture.  All
+// calls share the array and only the last call's contents remain: every
+// level is rewritten before it is read, and calls that overlap on the GPU
+// (two streams, or two host threads) race on it.
+// ---------------------------------------------------------------------------
+constexpr long MG_NOALLOC_DOUBLES = 1L << 19;
+static __device__ __align__(256) double g_mg_noalloc_scratch[MG_NOALLOC_DOUBLES];
+
+static int noalloc_scratch(double** out) {
+  static std::mutex mu;
+  static double* addr[64] = {};
+  int dev = -1;
+  WF_CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(WF_EUNSUPPORTED, "device ordinal beyond 63");
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_mg_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(multigrid scratch)");
+    addr[dev] = static_cast<double*>(p);
+  }
+  *out = addr[dev];
+  return WF_OK;
+}
+
+// the V-cycle of multigrid.py:301-322 over a fixed array of level views
+static int vcycle_fixed(Lvl<double>* lv, int L, const wf_case& c, cudaStream_t s) {
+  for (int l = 0; l < L; ++l) {
+    if (l > 0) {
+      const long m = (long)lv[l].n + 2;
+      k_zero<double><<<mg_blocks(m * m * m), MG_TPB, 0, s>>>(lv[l].phi, m * m * m);
+      WF_CKL("k_zero");
+      k_restrict<double><<<mg_blocks((long)lv[l].n * lv[l].n * lv[l].n), MG_TPB, 0, s>>>(
+          lv[l - 1], const_cast<double*>(lv[l].rhs), lv[l]);
+      WF_CKL("k_restrict");
+    }
+    WF_TRY(relax(lv[l], l < L - 1 ? c.n_pre : c.n_coarse, s));
+  }
+  for (int l = L - 2; l >= 0; --l) {
+    k_prolong<double><<<mg_blocks((long)lv[l].n * lv[l].n * lv[l].n), MG_TPB, 0, s>>>(
+        lv[l + 1], lv[l]);
+    WF_CKL("k_prolong");
+    WF_TRY(relax(lv[l], c.n_post, s));
+  }
+  return WF_OK;
+}
+
+int mg_solve_noalloc(const double* su, double* pp, int n, int nlev, double dx, double dy,
+                     double dz, cudaStream_t s) {
+  if (!su || !pp) return fail(WF_EINVAL, "wf_mg_solve_noalloc: null su or pp");
+  if (n < 4 || nlev < 1 || nlev > WF_MAX_LEVELS || n % (1 << (nlev - 1)) != 0)
+    return fail(WF_EINVAL, "wf_mg_solve_noalloc: n must be >= 4 and divisible by "
+                           "2**(nlev-1), 1 <= nlev <= 8");
+  if (!(dx > 0 && dy > 0 && dz > 0)) return fail(WF_EINVAL, "wf_mg_solve_noalloc: bad spacing");
+  long need = 0;
+  for (int l = 1; l < nlev; ++l) {
+    const long m = (long)(n >> l) + 2;
+    need += 2 * (((m * m * m) + 31) / 32) * 32;
+  }
+  if (need > MG_NOALLOC_DOUBLES)
+    return fail(WF_EINVAL, "wf_mg_solve_noalloc: n=" + std::to_string(n) + " with " +
+                               std::to_string(nlev) + " levels needs " + std::to_string(need) +
+                               " doubles of multigrid scratch; the static array holds " +
+                               std::to_string(MG_NOALLOC_DOUBLES) +
+                               " (n <= 112 at 3 levels); use wf_mg_solve with caller buffers");
+  double* base = nullptr;
+  WF_TRY(noalloc_scratch(&base));
+  const long P = padded(n);
+  const long off = (long)(NPL - 1) * (P * P + P + 1);
+  Lvl<double> lv[WF_MAX_LEVELS];
+  long used = 0;
+  for (int l = 0; l < nlev; ++l) {
+    const double s2 = (double)(1 << l);
+    const double dxl = dx * s2, dyl = dy * s2, dzl = dz * s2;
+    Lvl<double>& L = lv[l];
+    L.ax = 1.0 / (dxl * dxl);
+    L.ay = 1.0 / (dyl * dyl);
+    L.az = 1.0 / (dzl * dzl);
+    L.n = n >> l;
+    if (l == 0) {
+      L.phi = pp + off;
+      L.rhs = su + off;
+      L.sI = P * P;
+      L.sJ = P;
+    } else {
+      const long m = (long)L.n + 2;
+      const long cnt = ((m * m * m + 31) / 32) * 32;
+      L.phi = base + used;
+      L.rhs = base + used + cnt;
+      used += 2 * cnt;
+      L.sJ = m;
+      L.sI = m * m;
+    }
+  }
+  wf_case c{};
+  c.n_pre = 6;      // multigrid.py:257-260
+  c.n_post = 6;
+  c.n_coarse = 300;
+  c.n_vcycles = 4;
+  k_zero<double><<<mg_blocks(P * P * P), MG_TPB, 0, s>>>(pp, P * P * P);
+  WF_CKL("k_zero pp");
+  for (int cyc = 0; cyc < c.n_vcycles; ++cyc) WF_TRY(vcycle_fixed(lv, nlev, c, s));
   return WF_OK;
 }
 

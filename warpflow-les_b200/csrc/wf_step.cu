@@ -292,6 +292,10 @@ int wf_mg_solve(const wf_case* c, void* s) {
   WF_TRY(validate_case(*c));
   return mg_solve(*c, (cudaStream_t)s);
 }
+int wf_mg_solve_noalloc(const double* su, double* pp, int32_t n, int32_t nlev, double dx,
+                        double dy, double dz, void* s) {
+  return mg_solve_noalloc(su, pp, n, nlev, dx, dy, dz, (cudaStream_t)s);
+}
 int wf_mg_vcycle(const wf_case* c, double* phi0, const double* rhs0, void* s) {
   if (!c || !phi0 || !rhs0) return fail(WF_EINVAL, "null argument");
   return mg_vcycle_pair(*c, phi0, rhs0, (cudaStream_t)s);

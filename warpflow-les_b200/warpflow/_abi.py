@@ -97,6 +97,7 @@ SIGNATURES = {
     "wf_checkdt": (_I32, [_CP, _VP]),
     "wf_add_ring": (_I32, [_VP, _VP, _I32, _VP]),
     "wf_mg_solve": (_I32, [_CP, _VP]),
+    "wf_mg_solve_noalloc": (_I32, [_VP, _VP, _I32, _I32, _D, _D, _D, _VP]),
     "wf_mg_vcycle": (_I32, [_CP, _VP, _VP, _VP]),
     "wf_mg_relax": (_I32, [_CP, _VP, _VP, _I32, _VP]),
     "wf_mg_residual_max": (_I32, [_CP, _VP, _VP, _VP, _VP]),
