@@ -17,7 +17,10 @@
 //
 // Level 0 works in place: phi is the (n+2)^3 core of `pp` and rhs the core
 // of `su`, both with the padded (n+6) strides.
+#include <cooperative_groups.h>
+
 #include <algorithm>
+#include <cstdlib>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -228,6 +231,44 @@ __global__ void __launch_bounds__(1024) k_relax_smem(Lvl<T> L, int nsweeps) {
   }
 }
 
+// One colour of one column: the cells k = KP, KP+2, ... of the column.
+// Phase 1 gathers the four in-plane neighbour sums of every cell (all loads
+// independent), phase 2 updates the column top-down and publishes the new
+// values, so no shared-memory store sits between two loads.  The sum keeps
+// the reference's term order aw W + ae E + as S + an N + ab B + at T.
+template <class T, int NC, int KP, bool RHS_SMEM>
+__device__ __forceinline__ void half_sweep_cols(const T* __restrict__ oth, T* __restrict__ own,
+                                                int PLANE, int me, int oW, int oE, int oS,
+                                                int oN, T aw, T ae, T as, T an, T az, T inv_in,
+                                                T inv_lo, T inv_hi, T (&ph)[NC],
+                                                const T (&rh)[RHS_SMEM ? 1 : NC],
+                                                const T* __restrict__ srh) {
+  constexpr int NK = (NC - KP + 1) / 2;
+  T nb[NK];
+#pragma unroll
+  for (int t = 0; t < NK; ++t) {
+    const T* pl = oth + (KP + 2 * t) * PLANE;
+    nb[t] = aw * pl[oW] + ae * pl[oE] + as * pl[oS] + an * pl[oN];
+  }
+  T rr[RHS_SMEM ? NK : 1];
+  if (RHS_SMEM) {
+#pragma unroll
+    for (int t = 0; t < NK; ++t) rr[RHS_SMEM ? t : 0] = srh[(KP + 2 * t) * PLANE + me];
+  }
+#pragma unroll
+  for (int t = 0; t < NK; ++t) {
+    const int k = KP + 2 * t;
+    T sum = nb[t];
+    if (k > 0) sum = sum + az * ph[k - 1];
+    if (k < NC - 1) sum = sum + az * ph[k + 1];
+    const T r = RHS_SMEM ? rr[RHS_SMEM ? t : 0] : rh[RHS_SMEM ? 0 : k];
+    const T x = (r - sum) * (k == 0 ? inv_lo : (k == NC - 1 ? inv_hi : inv_in));
+    ph[k] = x;
+  }
+#pragma unroll
+  for (int t = 0; t < NK; ++t) own[(KP + 2 * t) * PLANE + me] = ph[KP + 2 * t];
+}
+
 // ---- the coarse level: many sweeps of an even n <= 24 in one CTA ----------
 // One thread per (i,j) column.  Columns are split by the parity of i+j into
 // two groups of warps, so within a warp every thread updates the same k
@@ -295,31 +336,12 @@ __global__ void __launch_bounds__(CoarseShape<NC>::THREADS) k_coarse_cols(Lvl<T>
       // (i+j+k+color) odd  <=>  k parity = (1 + g + color) & 1
       const int kp = (1 + g + color) & 1;
       if (active) {
-        if (kp == 0) {
-#pragma unroll
-          for (int k = 0; k < NC; k += 2) {
-            const T* pl = oth + k * PLANE;
-            T sum = aw * pl[oW] + ae * pl[oE] + as * pl[oS] + an * pl[oN];
-            if (k > 0) sum = sum + az * ph[k - 1];
-            if (k < NC - 1) sum = sum + az * ph[k + 1];
-            const T r = RHS_SMEM ? srh[(g * NC + k) * PLANE + me] : rh[RHS_SMEM ? 0 : k];
-            const T x = (r - sum) * (k == 0 ? inv_lo : (k == NC - 1 ? inv_hi : inv_in));
-            ph[k] = x;
-            own[k * PLANE + me] = x;
-          }
-        } else {
-#pragma unroll
-          for (int k = 1; k < NC; k += 2) {
-            const T* pl = oth + k * PLANE;
-            T sum = aw * pl[oW] + ae * pl[oE] + as * pl[oS] + an * pl[oN];
-            sum = sum + az * ph[k - 1];
-            if (k < NC - 1) sum = sum + az * ph[k + 1];
-            const T r = RHS_SMEM ? srh[(g * NC + k) * PLANE + me] : rh[RHS_SMEM ? 0 : k];
-            const T x = (r - sum) * (k == NC - 1 ? inv_hi : inv_in);
-            ph[k] = x;
-            own[k * PLANE + me] = x;
-          }
-        }
+        if (kp == 0) half_sweep_cols<T, NC, 0, RHS_SMEM>(oth, own, PLANE, me, oW, oE, oS, oN, aw, ae, as,
+                                                    an, az, inv_in, inv_lo, inv_hi, ph, rh,
+                                                    srh + g * NC * PLANE);
+        else half_sweep_cols<T, NC, 1, RHS_SMEM>(oth, own, PLANE, me, oW, oE, oS, oN, aw, ae, as, an,
+                                                 az, inv_in, inv_lo, inv_hi, ph, rh,
+                                                 srh + g * NC * PLANE);
       }
       __syncthreads();
     }
@@ -355,6 +377,162 @@ static int try_coarse(const Lvl<T>& L, int nsweeps, cudaStream_t s, int* rc) {
     case 16: *rc = launch_coarse<T, 16, false>(L, nsweeps, s); return 1;
     case 20: *rc = launch_coarse<T, 20, false>(L, nsweeps, s); return 1;
     case 24: *rc = launch_coarse<T, 24, true>(L, nsweeps, s); return 1;
+    default: return 0;
+  }
+}
+
+// ---- the coarse level spread over a thread-block cluster ------------------
+// The level is cut into C = NC/NCL slabs of NCL i-planes, one CTA per slab,
+// the CTAs forming one cluster.  A CTA keeps its slab plus one halo plane
+// on each side in shared memory ([parity][k][NCL+2][NC/2], red/black split
+// as in k_coarse_cols), so every neighbour read is local.  After updating a
+// cell on its first or last plane a thread also stores the value into the
+// neighbouring CTA's halo plane (distributed shared memory), and the cluster
+// barrier that ends each half-sweep publishes those stores.
+template <int NC, int NCL>
+struct ClusterShape {
+  static constexpr int C = NC / NCL;
+  static constexpr int H = NC / 2;
+  static constexpr int HALF = NCL * H;
+  static constexpr int GROUP = ((HALF + 31) / 32) * 32;
+  static constexpr int THREADS = 2 * GROUP;
+  static constexpr int PL = (NCL + 2) * H;  // one parity, one k
+};
+
+template <class T, int NC, int NCL>
+__global__ void __launch_bounds__(ClusterShape<NC, NCL>::THREADS)
+    k_coarse_cluster(Lvl<T> L, int nsweeps) {
+  using S = ClusterShape<NC, NCL>;
+  constexpr int H = S::H, HALF = S::HALF, GROUP = S::GROUP, PL = S::PL, C = S::C;
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* sp = reinterpret_cast<T*>(smraw);
+  const int tid = threadIdx.x;
+  for (int t = tid; t < 2 * NC * PL; t += blockDim.x) sp[t] = T(0);
+  const int g = tid / GROUP;
+  const int q = tid - g * GROUP;
+  const bool active = q < HALF;
+  const int il = active ? q / H : 0;
+  const int m = active ? q - il * H : 0;
+  const int i = rank * NCL + il;
+  const int j = 2 * m + ((i + g) & 1);
+  T* own = sp + g * NC * PL;
+  const T* oth = sp + (1 - g) * NC * PL;
+  const int me = (il + 1) * H + m;
+  const int oW = me - H, oE = me + H;
+  const int oS = j > 0 ? (il + 1) * H + ((j - 1) >> 1) : me;
+  const int oN = j < NC - 1 ? (il + 1) * H + ((j + 1) >> 1) : me;
+  const T aw = i > 0 ? L.ax : T(0), ae = i < NC - 1 ? L.ax : T(0);
+  const T as = j > 0 ? L.ay : T(0), an = j < NC - 1 ? L.ay : T(0);
+  const T az = L.az;
+  const T inv_in = T(1) / (-(aw + ae + as + an + az + az));
+  const T inv_lo = T(1) / (-(aw + ae + as + an + T(0) + az));
+  const T inv_hi = T(1) / (-(aw + ae + as + an + az + T(0)));
+  // halo slots of the neighbouring CTAs that mirror this thread's column
+  T* rW = nullptr;  // my first plane -> rank-1's east halo (plane NCL+1)
+  T* rE = nullptr;  // my last plane  -> rank+1's west halo (plane 0)
+  if (active && il == 0 && rank > 0)
+    rW = cl.map_shared_rank(own, rank - 1) + (NCL + 1) * H + m;
+  if (active && il == NCL - 1 && rank < C - 1)
+    rE = cl.map_shared_rank(own, rank + 1) + m;
+  T ph[NC], rh[NC];
+  const long c0 = lid(L, i + 1, j + 1, 1);
+  cl.sync();  // every CTA's halos are zeroed before anyone writes into them
+#pragma unroll
+  for (int k = 0; k < NC; ++k) {
+    ph[k] = active ? L.phi[c0 + k] : T(0);
+    rh[k] = active ? L.rhs[c0 + k] : T(0);
+    if (active) {
+      own[k * PL + me] = ph[k];
+      if (rW) rW[k * PL] = ph[k];
+      if (rE) rE[k * PL] = ph[k];
+    }
+  }
+  cl.sync();
+  for (int sw = 0; sw < nsweeps; ++sw) {
+#pragma unroll
+    for (int color = 0; color < 2; ++color) {
+      const int kp = (1 + g + color) & 1;
+      if (active) {
+        if (kp == 0) {
+          half_sweep_cols<T, NC, 0, false>(oth, own, PL, me, oW, oE, oS, oN, aw, ae, as, an, az,
+                                           inv_in, inv_lo, inv_hi, ph, rh, nullptr);
+          if (rW) {
+#pragma unroll
+            for (int k = 0; k < NC; k += 2) rW[k * PL] = ph[k];
+          }
+          if (rE) {
+#pragma unroll
+            for (int k = 0; k < NC; k += 2) rE[k * PL] = ph[k];
+          }
+        } else {
+          half_sweep_cols<T, NC, 1, false>(oth, own, PL, me, oW, oE, oS, oN, aw, ae, as, an, az,
+                                           inv_in, inv_lo, inv_hi, ph, rh, nullptr);
+          if (rW) {
+#pragma unroll
+            for (int k = 1; k < NC; k += 2) rW[k * PL] = ph[k];
+          }
+          if (rE) {
+#pragma unroll
+            for (int k = 1; k < NC; k += 2) rE[k * PL] = ph[k];
+          }
+        }
+      }
+      cl.sync();
+    }
+  }
+  if (!active) return;
+#pragma unroll
+  for (int k = 0; k < NC; ++k) {
+    const long c = c0 + k;
+    L.phi[c] = ph[k];
+    if (nsweeps > 0) ring_mirror(L, i, j, k, c, ph[k]);
+  }
+}
+
+template <class T, int NC, int NCL>
+static int launch_coarse_cluster(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
+  using S = ClusterShape<NC, NCL>;
+  const size_t sb = 2ull * NC * S::PL * sizeof(T);
+  auto kern = k_coarse_cluster<T, NC, NCL>;
+  WF_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(S::C, 1, 1);
+  cfg.blockDim = dim3(S::THREADS, 1, 1);
+  cfg.dynamicSmemBytes = sb;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = S::C;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  WF_CK(cudaLaunchKernelEx(&cfg, kern, L, nsweeps));
+  WF_CKL("k_coarse_cluster");
+  return WF_OK;
+}
+
+// coarse strategy: 0 = one CTA (k_coarse_cols), 1 = cluster (k_coarse_cluster)
+static int coarse_strategy() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("WF_COARSE");
+    v = (e && e[0] == '0') ? 0 : 1;
+  }
+  return v;
+}
+
+template <class T>
+static int try_coarse_cluster(const Lvl<T>& L, int nsweeps, cudaStream_t s, int* rc) {
+  switch (L.n) {
+    case 8: *rc = launch_coarse_cluster<T, 8, 1>(L, nsweeps, s); return 1;
+    case 12: *rc = launch_coarse_cluster<T, 12, 2>(L, nsweeps, s); return 1;
+    case 16: *rc = launch_coarse_cluster<T, 16, 2>(L, nsweeps, s); return 1;
+    case 20: *rc = launch_coarse_cluster<T, 20, 4>(L, nsweeps, s); return 1;
+    case 24: *rc = launch_coarse_cluster<T, 24, 3>(L, nsweeps, s); return 1;
     default: return 0;
   }
 }
@@ -413,6 +591,8 @@ static int relax(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
   // small levels with many sweeps: the column kernel
   if (nsweeps > 12 || L.n <= 12) {
     int rc = WF_OK;
+    if (nsweeps > 12 && coarse_strategy() == 1 && try_coarse_cluster<T>(L, nsweeps, s, &rc))
+      return rc;
     if (try_coarse<T>(L, nsweeps, s, &rc)) return rc;
   }
   const size_t sb = smem_bytes<T>(L.n);
