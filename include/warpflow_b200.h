@@ -173,6 +173,10 @@ WF_API int wf_mg_solve_noalloc(const double* su, double* pp, int32_t n, int32_t 
 /* multigrid.py:301-322 one V-cycle on an explicit level-0 pair (phi, rhs)
  * of (n+2)^3 doubles each (the standalone harness of tests/test_mg.py). */
 WF_API int wf_mg_vcycle(const wf_case* c, double* phi0, const double* rhs0, void* stream);
+/* multigrid.py:301-322 as an FP64 defect correction around an FP32 V-cycle:
+ * r = rhs0 - A phi0 (FP64), e = FP32 V-cycle from zero on A e = r, phi0 += e.
+ * FP32 level buffers (level 0 included) come from c->mg_phi / c->mg_rhs. */
+WF_API int wf_mg_dc_cycle(const wf_case* c, double* phi0, const double* rhs0, void* stream);
 /* multigrid.py:289-299 `nsweeps` RBGS sweeps + ring refill on level 0 pair */
 WF_API int wf_mg_relax(const wf_case* c, double* phi0, const double* rhs0,
                 int32_t nsweeps, void* stream);

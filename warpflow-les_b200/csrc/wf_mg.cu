@@ -674,8 +674,120 @@ static int build_levels(const wf_case& c, T* phi0, const T* rhs0, long sI, long 
   return WF_OK;
 }
 
+// ---- mixed precision: FP32 V-cycles inside an FP64 defect correction -------
+// One cycle on the FP64 level-0 pair (phi, rhs):
+//   r = rhs - A phi            (FP64, rounded once to FP32)
+//   e = V-cycle from zero on A e = r, every level in FP32
+//   phi += e                   (FP64, over the real cells and the ring)
+// In exact arithmetic a V-cycle from phi equals phi + V(rhs - A phi), so the
+// FP64 schedule of n_vcycles cycles is reproduced up to FP32 rounding of the
+// corrections; residual and accumulation stay FP64.
+__global__ void __launch_bounds__(MG_TPB) k_defect(const Lvl<double> F, float* rhs_f,
+                                                   float* phi_f, int n) {
+  const long m = (long)n + 2;
+  const long tot = (long)n * n * n;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
+       t += (long)gridDim.x * blockDim.x) {
+    const int k = (int)(t % n);
+    const int j = (int)((t / n) % n);
+    const int i = (int)(t / ((long)n * n));
+    const long c = lid(F, i + 1, j + 1, k + 1);
+    const double aw = i > 0 ? F.ax : 0.0, ae = i < n - 1 ? F.ax : 0.0;
+    const double as = j > 0 ? F.ay : 0.0, an = j < n - 1 ? F.ay : 0.0;
+    const double ab = k > 0 ? F.az : 0.0, at = k < n - 1 ? F.az : 0.0;
+    const double ap = -(aw + ae + as + an + ab + at);
+    const double* p = F.phi;
+    const double r = F.rhs[c] - (aw * p[c - F.sI] + ae * p[c + F.sI] + as * p[c - F.sJ] +
+                                 an * p[c + F.sJ] + ab * p[c - 1] + at * p[c + 1] + ap * p[c]);
+    const long cf = ((long)(i + 1) * m + (j + 1)) * m + (k + 1);
+    rhs_f[cf] = (float)r;
+  }
+  // the FP32 correction starts from zero, ring included
+  const long all = m * m * m;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < all;
+       t += (long)gridDim.x * blockDim.x)
+    phi_f[t] = 0.0f;
+}
+
+__global__ void k_correct(const Lvl<double> F, const float* __restrict__ phi_f, int n) {
+  const long m = (long)n + 2;
+  const long tot = m * m * m;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
+       t += (long)gridDim.x * blockDim.x) {
+    const int k = (int)(t % m);
+    const int j = (int)((t / m) % m);
+    const int i = (int)(t / (m * m));
+    F.phi[lid(F, i, j, k)] += (double)phi_f[t];
+  }
+}
+
+static int build_levels_f32(const wf_case& c, std::vector<Lvl<float>>& lv) {
+  lv.clear();
+  for (int l = 0; l < c.nlev; ++l) {
+    if (!c.mg_phi[l] || !c.mg_rhs[l]) return fail(WF_EINVAL, "missing FP32 multigrid buffer");
+    Lvl<float> L;
+    const double s2 = (double)(1 << l);
+    const double dxl = c.dx * s2, dyl = c.dy * s2, dzl = c.dz * s2;
+    L.ax = (float)(1.0 / (dxl * dxl));
+    L.ay = (float)(1.0 / (dyl * dyl));
+    L.az = (float)(1.0 / (dzl * dzl));
+    L.n = c.n >> l;
+    L.phi = (float*)c.mg_phi[l];
+    L.rhs = (const float*)c.mg_rhs[l];
+    L.sJ = L.n + 2;
+    L.sI = (long)(L.n + 2) * (L.n + 2);
+    lv.push_back(L);
+  }
+  return WF_OK;
+}
+
+static int dc_cycle(const Lvl<double>& F, std::vector<Lvl<float>>& lvf, const wf_case& c,
+                    cudaStream_t s) {
+  const int n = F.n;
+  k_defect<<<mg_blocks((long)n * n * n), MG_TPB, 0, s>>>(F, const_cast<float*>(lvf[0].rhs),
+                                                       lvf[0].phi, n);
+  WF_CKL("k_defect");
+  WF_TRY(vcycle<float>(lvf, c, s));
+  const long m = (long)n + 2;
+  k_correct<<<mg_blocks(m * m * m), MG_TPB, 0, s>>>(F, lvf[0].phi, n);
+  WF_CKL("k_correct");
+  return WF_OK;
+}
+
+static Lvl<double> level0_view(const wf_case& c, double* phi, const double* rhs, long sI,
+                               long sJ) {
+  Lvl<double> L;
+  L.phi = phi;
+  L.rhs = rhs;
+  L.n = c.n;
+  L.sI = sI;
+  L.sJ = sJ;
+  L.ax = 1.0 / (c.dx * c.dx);
+  L.ay = 1.0 / (c.dy * c.dy);
+  L.az = 1.0 / (c.dz * c.dz);
+  return L;
+}
+
+int mg_dc_cycle_pair(const wf_case& c, double* phi0, const double* rhs0, cudaStream_t s) {
+  const long m = c.n + 2;
+  std::vector<Lvl<float>> lvf;
+  WF_TRY(build_levels_f32(c, lvf));
+  return dc_cycle(level0_view(c, phi0, rhs0, m * m, m), lvf, c, s);
+}
+
 int mg_solve(const wf_case& c, cudaStream_t s) {
-  if (c.mg_fp32) return fail(WF_EUNSUPPORTED, "mixed-precision solve not built");
+  if (c.mg_fp32) {
+    const long P = padded(c.n);
+    const long off = (long)(NPL - 1) * (P * P + P + 1);
+    double* pp = c.fld[WF_PP];
+    std::vector<Lvl<float>> lvf;
+    WF_TRY(build_levels_f32(c, lvf));
+    const Lvl<double> F = level0_view(c, pp + off, c.fld[WF_SU] + off, P * P, P);
+    k_zero<double><<<mg_blocks(P * P * P), MG_TPB, 0, s>>>(pp, P * P * P);
+    WF_CKL("k_zero pp");
+    for (int cyc = 0; cyc < c.n_vcycles; ++cyc) WF_TRY(dc_cycle(F, lvf, c, s));
+    return WF_OK;
+  }
   const long P = padded(c.n);
   const long off = (long)(NPL - 1) * (P * P + P + 1);
   double* pp = c.fld[WF_PP];

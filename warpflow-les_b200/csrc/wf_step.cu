@@ -300,6 +300,10 @@ int wf_mg_vcycle(const wf_case* c, double* phi0, const double* rhs0, void* s) {
   if (!c || !phi0 || !rhs0) return fail(WF_EINVAL, "null argument");
   return mg_vcycle_pair(*c, phi0, rhs0, (cudaStream_t)s);
 }
+int wf_mg_dc_cycle(const wf_case* c, double* phi0, const double* rhs0, void* s) {
+  if (!c || !phi0 || !rhs0) return fail(WF_EINVAL, "null argument");
+  return mg_dc_cycle_pair(*c, phi0, rhs0, (cudaStream_t)s);
+}
 int wf_mg_relax(const wf_case* c, double* phi0, const double* rhs0, int32_t nsweeps, void* s) {
   if (!c || !phi0 || !rhs0) return fail(WF_EINVAL, "null argument");
   return mg_relax_pair(*c, phi0, rhs0, nsweeps, (cudaStream_t)s);

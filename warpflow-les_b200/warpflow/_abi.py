@@ -100,6 +100,7 @@ SIGNATURES = {
     "wf_mg_solve_noalloc": (_I32, [_VP, _VP, _I32, _I32, _D, _D, _D, _VP]),
     "wf_mg_vcycle": (_I32, [_CP, _VP, _VP, _VP]),
     "wf_mg_relax": (_I32, [_CP, _VP, _VP, _I32, _VP]),
+    "wf_mg_dc_cycle": (_I32, [_CP, _VP, _VP, _VP]),
     "wf_mg_residual_max": (_I32, [_CP, _VP, _VP, _VP, _VP]),
     "wf_mg_refill": (_I32, [_CP, _VP, _VP]),
     "wf_stepper_create": (_I32, [_CP, _I32, ctypes.POINTER(_VP)]),

@@ -11,6 +11,10 @@ the tunables ``n_pre``, ``n_post``, ``n_coarse``, ``n_vcycles``.
 ``pp`` with ``su`` as its right-hand side, so nothing is copied in or out.
 The level-0 ``phi``/``rhs`` arrays serve the standalone harness form
 (``_vcycle`` / ``_relax(0, n)``), as in tests/test_mg.py.
+
+``precision="mixed"`` (config ``numerics.mg_precision``) runs every V-cycle
+in FP32 as a correction of an FP64 defect correction: the residual, the
+accumulation of the solution and everything outside the multigrid stay FP64.
 """
 from __future__ import annotations
 
@@ -72,8 +76,11 @@ class _Level:
 
 
 class Multigrid:
-    def __init__(self, cfg, topo, device, dx, dy, dz):
+    def __init__(self, cfg, topo, device, dx, dy, dz, precision=None):
         self.cfg = cfg
+        self.precision = precision or getattr(cfg.numerics, "mg_precision", "fp64")
+        if self.precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
         self.topo = topo
         self.device = cuda_device(device)
         nb = topo.local_ncells
@@ -85,6 +92,11 @@ class Multigrid:
             s = 2.0 ** l
             self.levels.append(_Level(tuple(x >> l for x in nb),
                                       (dx * s, dy * s, dz * s), self.device))
+        self._f32 = []
+        if self.precision == "mixed":
+            for lev in self.levels:
+                self._f32.append((DeviceField.zeros(lev.shape, self.device, torch.float32),
+                                  DeviceField.zeros(lev.shape, self.device, torch.float32)))
         self.n_pre = 6       # multigrid.py:257-260
         self.n_post = 6
         self.n_coarse = 300
@@ -108,9 +120,15 @@ class Multigrid:
         c.n_pre, c.n_post = self.n_pre, self.n_post
         c.n_coarse, c.n_vcycles = self.n_coarse, self.n_vcycles
         c.dx, c.dy, c.dz = levels[0].h
-        for l in range(1, len(levels)):
-            c.mg_phi[l] = levels[l].phi.ptr
-            c.mg_rhs[l] = levels[l].rhs.ptr
+        if self._f32 and levels is self.levels:
+            c.mg_fp32 = 1
+            for l, (phi32, rhs32) in enumerate(self._f32):
+                c.mg_phi[l] = phi32.ptr
+                c.mg_rhs[l] = rhs32.ptr
+        else:
+            for l in range(1, len(levels)):
+                c.mg_phi[l] = levels[l].phi.ptr
+                c.mg_rhs[l] = levels[l].rhs.ptr
         if su is not None:
             c.fld[_abi.FIELD_NAMES.index("su")] = su.ptr
         if pp is not None:
@@ -129,10 +147,12 @@ class Multigrid:
                   int(nsweeps), self._stream())
 
     def _vcycle(self):
+        """One V-cycle on level 0 (multigrid.py:301-322); in mixed precision
+        one FP64 defect-correction cycle around an FP32 V-cycle."""
         lev0 = self.levels[0]
         c = self.case()
-        _abi.call("wf_mg_vcycle", ctypes.byref(c), lev0.phi.ptr, lev0.rhs.ptr,
-                  self._stream())
+        name = "wf_mg_dc_cycle" if c.mg_fp32 else "wf_mg_vcycle"
+        _abi.call(name, ctypes.byref(c), lev0.phi.ptr, lev0.rhs.ptr, self._stream())
 
     def residual_max(self, l=0):
         """max |rhs - A phi| of a level (reference tests/test_mg.py:16-32)."""

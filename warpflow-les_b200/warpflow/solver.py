@@ -56,13 +56,7 @@ class FlowSolver:
         self.bcs = BoundaryKernels(self.bnd, dev)
         self.ulid = b.lid_velocity
         self.mg = Multigrid(cfg, topo, dev, self.dx, self.dy, self.dz)
-        self.mixed = cfg.numerics.mg_precision == "mixed"
-        self._mg32 = []
-        if self.mixed:
-            for lev in self.mg.levels:
-                shp = lev.shape
-                self._mg32.append((DeviceField.zeros(shp, dev, torch.float32),
-                                   DeviceField.zeros(shp, dev, torch.float32)))
+        self.mixed = self.mg.precision == "mixed"
 
         nsc = ctypes.sizeof(_abi.WfScalars)
         self._sc = torch.zeros(nsc, dtype=torch.uint8, device=dev)
@@ -105,7 +99,6 @@ class FlowSolver:
         c.sgs = 1 if cfg.physics.sgs_enabled else 0
         c.variable_dt = 1 if cfg.time.variable_dt else 0
         c.maxcy = int(cfg.numerics.max_outer_iters)
-        c.mg_fp32 = 1 if self.mixed else 0
         c.dx, c.dy, c.dz = self.dx, self.dy, self.dz
         c.rrey = self.rey
         c.cw = float(cfg.physics.sgs_cw)
@@ -115,10 +108,6 @@ class FlowSolver:
         c.eps = float(cfg.numerics.div_tolerance)
         for i, name in enumerate(_abi.FIELD_NAMES):
             c.fld[i] = self.f[name].ptr
-        if self.mixed:
-            for l, (phi32, rhs32) in enumerate(self._mg32):
-                c.mg_phi[l] = phi32.ptr
-                c.mg_rhs[l] = rhs32.ptr
         c.sc = self._sc.data_ptr()
         return c
 
