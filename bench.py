@@ -163,6 +163,133 @@ def run_oracle(n, levels, steps, warmup):
     return n ** 3 * steps / dt / 1e6, dt
 
 
+def _events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def bench_ensemble(args):
+    """Config 3: 64 seeded cavity cases (N in {32..96}, Re in [100, 1000], lid
+    in [0.5, 1.5]), mixed-precision multigrid, advanced together; compared
+    with the plain FP64 per-case loop (one case after another) on the same
+    cases."""
+    import torch
+    from warpflow.ensemble import Ensemble, cavity_case, random_ensemble
+    specs = random_ensemble(args.cases, seed=0)
+    K, W = args.steps, max(3, args.warmup)
+
+    def run(precision, concurrent, steps, warm):
+        cfgs = [cavity_case(sp.n, sp.re, sp.ulid, precision=precision) for sp in specs]
+        ens = Ensemble(cfgs, nstreams=16 if concurrent else 1)
+        for _ in range(warm):
+            ens.step()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            if concurrent:
+                ens.step()
+            else:
+                for i in range(len(ens)):
+                    ens.step([i])
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        cells = ens.cells(range(len(ens)))
+        iters = sum(s.outer_iters for s in ens.solvers) / len(ens)
+        ens.close()
+        return cells * steps / dt / 1e6, dt, iters
+
+    val, dt, iters = run("mixed", True, K, W)
+    plain, pdt, _ = run("fp64", False, max(2, K // 4), 2)
+    print(json.dumps({
+        "mode": "ensemble", "metric": "Mcell-steps/s (64-case cavity ensemble, mixed MG)",
+        "value": round(val, 2), "unit": "Mcell-steps/s", "steps": K, "warmup": W,
+        "ms_per_batch_step": round(1e3 * dt / K, 3), "iters_mean": round(iters, 2),
+        "plain_fp64_per_case_loop": round(plain, 2),
+        "speedup_vs_plain": round(val / plain, 2),
+        "config": {"cases": args.cases, "sizes": sorted({sp.n for sp in specs}),
+                   "seed": 0, "timing": "wall clock around whole batch steps, synced"}}),
+        flush=True)
+
+
+def bench_serve(args):
+    """Config 4: a seeded Poisson request stream (20 req/s, N in {32..128},
+    Re in [100, 1000], steps in [100, 2000] scaled by --step-scale) served
+    with continuous batching under a 150 GB budget."""
+    from warpflow.serve import CavityServer, poisson_stream
+    reqs = poisson_stream(count=args.requests, rate=20.0, seed=0,
+                          step_scale=args.step_scale)
+    srv = CavityServer(budget_bytes=150 * 10 ** 9, nstreams=16)
+    srv.run(reqs)
+    s = srv.summary()
+    print(json.dumps({
+        "mode": "serve", "metric": "served cavity stream: p50/p99 latency, Mcell-steps/s",
+        "p50_s": round(s["p50_s"], 4), "p99_s": round(s["p99_s"], 4),
+        "value": round(s["mcell_steps_per_s"], 2), "unit": "Mcell-steps/s",
+        "wall_s": round(s["wall_s"], 2), "step_batches": s["step_batches"],
+        "peak_resident_GB": round(s["peak_resident_bytes"] / 1e9, 3),
+        "config": {"requests": args.requests, "rate_per_s": 20.0, "seed": 0,
+                   "step_scale": args.step_scale, "budget_GB": 150,
+                   "latency": "arrival to end of last step, wall clock"}}), flush=True)
+
+
+def bench_poisson(args):
+    """Config 2: standalone Poisson solve on 256^3 with 5 levels, RHS
+    N(0,1) on the 258^3 level-0 array with the ring zeroed and the mean
+    removed (the reference harness tests/test_mg.py), solved to a relative
+    max-norm residual of 1e-10 with FP64 V-cycles and with FP32 V-cycles in
+    FP64 defect correction."""
+    import numpy as np
+    import torch
+    from oracle.wf_oracle import make_mg_rhs
+    from warpflow import Multigrid, build_topology
+    from warpflow.config import case_from_dict
+    n, L = args.n if args.n != 80 else 256, 5
+    rhs = make_mg_rhs(n, seed=0)
+    out = {"mode": "poisson", "metric": "standalone Poisson to rel. residual 1e-10",
+           "config": {"n": n, "levels": L, "rhs": "default_rng(0).standard_normal, ring 0, "
+                                                 "mean removed", "tol": 1e-10}}
+    sols = {}
+    for prec in ("fp64", "mixed"):
+        cfg = case_from_dict({"grid": {"nx": n, "ny": n, "nz": n},
+                              "numerics": {"mg_levels": L, "mg_precision": prec}})
+        mg = Multigrid(cfg, build_topology(cfg), "cuda:0", 1.0 / n, 1.0 / n, 1.0 / n)
+        lev0 = mg.levels[0]
+        lev0.rhs.assign(rhs)
+        lev0.phi.zero_()
+        mg._refill(lev0)
+        r0 = mg.residual_max(0)
+        cyc, ms = 0, 0.0
+        hist = []
+        while cyc < 60:
+            a, b = _events()
+            a.record()
+            mg._vcycle()
+            b.record()
+            r = mg.residual_max(0)
+            ms += a.elapsed_time(b)
+            cyc += 1
+            hist.append(r / r0)
+            if r <= 1e-10 * r0:
+                break
+        s = slice(1, n + 1)
+        phi = lev0.phi.t[s, s, s]
+        res_l2 = None
+        sols[prec] = phi.double().clone()
+        # bytes per fine cell per cycle: FP64 V-cycle + residual check, or the
+        # FP32 V-cycle + FP64 residual (read phi, rhs, write r32) + FP64 correction
+        cell_b = (8 * vcycle_words(L) + 16) if prec == "fp64" else (4 * vcycle_words(L) + 40)
+        out[prec] = {"cycles": cyc, "ms": round(ms, 3), "ms_per_cycle": round(ms / cyc, 3),
+                     "rel_residual": hist[-1], "residual_history": [float("%.3e" % h) for h in hist],
+                     "alg_GBps": round(n ** 3 * cell_b * cyc / (ms / 1e3) / 1e9, 1)}
+        del mg
+        torch.cuda.empty_cache()
+    d = sols["mixed"] - sols["fp64"]
+    d = d - d.mean()
+    out["mixed_vs_fp64_max_abs"] = float(d.abs().max())
+    out["fp64_solution_max_abs"] = float((sols["fp64"] - sols["fp64"].mean()).abs().max())
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -174,7 +301,18 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--mode", default="step", choices=["step", "ensemble", "serve", "poisson"])
+    ap.add_argument("--cases", type=int, default=64)
+    ap.add_argument("--requests", type=int, default=48)
+    ap.add_argument("--step-scale", type=float, default=0.05)
     args = ap.parse_args()
+    if args.mode != "step":
+        import torch
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        {"ensemble": bench_ensemble, "serve": bench_serve, "poisson": bench_poisson}[
+            args.mode](args)
+        return
     K, W = args.steps, max(3, args.warmup)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

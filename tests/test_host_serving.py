@@ -1,0 +1,115 @@
+"""Host-side logic of batching and serving (CPU): request streams, the
+admission ledger, rank sharding and the max-over-ranks timing reduction
+over a 2-rank gloo group."""
+import os
+import socket
+
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+
+def test_poisson_stream_seeded():
+    from warpflow.serve import poisson_stream
+    a = poisson_stream(count=50, seed=3)
+    b = poisson_stream(count=50, seed=3)
+    assert [(r.n, r.n_steps, r.arrival) for r in a] == [(r.n, r.n_steps, r.arrival) for r in b]
+    assert all(32 <= r.n <= 128 and r.n % 16 == 0 for r in a)
+    assert all(100 <= r.n_steps <= 2000 for r in a)
+    arr = [r.arrival for r in a]
+    assert arr == sorted(arr)
+    # mean inter-arrival near 1/20 s
+    assert 0.02 < arr[-1] / len(arr) < 0.09
+
+
+def test_levels_for_keeps_coarse_small():
+    from warpflow.serve import levels_for
+    assert levels_for(80) == 3
+    assert levels_for(128) == 3      # coarse 32
+    assert levels_for(256) == 4      # coarse 32
+    assert (256 >> (levels_for(256) - 1)) <= 32
+
+
+def test_admission_fifo_budget():
+    from warpflow.serve import Admission, Request, case_bytes
+    b32 = case_bytes(32)
+    adm = Admission(budget_bytes=int(2.5 * b32))
+    reqs = [Request(i, 32, 400.0, 1.0, 10, arrival=0.1 * i) for i in range(4)]
+    for r in reqs:
+        adm.submit(r)
+    assert adm.admit(0.05) == [reqs[0]]
+    got = adm.admit(1.0)
+    assert got == [reqs[1]]              # third does not fit
+    assert adm.used == 2 * b32 <= adm.budget
+    adm.release(0)
+    assert adm.admit(1.0) == [reqs[2]]   # freed memory admits the next, in order
+    assert adm.peak <= adm.budget
+
+
+def test_admission_no_overtaking():
+    from warpflow.serve import Admission, Request, case_bytes
+    big, small = case_bytes(128), case_bytes(32)
+    adm = Admission(budget_bytes=big + small // 2)
+    adm.submit(Request(0, 32, 400.0, 1.0, 10, arrival=0.0))
+    adm.submit(Request(1, 128, 400.0, 1.0, 10, arrival=0.1))
+    adm.submit(Request(2, 32, 400.0, 1.0, 10, arrival=0.2))
+    assert [r.rid for r in adm.admit(1.0)] == [0]   # 1 blocks 2 (FIFO)
+    adm.release(0)
+    assert [r.rid for r in adm.admit(1.0)] == [1]
+
+
+def test_admission_rejects_oversize():
+    from warpflow.serve import Admission, Request
+    adm = Admission(budget_bytes=1000)
+    with pytest.raises(ValueError):
+        adm.submit(Request(0, 32, 400.0, 1.0, 10, arrival=0.0))
+
+
+def test_case_bytes_formula():
+    from warpflow.serve import case_bytes
+    n = 80
+    f = 13 * 86 ** 3 * 8
+    mg64 = 2 * 8 * (82 ** 3 + 42 ** 3 + 22 ** 3)
+    mg32 = 2 * 4 * (82 ** 3 + 42 ** 3 + 22 ** 3)
+    assert case_bytes(n, 3, "fp64") - f - mg64 < 4096
+    assert case_bytes(n, 3, "mixed") - f - mg64 - mg32 < 4096
+
+
+def test_shard_round_robin():
+    from warpflow.dist import shard
+    items = list(range(10))
+    parts = [shard(items, r, 3) for r in range(3)]
+    assert sorted(sum(parts, [])) == items
+    assert parts[1] == [1, 4, 7]
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    from warpflow.dist import max_over_ranks, shard, sum_over_ranks
+    mine = shard(range(7), rank, world)
+    tmax = max_over_ranks(1.5 + rank)
+    cells = sum_over_ranks(sum(mine))
+    out[rank] = (tmax, cells, len(mine))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_rank_replica_reductions():
+    """The N>1 bench path: each rank times its own replica, rank 0 reports
+    the max time and the summed work (gloo, world size 2, CPU)."""
+    port = _free_port()
+    mgr = mp.Manager()
+    out = mgr.dict()
+    mp.spawn(_worker, args=(2, port, out), nprocs=2, join=True)
+    assert out[0][0] == out[1][0] == 2.5
+    assert out[0][1] == out[1][1] == sum(range(7))
+    assert out[0][2] + out[1][2] == 7

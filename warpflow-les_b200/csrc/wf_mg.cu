@@ -528,11 +528,16 @@ static int coarse_strategy() {
 template <class T>
 static int try_coarse_cluster(const Lvl<T>& L, int nsweeps, cudaStream_t s, int* rc) {
   switch (L.n) {
+    case 6: *rc = launch_coarse_cluster<T, 6, 1>(L, nsweeps, s); return 1;
     case 8: *rc = launch_coarse_cluster<T, 8, 1>(L, nsweeps, s); return 1;
+    case 10: *rc = launch_coarse_cluster<T, 10, 2>(L, nsweeps, s); return 1;
     case 12: *rc = launch_coarse_cluster<T, 12, 2>(L, nsweeps, s); return 1;
+    case 14: *rc = launch_coarse_cluster<T, 14, 2>(L, nsweeps, s); return 1;
     case 16: *rc = launch_coarse_cluster<T, 16, 2>(L, nsweeps, s); return 1;
     case 20: *rc = launch_coarse_cluster<T, 20, 4>(L, nsweeps, s); return 1;
     case 24: *rc = launch_coarse_cluster<T, 24, 3>(L, nsweeps, s); return 1;
+    case 28: *rc = launch_coarse_cluster<T, 28, 4>(L, nsweeps, s); return 1;
+    case 32: *rc = launch_coarse_cluster<T, 32, 4>(L, nsweeps, s); return 1;
     default: return 0;
   }
 }

@@ -1,0 +1,238 @@
+"""Continuous-batching server for cavity solves.
+
+Requests (N, Re, lid velocity, step count) arrive over time.  The server
+admits a queued request as soon as its device memory -- fields plus
+multigrid hierarchy, computed exactly by ``case_bytes`` -- fits in the HBM
+budget next to the cases already resident, keeps every admitted case
+resident until its last step, and advances all resident cases together one
+step at a time (``Ensemble``-style concurrent graph launches).  Requests
+that arrive while others run join at the next step boundary; finished
+cases leave at a step boundary and free their memory for the queue.
+Latency is measured from arrival to the end of the request's last step.
+
+``Admission`` holds the queueing policy and the memory ledger with no GPU
+dependency, so it is tested on the CPU.
+"""
+from __future__ import annotations
+
+import collections
+import ctypes
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _abi
+from .ensemble import cavity_case
+from .fields import cuda_device
+from .solver import FlowSolver
+from .topology import build_topology
+
+NFIELDS = 13
+
+
+def case_bytes(n, levels=3, precision="mixed"):
+    """Device bytes a FlowSolver of an n^3 case allocates: 13 padded FP64
+    fields, FP64 multigrid levels (phi, rhs with one ring, level 0
+    included), the FP32 copies of every level in mixed precision, and two
+    scalar blocks plus one residual slot."""
+    fields = NFIELDS * (n + 6) ** 3 * 8
+    mg = 0
+    for l in range(levels):
+        m = (n >> l) + 2
+        mg += 2 * m ** 3 * 8
+        if precision == "mixed":
+            mg += 2 * m ** 3 * 4
+    return fields + mg + 2 * ctypes.sizeof(_abi.WfScalars) + 8
+
+
+def levels_for(n, coarse_max=32):
+    """Multigrid depth for a request: 3 levels (the reference cases') unless
+    the coarse grid would exceed `coarse_max` cells per axis."""
+    levels = 3
+    while (n >> (levels - 1)) > coarse_max and n % (1 << levels) == 0:
+        levels += 1
+    return levels
+
+
+@dataclass
+class Request:
+    rid: int
+    n: int
+    re: float
+    ulid: float
+    n_steps: int
+    arrival: float            # seconds after the stream starts
+    levels: int = 3
+    precision: str = "mixed"
+
+    @property
+    def bytes(self):
+        return case_bytes(self.n, self.levels, self.precision)
+
+
+@dataclass
+class Completion:
+    rid: int
+    arrival: float
+    admitted: float
+    finished: float
+    steps: int
+    cells: int
+    info: dict = field(default_factory=dict)
+    error: str = ""
+
+    @property
+    def latency(self):
+        return self.finished - self.arrival
+
+
+class Admission:
+    """FIFO admission against a memory budget (no GPU needed)."""
+
+    def __init__(self, budget_bytes, max_active=None):
+        self.budget = int(budget_bytes)
+        self.max_active = max_active
+        self.queue = collections.deque()
+        self.resident = {}     # rid -> bytes
+        self.peak = 0
+
+    @property
+    def used(self):
+        return sum(self.resident.values())
+
+    def submit(self, req):
+        if req.bytes > self.budget:
+            raise ValueError("request %d needs %d bytes, more than the whole budget %d"
+                             % (req.rid, req.bytes, self.budget))
+        self.queue.append(req)
+
+    def admit(self, now):
+        """Pop the requests that have arrived by `now` and fit, in arrival
+        order; stop at the first one that does not fit (no overtaking)."""
+        out = []
+        while self.queue and self.queue[0].arrival <= now:
+            req = self.queue[0]
+            if self.max_active is not None and len(self.resident) >= self.max_active:
+                break
+            if self.used + req.bytes > self.budget:
+                break
+            self.queue.popleft()
+            self.resident[req.rid] = req.bytes
+            self.peak = max(self.peak, self.used)
+            out.append(req)
+        return out
+
+    def release(self, rid):
+        self.resident.pop(rid, None)
+
+
+def poisson_stream(count=256, rate=20.0, seed=0, sizes=tuple(range(32, 129, 16)),
+                   re=(100.0, 1000.0), ulid=(1.0, 1.0), steps=(100, 2000),
+                   precision="mixed", step_scale=1.0):
+    """Seeded request stream: exponential inter-arrival times at `rate`
+    requests/s, N uniform over `sizes`, Re uniform, step counts uniform over
+    the integer range (scaled by `step_scale`, at least 1)."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for rid in range(count):
+        t += float(rng.exponential(1.0 / rate))
+        n = int(rng.choice(sizes))
+        ns = int(rng.integers(steps[0], steps[1] + 1))
+        out.append(Request(rid=rid, n=n, re=float(rng.uniform(*re)),
+                           ulid=float(rng.uniform(*ulid)),
+                           n_steps=max(1, int(round(ns * step_scale))), arrival=t,
+                           levels=levels_for(n), precision=precision))
+    return out
+
+
+class CavityServer:
+    """Runs a request stream to completion with continuous batching."""
+
+    def __init__(self, device="cuda:0", budget_bytes=150 * 10 ** 9, nstreams=16,
+                 max_active=None, keep_fields=False):
+        self.device = cuda_device(device)
+        self.adm = Admission(budget_bytes, max_active)
+        self.streams = [torch.cuda.Stream(self.device) for _ in range(nstreams)]
+        self.keep_fields = keep_fields
+        self.results = {}
+        self.fields = {}
+        self.cell_steps = 0
+        self.step_batches = 0
+        self._nsc = ctypes.sizeof(_abi.WfScalars)
+        self._host = torch.empty(4096 * self._nsc, dtype=torch.uint8, pin_memory=True)
+
+    def _build(self, req):
+        cfg = cavity_case(req.n, req.re, req.ulid, levels=req.levels,
+                          precision=req.precision, name="req%d" % req.rid)
+        return FlowSolver(cfg, build_topology(cfg), self.device)
+
+    def run(self, requests, time_scale=1.0):
+        """Serve `requests` (arrival times in seconds, compressed by
+        `time_scale`); returns the completions in request order."""
+        for r in sorted(requests, key=lambda r: r.arrival):
+            self.adm.submit(r)
+        live = {}          # rid -> (req, solver, admitted_at, steps_done)
+        t0 = time.perf_counter()
+        main = torch.cuda.current_stream(self.device)
+        total = len(requests)
+        while len(self.results) < total:
+            now = (time.perf_counter() - t0) / time_scale
+            for req in self.adm.admit(now):
+                live[req.rid] = [req, self._build(req), now, 0]
+            if not live:
+                nxt = self.adm.queue[0].arrival if self.adm.queue else now
+                time.sleep(max(0.0, (nxt - now) * time_scale))
+                continue
+            rids = list(live)
+            start = torch.cuda.Event()
+            start.record(main)
+            used = set()
+            for slot, rid in enumerate(rids):
+                s = self.streams[slot % len(self.streams)]
+                used.add(s)
+                s.wait_event(start)
+                with torch.cuda.stream(s):
+                    live[rid][1].launch_step()
+            for s in used:
+                main.wait_stream(s)
+            blob = torch.cat([live[rid][1]._sc for rid in rids])
+            if blob.numel() > self._host.numel():
+                self._host = torch.empty(blob.numel(), dtype=torch.uint8, pin_memory=True)
+            host = self._host[:blob.numel()]
+            host.copy_(blob, non_blocking=True)
+            main.synchronize()
+            self.step_batches += 1
+            done_t = (time.perf_counter() - t0) / time_scale
+            for k, rid in enumerate(rids):
+                req, sol, adm_t, nst = live[rid]
+                view = _abi.WfScalars.from_address(host.data_ptr() + k * self._nsc)
+                err = ""
+                try:
+                    info = sol.apply_scalars(view)
+                except RuntimeError as e:
+                    info, err = {}, str(e)
+                nst += 1
+                live[rid][3] = nst
+                self.cell_steps += req.n ** 3
+                if nst >= req.n_steps or err:
+                    self.results[rid] = Completion(rid, req.arrival, adm_t, done_t, nst,
+                                                   req.n ** 3, info, err)
+                    if self.keep_fields:
+                        self.fields[rid] = {k2: sol.f[k2].numpy() for k2 in ("u", "v", "w", "p")}
+                    sol.close()
+                    del live[rid]
+                    self.adm.release(rid)
+        self.wall = time.perf_counter() - t0
+        return [self.results[r.rid] for r in requests]
+
+    def summary(self):
+        lat = np.array([c.latency for c in self.results.values()])
+        return {"requests": len(lat),
+                "p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
+                "p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
+                "mcell_steps_per_s": self.cell_steps / self.wall / 1e6 if self.wall else None,
+                "wall_s": self.wall, "step_batches": self.step_batches,
+                "peak_resident_bytes": self.adm.peak}

@@ -170,7 +170,11 @@ class FlowSolver:
     def finish_step(self):
         """Wait for the enqueued step, update the host-side scalars and raise
         the reference's errors."""
-        sc = self._pull_scalars()
+        return self.apply_scalars(self._pull_scalars())
+
+    def apply_scalars(self, sc):
+        """Take the device scalar block of a finished step (a WfScalars view)
+        into the host attributes; raise the reference's errors."""
         self.last_nmg = int(sc.nmg)
         self.itime = int(sc.itime)
         self._dt = float(sc.dt)
@@ -194,6 +198,17 @@ class FlowSolver:
             self._push_scalar("status", _abi.ST_OK)
         return {"ctime": self._ctime, "dt": self._dt, "rmax": self.rmax,
                 "iters": self.outer_iters, "cfl": self.cfl}
+
+    def device_bytes(self):
+        """Device memory held by this solver's fields, multigrid hierarchy
+        and scalar block."""
+        ts = [f.t for f in self.f.values()] + [self._sc]
+        for lev in self.mg.levels:
+            ts += [lev.phi.t, lev.rhs.t]
+        for a, b in self.mg._f32:
+            ts += [a.t, b.t]
+        ts += [self.mg._sc, self.mg._out]
+        return int(sum(t.numel() * t.element_size() for t in ts))
 
     def close(self):
         if getattr(self, "_stepper", None):
