@@ -110,6 +110,11 @@ WF_API const char* wf_last_error(void);
 WF_API int wf_struct_sizes(int64_t* scalars, int64_t* casebytes);
 /* solver.py:60-65 initial scalars: dt = dt0, ctime = 0, itime = 0, ... */
 WF_API int wf_scalars_init(wf_scalars* sc, double dt0, void* stream);
+/* Tuning knob (no reference counterpart): how a many-sweep relax of an n^3
+ * level (n <= 64) runs -- 0 one CTA, 1 cluster with a barrier per
+ * half-sweep, 2 cluster with point-to-point halo pushes.  Process-wide;
+ * set before graphs are built.  fp32 selects the mixed-precision table. */
+WF_API int wf_set_coarse_strategy(int32_t n, int32_t fp32, int32_t strategy);
 /* bytes of MG workspace a case needs at each level (caller allocates) */
 WF_API int wf_mg_level_elems(int32_t n, int32_t nlev, int32_t level, int64_t* elems);
 

@@ -71,6 +71,7 @@ int mg_vcycle_pair(const wf_case& c, double* phi0, const double* rhs0, cudaStrea
 int mg_relax_pair(const wf_case& c, double* phi0, const double* rhs0, int nsweeps,
                   cudaStream_t s);
 int mg_refill_pair(const wf_case& c, double* phi0, cudaStream_t s);
+int set_coarse_strategy(int n, int fp32, int strategy);
 int mg_dc_cycle_pair(const wf_case& c, double* phi0, const double* rhs0, cudaStream_t s);
 int mg_solve_noalloc(const double* su, double* pp, int n, int nlev, double dx, double dy,
                      double dz, cudaStream_t s);

@@ -39,6 +39,7 @@ struct Lvl {
   int n;         // real cells per axis
   long sI, sJ;   // strides (k stride 1)
   T ax, ay, az;  // 1/h^2 per axis of this level
+  int* err;      // where a device-side wait records a timeout (may be null)
 };
 
 template <class T>
@@ -515,14 +516,290 @@ static int launch_coarse_cluster(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
   return WF_OK;
 }
 
-// coarse strategy: 0 = one CTA (k_coarse_cols), 1 = cluster (k_coarse_cluster)
-static int coarse_strategy() {
-  static int v = -1;
-  if (v < 0) {
-    const char* e = getenv("WF_COARSE");
-    v = (e && e[0] == '0') ? 0 : 1;
+// ---- point-to-point variant: halo pushes complete on the receiver's mbarrier
+// Same slab decomposition as k_coarse_cluster, but no cluster-wide barrier
+// inside the sweep loop.  A thread on a slab's first/last plane sends each
+// value it updates straight into the neighbouring CTA's halo plane with
+// st.async, whose completion is counted in bytes on that CTA's mbarrier for
+// the colour of the data.  Before a half-sweep reads halo values of one
+// colour, every thread waits on its own CTA's barrier for that colour, so
+// nobody waits for a memory fence or for CTAs it does not exchange with.
+// Ordering: a neighbour can only produce the next values of a colour after
+// receiving the values this CTA computes from the current ones, so a halo
+// cell is never overwritten while it may still be read.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ uint32_t mapa_u32(uint32_t a, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void mbar_init(uint32_t a, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t a, uint32_t tx) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(tx)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t a, uint32_t parity, int mode) {
+  uint32_t ok;
+  if (mode == 0) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity), "r"(1000u)
+        : "memory");
+  } else if (mode == 1) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+  } else {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
   }
-  return v;
+  return ok != 0;
+}
+__device__ __forceinline__ void st_async(uint32_t raddr, double v, uint32_t rmbar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b64 [%0], %1, [%2];" ::"r"(
+                   raddr),
+               "l"(__double_as_longlong(v)), "r"(rmbar)
+               : "memory");
+}
+__device__ __forceinline__ void st_async(uint32_t raddr, float v, uint32_t rmbar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b32 [%0], %1, [%2];" ::"r"(
+                   raddr),
+               "r"(__float_as_uint(v)), "r"(rmbar)
+               : "memory");
+}
+
+// bounded wait: at most 2^22 tries (about a second with suspending tries,
+// much less when spinning)
+constexpr int MBAR_WAIT_TRIES = 1 << 22;
+
+template <class T, int NC, int NCL>
+__global__ void __launch_bounds__(ClusterShape<NC, NCL>::THREADS)
+    k_coarse_p2p(Lvl<T> L, int nsweeps, int wmode) {
+  using S = ClusterShape<NC, NCL>;
+  constexpr int H = S::H, HALF = S::HALF, GROUP = S::GROUP, PL = S::PL, C = S::C;
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  extern __shared__ __align__(16) unsigned char smraw[];
+  __shared__ __align__(8) unsigned long long mbar[2];
+  __shared__ int s_bail;
+  T* sp = reinterpret_cast<T*>(smraw);
+  const int tid = threadIdx.x;
+  const uint32_t mb[2] = {smem_u32(&mbar[0]), smem_u32(&mbar[1])};
+  if (tid == 0) {
+    mbar_init(mb[0], 1);
+    mbar_init(mb[1], 1);
+    s_bail = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  for (int t = tid; t < 2 * NC * PL; t += blockDim.x) sp[t] = T(0);
+  const int g = tid / GROUP;
+  const int q = tid - g * GROUP;
+  const bool active = q < HALF;
+  const int il = active ? q / H : 0;
+  const int m = active ? q - il * H : 0;
+  const int i = rank * NCL + il;
+  const int j = 2 * m + ((i + g) & 1);
+  T* own = sp + g * NC * PL;
+  const T* oth = sp + (1 - g) * NC * PL;
+  const int me = (il + 1) * H + m;
+  const int oW = me - H, oE = me + H;
+  const int oS = j > 0 ? (il + 1) * H + ((j - 1) >> 1) : me;
+  const int oN = j < NC - 1 ? (il + 1) * H + ((j + 1) >> 1) : me;
+  const T aw = i > 0 ? L.ax : T(0), ae = i < NC - 1 ? L.ax : T(0);
+  const T as = j > 0 ? L.ay : T(0), an = j < NC - 1 ? L.ay : T(0);
+  const T az = L.az;
+  const T inv_in = T(1) / (-(aw + ae + as + an + az + az));
+  const T inv_lo = T(1) / (-(aw + ae + as + an + T(0) + az));
+  const T inv_hi = T(1) / (-(aw + ae + as + an + az + T(0)));
+  const bool sendW = active && il == 0 && rank > 0;
+  const bool sendE = active && il == NCL - 1 && rank < C - 1;
+  // this column's halo slot in the neighbour (same parity array, k = 0)
+  const uint32_t own_u32 = smem_u32(own);
+  uint32_t aW = 0, aE = 0, mW[2] = {0, 0}, mE[2] = {0, 0};
+  if (sendW) {
+    aW = mapa_u32(own_u32 + (uint32_t)(((NCL + 1) * H + m) * sizeof(T)), rank - 1);
+    mW[0] = mapa_u32(mb[0], rank - 1);
+    mW[1] = mapa_u32(mb[1], rank - 1);
+  }
+  if (sendE) {
+    aE = mapa_u32(own_u32 + (uint32_t)(m * sizeof(T)), rank + 1);
+    mE[0] = mapa_u32(mb[0], rank + 1);
+    mE[1] = mapa_u32(mb[1], rank + 1);
+  }
+  const int nbr = (rank > 0 ? 1 : 0) + (rank < C - 1 ? 1 : 0);
+  const uint32_t tx = (uint32_t)(nbr * (NC * NC / 2) * sizeof(T));
+  T ph[NC], rh[NC];
+  const long c0 = lid(L, i + 1, j + 1, 1);
+  cl.sync();  // barriers initialised and halos zeroed in every CTA
+  T* rWp = sendW ? cl.map_shared_rank(own, rank - 1) + (NCL + 1) * H + m : nullptr;
+  T* rEp = sendE ? cl.map_shared_rank(own, rank + 1) + m : nullptr;
+#pragma unroll
+  for (int k = 0; k < NC; ++k) {
+    ph[k] = active ? L.phi[c0 + k] : T(0);
+    rh[k] = active ? L.rhs[c0 + k] : T(0);
+    if (active) {
+      own[k * PL + me] = ph[k];
+      if (rWp) rWp[k * PL] = ph[k];
+      if (rEp) rEp[k * PL] = ph[k];
+    }
+  }
+  if (tid == 0 && nsweeps > 0) {
+    mbar_arrive_expect_tx(mb[0], tx);
+    mbar_arrive_expect_tx(mb[1], tx);
+  }
+  cl.sync();  // initial halos in place everywhere
+  const int nh = 2 * nsweeps;
+  bool bailed = false;
+  for (int t = 0; t < nh; ++t) {
+    if (t > 0) {
+      // halo values of the colour read now were produced at t-1
+      const int c = (t - 1) & 1;
+      const uint32_t par = (uint32_t)(((t - 1) >> 1) & 1);
+      bool ok = false;
+      for (int it = 0; it < MBAR_WAIT_TRIES && !ok; ++it) ok = mbar_try_wait(mb[c], par, wmode);
+      if (!ok) s_bail = 1;
+      if (tid == 0 && t + 1 < nh) mbar_arrive_expect_tx(mb[c], tx);
+    }
+    __syncthreads();  // local values of t-1 visible; bail decision uniform
+    if (s_bail) {
+      bailed = true;
+      break;
+    }
+    const int kp = (1 + g + (t & 1)) & 1;
+    if (active) {
+      if (kp == 0)
+        half_sweep_cols<T, NC, 0, false>(oth, own, PL, me, oW, oE, oS, oN, aw, ae, as, an, az,
+                                         inv_in, inv_lo, inv_hi, ph, rh, nullptr);
+      else
+        half_sweep_cols<T, NC, 1, false>(oth, own, PL, me, oW, oE, oS, oN, aw, ae, as, an, az,
+                                         inv_in, inv_lo, inv_hi, ph, rh, nullptr);
+      const uint32_t mc = (uint32_t)(t & 1);
+      if (sendW) {
+#pragma unroll
+        for (int k = 0; k < NC; ++k)
+          if ((k & 1) == kp) st_async(aW + (uint32_t)(k * PL * sizeof(T)), ph[k], mW[mc]);
+      }
+      if (sendE) {
+#pragma unroll
+        for (int k = 0; k < NC; ++k)
+          if ((k & 1) == kp) st_async(aE + (uint32_t)(k * PL * sizeof(T)), ph[k], mE[mc]);
+      }
+    }
+  }
+  if (!bailed && nh > 0) {
+    // the neighbours' last pushes (colour of t = nh-1) must land before exit
+    const int c = (nh - 1) & 1;
+    const uint32_t par = (uint32_t)(((nh - 1) >> 1) & 1);
+    bool ok = false;
+    for (int it = 0; it < MBAR_WAIT_TRIES && !ok; ++it) ok = mbar_try_wait(mb[c], par, wmode);
+    if (!ok) s_bail = 1;
+  }
+  __syncthreads();
+  if (s_bail && tid == 0 && L.err) atomicExch(L.err, (int)WF_ST_WAIT_TIMEOUT);
+  cl.sync();
+  if (!active) return;
+#pragma unroll
+  for (int k = 0; k < NC; ++k) {
+    const long c = c0 + k;
+    L.phi[c] = ph[k];
+    if (nsweeps > 0) ring_mirror(L, i, j, k, c, ph[k]);
+  }
+}
+
+template <class T, int NC, int NCL>
+static int launch_coarse_p2p(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
+  using S = ClusterShape<NC, NCL>;
+  const size_t sb = 2ull * NC * S::PL * sizeof(T);
+  auto kern = k_coarse_p2p<T, NC, NCL>;
+  WF_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(S::C, 1, 1);
+  cfg.blockDim = dim3(S::THREADS, 1, 1);
+  cfg.dynamicSmemBytes = sb;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = S::C;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  static int wmode = -1;
+  if (wmode < 0) {
+    const char* e = getenv("WF_MBWAIT");
+    wmode = (e && e[0] >= '0' && e[0] <= '2') ? e[0] - '0' : 1;
+  }
+  WF_CK(cudaLaunchKernelEx(&cfg, kern, L, nsweeps, wmode));
+  WF_CKL("k_coarse_p2p");
+  return WF_OK;
+}
+
+template <class T>
+static int try_coarse_p2p(const Lvl<T>& L, int nsweeps, cudaStream_t s, int* rc) {
+  switch (L.n) {
+    case 6: *rc = launch_coarse_p2p<T, 6, 1>(L, nsweeps, s); return 1;
+    case 8: *rc = launch_coarse_p2p<T, 8, 1>(L, nsweeps, s); return 1;
+    case 10: *rc = launch_coarse_p2p<T, 10, 2>(L, nsweeps, s); return 1;
+    case 12: *rc = launch_coarse_p2p<T, 12, 2>(L, nsweeps, s); return 1;
+    case 14: *rc = launch_coarse_p2p<T, 14, 2>(L, nsweeps, s); return 1;
+    case 16: *rc = launch_coarse_p2p<T, 16, 2>(L, nsweeps, s); return 1;
+    case 20: *rc = launch_coarse_p2p<T, 20, 4>(L, nsweeps, s); return 1;
+    case 24: *rc = launch_coarse_p2p<T, 24, 3>(L, nsweeps, s); return 1;
+    case 28: *rc = launch_coarse_p2p<T, 28, 4>(L, nsweeps, s); return 1;
+    case 32: *rc = launch_coarse_p2p<T, 32, 4>(L, nsweeps, s); return 1;
+    default: return 0;
+  }
+}
+
+// coarse strategy: 0 = one CTA (k_coarse_cols), 1 = cluster with a cluster
+// barrier per half-sweep (k_coarse_cluster), 2 = cluster with point-to-point
+// halo pushes (k_coarse_p2p).  Chosen per level size and precision from a
+// table that the autotuner (warpflow/autotune.py) can overwrite through
+// wf_set_coarse_strategy; WF_COARSE forces one strategy for every size.
+// Defaults measured on B200 (ns per half-sweep, FP64, 300-sweep relax):
+//   n:        8    12    16    20    24    32
+//   1 CTA:  133   263   407   903  1530  4090
+//   barrier 442   449   488   651   686   921
+//   p2p:    402   488   500   602   895   815
+static int g_strategy[2][65];
+static bool g_strategy_init = false;
+
+static void strategy_defaults() {
+  for (int f = 0; f < 2; ++f)
+    for (int n = 0; n <= 64; ++n) g_strategy[f][n] = n <= 16 ? 0 : (n == 24 ? 1 : 2);
+  g_strategy_init = true;
+}
+
+static int coarse_strategy(int n, bool fp32) {
+  const char* e = getenv("WF_COARSE");
+  if (e && e[0] >= '0' && e[0] <= '2') return e[0] - '0';
+  if (!g_strategy_init) strategy_defaults();
+  return (n >= 0 && n <= 64) ? g_strategy[fp32 ? 1 : 0][n] : 2;
+}
+
+int set_coarse_strategy(int n, int fp32, int strategy) {
+  if (n < 0 || n > 64 || strategy < 0 || strategy > 2)
+    return fail(WF_EINVAL, "wf_set_coarse_strategy: n in 0..64, strategy in 0..2");
+  if (!g_strategy_init) strategy_defaults();
+  g_strategy[fp32 ? 1 : 0][n] = strategy;
+  return WF_OK;
 }
 
 template <class T>
@@ -596,8 +873,9 @@ static int relax(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
   // small levels with many sweeps: the column kernel
   if (nsweeps > 12 || L.n <= 12) {
     int rc = WF_OK;
-    if (nsweeps > 12 && coarse_strategy() == 1 && try_coarse_cluster<T>(L, nsweeps, s, &rc))
-      return rc;
+    const int strat = coarse_strategy(L.n, sizeof(T) == 4);
+    if (nsweeps > 12 && strat == 2 && try_coarse_p2p<T>(L, nsweeps, s, &rc)) return rc;
+    if (nsweeps > 12 && strat == 1 && try_coarse_cluster<T>(L, nsweeps, s, &rc)) return rc;
     if (try_coarse<T>(L, nsweeps, s, &rc)) return rc;
   }
   const size_t sb = smem_bytes<T>(L.n);
@@ -660,6 +938,7 @@ static int build_levels(const wf_case& c, T* phi0, const T* rhs0, long sI, long 
     L.ay = (T)(1.0 / (dyl * dyl));
     L.az = (T)(1.0 / (dzl * dzl));
     L.n = c.n >> l;
+    L.err = c.sc ? &c.sc->status : nullptr;
     if ((L.n << l) != c.n || L.n < 1)
       return fail(WF_EINVAL, "n must be divisible by 2^(nlev-1)");
     if (l == 0) {
@@ -737,6 +1016,7 @@ static int build_levels_f32(const wf_case& c, std::vector<Lvl<float>>& lv) {
     L.ay = (float)(1.0 / (dyl * dyl));
     L.az = (float)(1.0 / (dzl * dzl));
     L.n = c.n >> l;
+    L.err = c.sc ? &c.sc->status : nullptr;
     L.phi = (float*)c.mg_phi[l];
     L.rhs = (const float*)c.mg_rhs[l];
     L.sJ = L.n + 2;
@@ -767,6 +1047,7 @@ static Lvl<double> level0_view(const wf_case& c, double* phi, const double* rhs,
   L.n = c.n;
   L.sI = sI;
   L.sJ = sJ;
+  L.err = c.sc ? &c.sc->status : nullptr;
   L.ax = 1.0 / (c.dx * c.dx);
   L.ay = 1.0 / (c.dy * c.dy);
   L.az = 1.0 / (c.dz * c.dz);
@@ -950,6 +1231,7 @@ int mg_solve_noalloc(const double* su, double* pp, int n, int nlev, double dx, d
     const double s2 = (double)(1 << l);
     const double dxl = dx * s2, dyl = dy * s2, dzl = dz * s2;
     Lvl<double>& L = lv[l];
+    L.err = nullptr;
     L.ax = 1.0 / (dxl * dxl);
     L.ay = 1.0 / (dyl * dyl);
     L.az = 1.0 / (dzl * dzl);

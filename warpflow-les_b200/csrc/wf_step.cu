@@ -216,6 +216,10 @@ int wf_struct_sizes(int64_t* scalars, int64_t* casebytes) {
   return WF_OK;
 }
 
+int wf_set_coarse_strategy(int32_t n, int32_t fp32, int32_t strategy) {
+  return set_coarse_strategy(n, fp32, strategy);
+}
+
 int wf_mg_level_elems(int32_t n, int32_t nlev, int32_t level, int64_t* elems) {
   if (!elems || level < 0 || level >= nlev || nlev > WF_MAX_LEVELS)
     return fail(WF_EINVAL, "wf_mg_level_elems: bad level");

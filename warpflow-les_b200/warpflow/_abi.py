@@ -80,6 +80,7 @@ SIGNATURES = {
     "wf_last_error": (ctypes.c_char_p, []),
     "wf_struct_sizes": (_I32, [ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
     "wf_scalars_init": (_I32, [_VP, _D, _VP]),
+    "wf_set_coarse_strategy": (_I32, [_I32, _I32, _I32]),
     "wf_mg_level_elems": (_I32, [_I32, _I32, _I32, ctypes.POINTER(ctypes.c_int64)]),
     "wf_init_noise": (_I32, [_VP, _VP, _VP, _I32, _D, _I32, _VP]),
     "wf_fill_initial": (_I32, [_CP, _VP]),

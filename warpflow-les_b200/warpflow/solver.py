@@ -190,6 +190,9 @@ class FlowSolver:
         if st == _abi.ST_DIVERGED:
             raise RuntimeError("projection diverged: rmax = %.6e at itime %d"
                                % (self.rmax, self.itime))
+        if st == _abi.ST_WAIT_TIMEOUT:
+            raise RuntimeError("device-side wait timed out in the multigrid coarse solve "
+                               "(itime %d); results of this step are invalid" % self.itime)
         if st == _abi.ST_NOT_CONVERGED:
             if self.topo.rank == 0:
                 print("warning: projection did not converge, rmax = %.6e after %d "
