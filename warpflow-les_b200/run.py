@@ -1,0 +1,66 @@
+"""Command-line driver (reference run.py:20-65, same flags and log lines).
+
+    python warpflow-les_b200/run.py --case case.yaml [--device auto|cuda:0]
+                                    [--steps N] [--outdir D] [--resume SNAP]
+
+Runs `time.n_steps` (or --steps) FlowSolver steps, prints the reference's
+log line every `output.log_interval` steps and writes a snapshot every
+`output.n_out` steps and at the end.  --resume continues from a snapshot
+written by this build.
+"""
+import argparse
+import os
+import sys
+import time
+
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+
+from warpflow import FlowSolver, __version__, build_topology, load_case  # noqa: E402
+from warpflow.io import read_snapshot, restore, write_snapshot  # noqa: E402
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description="warpflow-les solver (B200 build)")
+    ap.add_argument("--case", required=True, help="case YAML file")
+    ap.add_argument("--device", default="auto", help="auto | cuda:N (no CPU path)")
+    ap.add_argument("--steps", type=int, default=None,
+                    help="override time.n_steps from the case file")
+    ap.add_argument("--outdir", default=None, help="override output.outdir")
+    ap.add_argument("--resume", default=None, help="snapshot .npz to continue from")
+    args = ap.parse_args(argv)
+
+    cfg = load_case(args.case)
+    if args.outdir:
+        cfg.output.outdir = args.outdir
+    nsteps = args.steps if args.steps is not None else cfg.time.n_steps
+    topo = build_topology(cfg)
+    device = "cuda:0" if args.device == "auto" else args.device
+    if topo.rank == 0:
+        print("warpflow-les %s: case=%s grid=%dx%dx%d domains=%s device=%s"
+              % (__version__, cfg.name, cfg.grid.nx, cfg.grid.ny, cfg.grid.nz,
+                 list(cfg.mpi.domains), device), flush=True)
+    sol = FlowSolver(cfg, topo, device=device)
+    start = 0
+    if args.resume:
+        restore(sol, read_snapshot(args.resume))
+        start = sol.itime
+    t0 = time.time()
+    for itime in range(start + 1, start + nsteps + 1):
+        info = sol.step()
+        if itime % cfg.output.log_interval == 0 and topo.rank == 0:
+            print("it %6d  ctime %.6f  dt %.3e  rmax %.3e  outer %2d  cfl %.2f"
+                  % (itime, info["ctime"], info["dt"], info["rmax"], info["iters"],
+                     info["cfl"]), flush=True)
+        if itime % cfg.output.n_out == 0:
+            write_snapshot(sol, itime)
+    last = start + nsteps
+    if last % cfg.output.n_out != 0:
+        write_snapshot(sol, last)
+    if topo.rank == 0:
+        print("done: itime=%d ctime=%.6f wall=%.1fs" % (last, sol.ctime, time.time() - t0),
+              flush=True)
+    sol.close()
+
+
+if __name__ == "__main__":
+    main()

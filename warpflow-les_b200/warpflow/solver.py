@@ -140,6 +140,14 @@ class FlowSolver:
         self._ctime = float(value)
         self._push_scalar("ctime", self._ctime)
 
+    def set_time_state(self, dt, ctime, itime):
+        """Set dt, ctime and itime on the device and the host (resume)."""
+        sc = self._pull_scalars()
+        sc.dt, sc.ctime, sc.itime = float(dt), float(ctime), int(itime)
+        self._sc.copy_(self._sc_host, non_blocking=True)
+        torch.cuda.current_stream(self.device).synchronize()
+        self._dt, self._ctime, self.itime = float(dt), float(ctime), int(itime)
+
     # ------------------------------------------------------------------ #
     def fill_bc(self, name, alfabc=0):
         """One boundu/boundv/boundw call (reference solver.py:88-97)."""
