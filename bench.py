@@ -169,7 +169,7 @@ def _events():
 
 
 def bench_ensemble(args):
-    """Config 3: 64 seeded cavity cases (N in {32..96}, Re in [100, 1000], lid
+    """Ensemble: 64 seeded cavity cases (N in {32..96}, Re in [100, 1000], lid
     in [0.5, 1.5]), mixed-precision multigrid, advanced together; compared
     with the plain FP64 per-case loop (one case after another) on the same
     cases."""
@@ -212,7 +212,7 @@ def bench_ensemble(args):
 
 
 def bench_serve(args):
-    """Config 4: a seeded Poisson request stream (20 req/s, N in {32..128},
+    """Serving: a seeded Poisson request stream (20 req/s, N in {32..128},
     Re in [100, 1000], steps in [100, 2000] scaled by --step-scale) served
     with continuous batching under a 150 GB budget."""
     from warpflow.serve import CavityServer, poisson_stream
@@ -233,7 +233,7 @@ def bench_serve(args):
 
 
 def bench_poisson(args):
-    """Config 2: standalone Poisson solve on 256^3 with 5 levels, RHS
+    """Standalone Poisson solve on 256^3 with 5 levels, RHS
     N(0,1) on the 258^3 level-0 array with the ring zeroed and the mean
     removed (the reference harness tests/test_mg.py), solved to a relative
     max-norm residual of 1e-10 with FP64 V-cycles and with FP32 V-cycles in

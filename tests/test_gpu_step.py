@@ -67,7 +67,7 @@ def _compare_run(cfg, nsteps, check_every=1):
 
 
 def test_one_step_1e10_at_32():
-    """configs[0] geometry, first step: every field within 1e-10."""
+    """The 32^3 fixed-dt cavity, first step: every field within 1e-10."""
     cfg = make_cfg(n=32, levels=3, vdt=False)
     sol = _solver(cfg)
     ora = O.OracleSolver(cfg)

@@ -9,8 +9,9 @@ concurrently -- a small case's latency-bound coarse solve overlaps with a
 large case's bandwidth-bound sweeps -- then gathers all scalar blocks with
 one device-to-host copy.
 
-The ensemble of BASELINE config 3 (64 cases, N in {32,...,96}, Re in
-[100, 1000], lid velocity in [0.5, 1.5]) is built by ``random_ensemble``.
+The 64-case benchmark ensemble (N in {32, 48, 64, 80, 96}, Re in
+[100, 1000], lid velocity in [0.5, 1.5], seeded) is built by
+``random_ensemble``.
 """
 from __future__ import annotations
 
