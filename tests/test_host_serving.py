@@ -70,10 +70,11 @@ def test_case_bytes_formula():
     from warpflow.serve import case_bytes
     n = 80
     f = 13 * 86 ** 3 * 8
-    mg64 = 2 * 8 * (82 ** 3 + 42 ** 3 + 22 ** 3)
-    mg32 = 2 * 4 * (82 ** 3 + 42 ** 3 + 22 ** 3)
+    vol = 82 ** 3 + 42 ** 3 + 22 ** 3
+    mg64 = 2 * 8 * vol + 8 * vol          # phi, rhs + sweep buffer
+    mg32 = 2 * 4 * vol + 4 * vol
     assert case_bytes(n, 3, "fp64") - f - mg64 < 4096
-    assert case_bytes(n, 3, "mixed") - f - mg64 - mg32 < 4096
+    assert case_bytes(n, 3, "mixed") - f - 2 * 8 * vol - mg32 < 4096
 
 
 def test_shard_round_robin():

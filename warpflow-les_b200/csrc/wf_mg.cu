@@ -40,6 +40,8 @@ struct Lvl {
   long sI, sJ;   // strides (k stride 1)
   T ax, ay, az;  // 1/h^2 per axis of this level
   int* err;      // where a device-side wait records a timeout (may be null)
+  T* tmp;        // second buffer for one-launch sweeps (may be null)
+  long tI, tJ;   // its strides
 };
 
 template <class T>
@@ -819,6 +821,187 @@ static int try_coarse_cluster(const Lvl<T>& L, int nsweeps, cudaStream_t s, int*
   }
 }
 
+// ---- one whole red-black sweep per launch (fine levels) -------------------
+// Red values depend only on the old black values, so a sweep can run as one
+// launch if every CTA reads the old state from `src` and writes the new
+// state to a different buffer `dst` (the two buffers alternate over the
+// sweeps of a relax; an even sweep count ends in the level's own array).
+// A CTA owns a TJ x TK tile of (j,k) columns and a segment of i-planes and
+// marches along i with a 4-plane window in shared memory covering the tile
+// plus a 2-cell halo: at plane p it computes red on the tile plus a 1-cell
+// halo (the halo redundantly, from old black values), then black on plane
+// p-1 of the tile, and stores both colours of plane p-1.  Red is also
+// computed redundantly on the plane before and after the segment.  Every
+// cell keeps the reference's arithmetic (same terms, same order, division by
+// ap), so results equal the one-colour-per-launch kernel bit for bit.  The
+// face-ring mirrors are written on the last sweep of a relax only; no sweep
+// reads the ring (its coefficients are zero).
+template <int TJ, int TK>
+struct SweepTile {
+  static constexpr int WJ = TJ + 4, WK = TK + 4;
+  static constexpr int PLANE = WJ * WK;
+  static constexpr int THREADS = 320;
+};
+
+template <class T, int TJ, int TK>
+__global__ void __launch_bounds__(SweepTile<TJ, TK>::THREADS)
+    k_sweep2(const T* __restrict__ src, long sIs, long sJs, T* __restrict__ dst, long sId,
+             long sJd, const T* __restrict__ rhs, long sIr, long sJr, int n, T ax, T ay,
+             T az, int seg, int write_ring) {
+  using W = SweepTile<TJ, TK>;
+  constexpr int WK = W::WK, PLANE = W::PLANE, NT = W::THREADS;
+  constexpr int PER = (PLANE + NT - 1) / NT;  // window elements per thread
+  __shared__ T win[4][PLANE];
+  __shared__ T rb[2][PLANE];
+  const int ntk = (n + TK - 1) / TK;
+  const int j0 = (blockIdx.x / ntk) * TJ;
+  const int k0 = (blockIdx.x % ntk) * TK;
+  const int i0 = blockIdx.y * seg;
+  const int i1 = min(n, i0 + seg);
+  const int tid = threadIdx.x;
+  // this thread's window elements: offsets into a plane of src / rhs
+  long offs[PER], roff[PER];
+  bool okp[PER], okr[PER];
+#pragma unroll
+  for (int e = 0; e < PER; ++e) {
+    const int t = tid + e * NT;
+    const int jj = t / WK, kk = t - jj * WK;
+    const int j = j0 - 2 + jj, k = k0 - 2 + kk;
+    okp[e] = t < PLANE && j >= -1 && j <= n && k >= -1 && k <= n;
+    okr[e] = t < PLANE && j >= 0 && j < n && k >= 0 && k < n;
+    offs[e] = okp[e] ? (long)(j + 1) * sJs + (k + 1) : 0;
+    roff[e] = okr[e] ? (long)(j + 1) * sJr + (k + 1) : 0;
+  }
+  T pf[PER], rf[PER];  // prefetched plane values (phi of plane q, rhs of plane q-1)
+  auto fetch = [&](int q) {
+#pragma unroll
+    for (int e = 0; e < PER; ++e) {
+      pf[e] = (okp[e] && q <= n) ? src[(long)(q + 1) * sIs + offs[e]] : T(0);
+      rf[e] = (okr[e] && q - 1 >= 0 && q - 1 < n) ? rhs[(long)q * sIr + roff[e]] : T(0);
+    }
+  };
+  auto deposit = [&](int q) {
+    T* w = win[(q + 4) & 3];
+    T* r = rb[(q + 3) & 1];
+#pragma unroll
+    for (int e = 0; e < PER; ++e) {
+      const int t = tid + e * NT;
+      if (t < PLANE) {
+        w[t] = pf[e];
+        r[t] = rf[e];
+      }
+    }
+  };
+  // loop invariant at plane p: the window holds planes p-2, p-1, p (and the
+  // rhs of p-1); plane p+1 with the rhs of p sits in registers
+  if (i0 - 2 >= -1) {
+    fetch(i0 - 2);
+    deposit(i0 - 2);
+  }
+  fetch(i0 - 1);
+  deposit(i0 - 1);
+  fetch(i0);
+  for (int p = i0 - 1; p <= i1; ++p) {
+    __syncthreads();  // previous plane's reads of the slots about to change are done
+    deposit(p + 1);   // plane p+1 and rhs of plane p
+    __syncthreads();
+    if (p + 2 <= i1 + 1) fetch(p + 2);  // in flight during this plane's compute
+    // red on plane p over the tile plus a one-cell halo (real cells only)
+    if (p >= 0 && p < n) {
+      T* wc = win[(p + 4) & 3];
+      const T* wm = win[(p + 3) & 3];
+      const T* wp = win[(p + 5) & 3];
+      const T* rr = rb[p & 1];
+      constexpr int RJ = TJ + 2, RK = (TK + 2) / 2;
+      for (int t = tid; t < RJ * RK; t += NT) {
+        const int a = t / RK, b = t - a * RK;
+        const int j = j0 - 1 + a;
+        int k = k0 - 1 + 2 * b;
+        if (((p + j + k) & 1) == 0) ++k;  // the odd (red) cell of the pair
+        if (j < 0 || j >= n || k < 0 || k >= n || k > k0 + TK) continue;
+        const int c = (j - j0 + 2) * WK + (k - k0 + 2);
+        const T aw = p > 0 ? ax : T(0), ae = p < n - 1 ? ax : T(0);
+        const T as = j > 0 ? ay : T(0), an = j < n - 1 ? ay : T(0);
+        const T ab = k > 0 ? az : T(0), at = k < n - 1 ? az : T(0);
+        const T ap = -(aw + ae + as + an + ab + at);
+        const T sum = aw * wm[c] + ae * wp[c] + as * wc[c - WK] + an * wc[c + WK] +
+                      ab * wc[c - 1] + at * wc[c + 1];
+        wc[c] = (rr[c] - sum) / ap;
+      }
+    }
+    __syncthreads();
+    // black on plane q = p-1 of the tile, then store both colours of q
+    const int q = p - 1;
+    if (q >= i0 && q < i1) {
+      T* wc = win[(q + 4) & 3];
+      const T* wm = win[(q + 3) & 3];
+      const T* wp = win[(q + 5) & 3];
+      const T* rr = rb[q & 1];
+      constexpr int BK = TK / 2;
+      for (int t = tid; t < TJ * BK; t += NT) {
+        const int a = t / BK, b = t - a * BK;
+        const int j = j0 + a;
+        const int kr = k0 + 2 * b;
+        if (j >= n || kr >= n) continue;
+        int k = kr;
+        if (((q + j + k) & 1) == 1) ++k;  // the even (black) cell of the pair
+        const int ck = (j - j0 + 2) * WK;
+        if (k < n) {
+          const int c = ck + (k - k0 + 2);
+          const T aw = q > 0 ? ax : T(0), ae = q < n - 1 ? ax : T(0);
+          const T as = j > 0 ? ay : T(0), an = j < n - 1 ? ay : T(0);
+          const T ab = k > 0 ? az : T(0), at = k < n - 1 ? az : T(0);
+          const T ap = -(aw + ae + as + an + ab + at);
+          const T sum = aw * wm[c] + ae * wp[c] + as * wc[c - WK] + an * wc[c + WK] +
+                        ab * wc[c - 1] + at * wc[c + 1];
+          wc[c] = (rr[c] - sum) / ap;
+        }
+        for (int kk = kr; kk < kr + 2 && kk < n; ++kk) {
+          const T x = wc[ck + (kk - k0 + 2)];
+          const long o = (long)(q + 1) * sId + (long)(j + 1) * sJd + (kk + 1);
+          dst[o] = x;
+          if (write_ring) {
+            if (q == 0) dst[o - sId] = x;
+            if (q == n - 1) dst[o + sId] = x;
+            if (j == 0) dst[o - sJd] = x;
+            if (j == n - 1) dst[o + sJd] = x;
+            if (kk == 0) dst[o - 1] = x;
+            if (kk == n - 1) dst[o + 1] = x;
+          }
+        }
+      }
+    }
+  }
+}
+
+constexpr int SWEEP_TJ = 16, SWEEP_TK = 32;
+
+// smallest level edge that uses one-launch sweeps (WF_SWEEP2_MIN overrides)
+static int sweep2_min_n() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("WF_SWEEP2_MIN");
+    v = e ? atoi(e) : 128;
+  }
+  return v;
+}
+
+template <class T>
+static int launch_sweep2(const T* src, long sIs, long sJs, T* dst, long sId, long sJd,
+                         const Lvl<T>& L, int write_ring, cudaStream_t s) {
+  const int n = L.n;
+  const int ntj = (n + SWEEP_TJ - 1) / SWEEP_TJ, ntk = (n + SWEEP_TK - 1) / SWEEP_TK;
+  // at least ~2 CTAs per SM, segments of 4 to 32 planes
+  int nseg = std::max(1, (2 * 148 + ntj * ntk - 1) / (ntj * ntk));
+  int seg = std::min(32, std::max(4, (n + nseg - 1) / nseg));
+  nseg = (n + seg - 1) / seg;
+  k_sweep2<T, SWEEP_TJ, SWEEP_TK><<<dim3(ntj * ntk, nseg), SweepTile<SWEEP_TJ, SWEEP_TK>::THREADS,
+                                    0, s>>>(src, sIs, sJs, dst, sId, sJd, L.rhs, L.sI, L.sJ, n,
+                                            L.ax, L.ay, L.az, seg, write_ring);
+  WF_CKL("k_sweep2");
+  return WF_OK;
+}
+
 // max |rhs - A phi| over a level (tests/test_mg.py:16-32)
 __global__ void k_resmax(const Lvl<double> L, double* out, unsigned int* ticket,
                          unsigned long long* acc) {
@@ -877,6 +1060,24 @@ static int relax(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
     if (nsweeps > 12 && strat == 2 && try_coarse_p2p<T>(L, nsweeps, s, &rc)) return rc;
     if (nsweeps > 12 && strat == 1 && try_coarse_cluster<T>(L, nsweeps, s, &rc)) return rc;
     if (try_coarse<T>(L, nsweeps, s, &rc)) return rc;
+  }
+  if (L.tmp && nsweeps >= 2 && L.n >= sweep2_min_n()) {
+    // pairs of one-launch sweeps: phi -> tmp -> phi
+    const int pairs = nsweeps / 2;
+    for (int p = 0; p < pairs; ++p) {
+      WF_TRY(launch_sweep2<T>(L.phi, L.sI, L.sJ, L.tmp, L.tI, L.tJ, L, 0, s));
+      const int ring = (p == pairs - 1 && (nsweeps & 1) == 0) ? 1 : 0;
+      WF_TRY(launch_sweep2<T>(L.tmp, L.tI, L.tJ, L.phi, L.sI, L.sJ, L, ring, s));
+    }
+    if (nsweeps & 1) {
+      const long half = (long)L.n * L.n * ((L.n + 1) / 2);
+      const int nb = mg_blocks(half);
+      k_rbgs<T><<<nb, MG_TPB, 0, s>>>(L, 0);
+      WF_CKL("k_rbgs");
+      k_rbgs<T><<<nb, MG_TPB, 0, s>>>(L, 1);
+      WF_CKL("k_rbgs");
+    }
+    return WF_OK;
   }
   const size_t sb = smem_bytes<T>(L.n);
   if (sb <= SMEM_CAP) {
@@ -939,6 +1140,9 @@ static int build_levels(const wf_case& c, T* phi0, const T* rhs0, long sI, long 
     L.az = (T)(1.0 / (dzl * dzl));
     L.n = c.n >> l;
     L.err = c.sc ? &c.sc->status : nullptr;
+    L.tmp = (T*)c.mg_tmp[l];
+    L.tJ = L.n + 2;
+    L.tI = (long)(L.n + 2) * (L.n + 2);
     if ((L.n << l) != c.n || L.n < 1)
       return fail(WF_EINVAL, "n must be divisible by 2^(nlev-1)");
     if (l == 0) {
@@ -1017,6 +1221,9 @@ static int build_levels_f32(const wf_case& c, std::vector<Lvl<float>>& lv) {
     L.az = (float)(1.0 / (dzl * dzl));
     L.n = c.n >> l;
     L.err = c.sc ? &c.sc->status : nullptr;
+    L.tmp = (float*)c.mg_tmp[l];
+    L.tJ = L.n + 2;
+    L.tI = (long)(L.n + 2) * (L.n + 2);
     L.phi = (float*)c.mg_phi[l];
     L.rhs = (const float*)c.mg_rhs[l];
     L.sJ = L.n + 2;
@@ -1048,6 +1255,7 @@ static Lvl<double> level0_view(const wf_case& c, double* phi, const double* rhs,
   L.sI = sI;
   L.sJ = sJ;
   L.err = c.sc ? &c.sc->status : nullptr;
+  L.tmp = nullptr;
   L.ax = 1.0 / (c.dx * c.dx);
   L.ay = 1.0 / (c.dy * c.dy);
   L.az = 1.0 / (c.dz * c.dz);
@@ -1232,6 +1440,7 @@ int mg_solve_noalloc(const double* su, double* pp, int n, int nlev, double dx, d
     const double dxl = dx * s2, dyl = dy * s2, dzl = dz * s2;
     Lvl<double>& L = lv[l];
     L.err = nullptr;
+    L.tmp = nullptr;
     L.ax = 1.0 / (dxl * dxl);
     L.ay = 1.0 / (dyl * dyl);
     L.az = 1.0 / (dzl * dzl);

@@ -65,6 +65,7 @@ class WfCase(ctypes.Structure):
         ("fld", ctypes.c_void_p * NFIELDS),
         ("mg_phi", ctypes.c_void_p * MAX_LEVELS),
         ("mg_rhs", ctypes.c_void_p * MAX_LEVELS),
+        ("mg_tmp", ctypes.c_void_p * MAX_LEVELS),
         ("sc", ctypes.c_void_p),
     ]
 

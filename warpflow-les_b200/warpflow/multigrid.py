@@ -97,6 +97,10 @@ class Multigrid:
             for lev in self.levels:
                 self._f32.append((DeviceField.zeros(lev.shape, self.device, torch.float32),
                                   DeviceField.zeros(lev.shape, self.device, torch.float32)))
+        # second buffer per level: a whole red-black sweep becomes one launch
+        dt = torch.float32 if self.precision == "mixed" else torch.float64
+        self._tmp = [DeviceField.zeros(lev.shape, self.device, dt) for lev in self.levels]
+        self._tmp64 = self._tmp if dt == torch.float64 else None
         self.n_pre = 6       # multigrid.py:257-260
         self.n_post = 6
         self.n_coarse = 300
@@ -125,10 +129,15 @@ class Multigrid:
             for l, (phi32, rhs32) in enumerate(self._f32):
                 c.mg_phi[l] = phi32.ptr
                 c.mg_rhs[l] = rhs32.ptr
+                c.mg_tmp[l] = self._tmp[l].ptr
         else:
             for l in range(1, len(levels)):
                 c.mg_phi[l] = levels[l].phi.ptr
                 c.mg_rhs[l] = levels[l].rhs.ptr
+            if self._tmp64 is not None:
+                for l, lev in enumerate(levels):
+                    if lev in self.levels:
+                        c.mg_tmp[l] = self._tmp64[self.levels.index(lev)].ptr
         if su is not None:
             c.fld[_abi.FIELD_NAMES.index("su")] = su.ptr
         if pp is not None:

@@ -35,15 +35,18 @@ NFIELDS = 13
 def case_bytes(n, levels=3, precision="mixed"):
     """Device bytes a FlowSolver of an n^3 case allocates: 13 padded FP64
     fields, FP64 multigrid levels (phi, rhs with one ring, level 0
-    included), the FP32 copies of every level in mixed precision, and two
-    scalar blocks plus one residual slot."""
+    included), the FP32 copies of every level in mixed precision, one sweep
+    buffer per level in the multigrid's precision, and two scalar blocks
+    plus one residual slot."""
     fields = NFIELDS * (n + 6) ** 3 * 8
     mg = 0
     for l in range(levels):
         m = (n >> l) + 2
         mg += 2 * m ** 3 * 8
         if precision == "mixed":
-            mg += 2 * m ** 3 * 4
+            mg += 2 * m ** 3 * 4 + m ** 3 * 4
+        else:
+            mg += m ** 3 * 8
     return fields + mg + 2 * ctypes.sizeof(_abi.WfScalars) + 8
 
 

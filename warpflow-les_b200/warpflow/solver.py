@@ -218,6 +218,7 @@ class FlowSolver:
             ts += [lev.phi.t, lev.rhs.t]
         for a, b in self.mg._f32:
             ts += [a.t, b.t]
+        ts += [t.t for t in self.mg._tmp]
         ts += [self.mg._sc, self.mg._out]
         return int(sum(t.numel() * t.element_size() for t in ts))
 
