@@ -81,6 +81,7 @@ typedef struct wf_scalars {
   int32_t loop;       /* device loop flag of the projection */
   uint32_t ticket;    /* last-block-done counter */
   int32_t nmg;        /* multigrid solves run in the last step */
+  uint32_t gbar[2];   /* grid barrier of the persistent relax (count, generation) */
 } wf_scalars;
 
 /* One cavity case: geometry, physics, numerics and the caller's buffers. */

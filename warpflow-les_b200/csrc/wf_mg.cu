@@ -42,6 +42,7 @@ struct Lvl {
   int* err;      // where a device-side wait records a timeout (may be null)
   T* tmp;        // second buffer for one-launch sweeps (may be null)
   long tI, tJ;   // its strides
+  unsigned* gbar;  // two words of grid-barrier state (may be null)
 };
 
 template <class T>
@@ -770,6 +771,224 @@ static int try_coarse_p2p(const Lvl<T>& L, int nsweeps, cudaStream_t s, int* rc)
   }
 }
 
+// ---- temporal blocking: one exchange per full sweep ----------------------
+// As k_coarse_p2p, but each CTA also keeps two halo planes on each side, so
+// it can run a whole sweep locally: red on its slab plus one plane on each
+// side (the extra planes redundantly, from the neighbours' values of the
+// previous sweep), then black on its slab.  Only then do the slab's two
+// outer planes (both colours) go to the neighbours, into a staging buffer
+// that alternates between sweeps so that a sender one sweep ahead never
+// overwrites values still being read; the receiver copies them into its
+// halo planes before the next sweep.  Half as many exchanges as k_coarse_p2p
+// for 25 % more red work.
+template <int NC, int NCL>
+struct TbShape {
+  static constexpr int C = NC / NCL;
+  static constexpr int H = NC / 2;
+  static constexpr int NLP = NCL + 4;          // local planes incl. halos
+  static constexpr int HALF = NLP * H;         // columns per parity
+  static constexpr int GROUP = ((HALF + 31) / 32) * 32;
+  static constexpr int THREADS = 2 * GROUP;
+  static constexpr int PL = NLP * H;           // one parity, one k
+  static constexpr int SIDE = 2 * NC * NC;     // staged values per side
+};
+
+template <class T, int NC, int NCL>
+__global__ void __launch_bounds__(TbShape<NC, NCL>::THREADS)
+    k_coarse_tb(Lvl<T> L, int nsweeps, int wmode) {
+  using S = TbShape<NC, NCL>;
+  constexpr int H = S::H, HALF = S::HALF, GROUP = S::GROUP, PL = S::PL, C = S::C;
+  constexpr int SIDE = S::SIDE;
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  extern __shared__ __align__(16) unsigned char smraw[];
+  __shared__ __align__(8) unsigned long long mbar[2];
+  __shared__ int s_bail;
+  T* sp = reinterpret_cast<T*>(smraw);
+  T* stage = sp + 2 * NC * PL;  // [buf 2][side 2 (0 = from rank-1, 1 = from rank+1)][SIDE]
+  const int tid = threadIdx.x;
+  const uint32_t mb[2] = {smem_u32(&mbar[0]), smem_u32(&mbar[1])};
+  if (tid == 0) {
+    mbar_init(mb[0], 1);
+    mbar_init(mb[1], 1);
+    s_bail = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  for (int t = tid; t < 2 * NC * PL; t += blockDim.x) sp[t] = T(0);
+  const int g = tid / GROUP;
+  const int q = tid - g * GROUP;
+  const bool slot = q < HALF;
+  const int il = slot ? q / H : 0;                 // local plane 0 .. NCL+3
+  const int m = slot ? q - il * H : 0;
+  const int i = rank * NCL - 2 + il;               // global plane (may be outside)
+  const bool active = slot && i >= 0 && i < NC;
+  const int j = 2 * m + ((i + g) & 1);
+  T* own = sp + g * NC * PL;
+  const T* oth = sp + (1 - g) * NC * PL;
+  const int me = il * H + m;
+  const int oW = il > 0 ? me - H : me, oE = il < S::NLP - 1 ? me + H : me;
+  const int oS = j > 0 ? il * H + ((j - 1) >> 1) : me;
+  const int oN = j < NC - 1 ? il * H + ((j + 1) >> 1) : me;
+  const T aw = i > 0 ? L.ax : T(0), ae = i < NC - 1 ? L.ax : T(0);
+  const T as = j > 0 ? L.ay : T(0), an = j < NC - 1 ? L.ay : T(0);
+  const T az = L.az;
+  const T inv_in = T(1) / (-(aw + ae + as + an + az + az));
+  const T inv_lo = T(1) / (-(aw + ae + as + an + T(0) + az));
+  const T inv_hi = T(1) / (-(aw + ae + as + an + az + T(0)));
+  const int olo = rank * NCL, ohi = olo + NCL;      // owned planes [olo, ohi)
+  const bool do_red = active && i >= olo - 1 && i < ohi + 1;
+  const bool do_black = active && i >= olo && i < ohi;
+  const bool halo_lo = active && i < olo;           // filled from rank-1
+  const bool halo_hi = active && i >= ohi;          // filled from rank+1
+  // my column goes to a neighbour when it is one of my two outer planes
+  const bool sendW = active && rank > 0 && i >= olo && i < olo + 2;
+  const bool sendE = active && rank < C - 1 && i >= ohi - 2 && i < ohi;
+  uint32_t aW[2] = {0, 0}, aE[2] = {0, 0}, mW[2] = {0, 0}, mE[2] = {0, 0};
+  const uint32_t st_u32 = smem_u32(stage);
+  if (sendW) {  // rank-1 stores me as side 1 (from its right), plane i - olo
+    const int pw = i - olo;
+    for (int b = 0; b < 2; ++b) {
+      aW[b] = mapa_u32(st_u32 + (uint32_t)(((b * 2 + 1) * SIDE + (pw * NC + j) * NC) * sizeof(T)),
+                       rank - 1);
+      mW[b] = mapa_u32(mb[b], rank - 1);
+    }
+  }
+  if (sendE) {  // rank+1 stores me as side 0 (from its left), plane i - (ohi - 2)
+    const int pe = i - (ohi - 2);
+    for (int b = 0; b < 2; ++b) {
+      aE[b] = mapa_u32(st_u32 + (uint32_t)(((b * 2 + 0) * SIDE + (pe * NC + j) * NC) * sizeof(T)),
+                       rank + 1);
+      mE[b] = mapa_u32(mb[b], rank + 1);
+    }
+  }
+  // where a halo column of mine finds its staged values
+  const int hside = halo_lo ? 0 : 1;
+  const int hplane = halo_lo ? i - (olo - 2) : i - ohi;
+  const int hoff = hside * SIDE + (hplane * NC + j) * NC;
+  const int nbr = (rank > 0 ? 1 : 0) + (rank < C - 1 ? 1 : 0);
+  const uint32_t tx = (uint32_t)(nbr * SIDE * sizeof(T));
+  T ph[NC], rh[NC];
+  const long c0 = lid(L, (active ? i : 0) + 1, j + 1, 1);
+  cl.sync();  // barriers initialised everywhere before any push
+#pragma unroll
+  for (int k = 0; k < NC; ++k) {
+    ph[k] = active ? L.phi[c0 + k] : T(0);
+    rh[k] = active ? L.rhs[c0 + k] : T(0);
+    if (slot) own[k * PL + me] = ph[k];
+  }
+  // data of sweep s (s < nsweeps-1) lands in staging buffer s&1
+  if (tid == 0) {
+    if (nsweeps > 1) mbar_arrive_expect_tx(mb[0], tx);
+    if (nsweeps > 2) mbar_arrive_expect_tx(mb[1], tx);
+  }
+  __syncthreads();
+  bool bailed = false;
+  for (int sw = 0; sw < nsweeps; ++sw) {
+    if (sw > 0) {
+      const int b = (sw - 1) & 1;
+      const uint32_t par = (uint32_t)(((sw - 1) >> 1) & 1);
+      bool ok = false;
+      for (int it = 0; it < MBAR_WAIT_TRIES && !ok; ++it) ok = mbar_try_wait(mb[b], par, wmode);
+      if (!ok) s_bail = 1;
+      if (tid == 0 && sw + 1 < nsweeps - 1) mbar_arrive_expect_tx(mb[b], tx);
+      if (ok && (halo_lo || halo_hi)) {
+        const T* src = stage + b * 2 * SIDE + hoff;
+#pragma unroll
+        for (int k = 0; k < NC; ++k) {
+          ph[k] = src[k];
+          own[k * PL + me] = ph[k];
+        }
+      }
+    }
+    __syncthreads();
+    if (s_bail) {
+      bailed = true;
+      break;
+    }
+    // red: colour 0, cells with (i+j+k) odd  <=>  k parity (1 + g) & 1
+    if (do_red) {
+      if (((1 + g) & 1) == 0)
+        half_sweep_cols<T, NC, 0, false>(oth, own, PL, me, oW, oE, oS, oN, aw, ae, as, an, az,
+                                         inv_in, inv_lo, inv_hi, ph, rh, nullptr);
+      else
+        half_sweep_cols<T, NC, 1, false>(oth, own, PL, me, oW, oE, oS, oN, aw, ae, as, an, az,
+                                         inv_in, inv_lo, inv_hi, ph, rh, nullptr);
+    }
+    __syncthreads();
+    if (do_black) {
+      if ((g & 1) == 0)
+        half_sweep_cols<T, NC, 0, false>(oth, own, PL, me, oW, oE, oS, oN, aw, ae, as, an, az,
+                                         inv_in, inv_lo, inv_hi, ph, rh, nullptr);
+      else
+        half_sweep_cols<T, NC, 1, false>(oth, own, PL, me, oW, oE, oS, oN, aw, ae, as, an, az,
+                                         inv_in, inv_lo, inv_hi, ph, rh, nullptr);
+    }
+    if (sw + 1 < nsweeps) {
+      const int b = sw & 1;
+      if (sendW) {
+#pragma unroll
+        for (int k = 0; k < NC; ++k) st_async(aW[b] + (uint32_t)(k * sizeof(T)), ph[k], mW[b]);
+      }
+      if (sendE) {
+#pragma unroll
+        for (int k = 0; k < NC; ++k) st_async(aE[b] + (uint32_t)(k * sizeof(T)), ph[k], mE[b]);
+      }
+    }
+    __syncthreads();  // this sweep's reads of the halo planes are done
+  }
+  __syncthreads();
+  if (s_bail && tid == 0 && L.err) atomicExch(L.err, (int)WF_ST_WAIT_TIMEOUT);
+  cl.sync();
+  if (!do_black) return;
+#pragma unroll
+  for (int k = 0; k < NC; ++k) {
+    const long c = c0 + k;
+    L.phi[c] = ph[k];
+    if (nsweeps > 0) ring_mirror(L, i, j, k, c, ph[k]);
+  }
+  (void)bailed;
+}
+
+template <class T, int NC, int NCL>
+static int launch_coarse_tb(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
+  using S = TbShape<NC, NCL>;
+  const size_t sb = (2ull * NC * S::PL + 4ull * S::SIDE) * sizeof(T);
+  auto kern = k_coarse_tb<T, NC, NCL>;
+  WF_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(S::C, 1, 1);
+  cfg.blockDim = dim3(S::THREADS, 1, 1);
+  cfg.dynamicSmemBytes = sb;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = S::C;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  WF_CK(cudaLaunchKernelEx(&cfg, kern, L, nsweeps, 1));
+  WF_CKL("k_coarse_tb");
+  return WF_OK;
+}
+
+template <class T>
+static int try_coarse_tb(const Lvl<T>& L, int nsweeps, cudaStream_t s, int* rc) {
+  switch (L.n) {
+    case 8: *rc = launch_coarse_tb<T, 8, 2>(L, nsweeps, s); return 1;
+    case 10: *rc = launch_coarse_tb<T, 10, 2>(L, nsweeps, s); return 1;
+    case 12: *rc = launch_coarse_tb<T, 12, 2>(L, nsweeps, s); return 1;
+    case 14: *rc = launch_coarse_tb<T, 14, 2>(L, nsweeps, s); return 1;
+    case 16: *rc = launch_coarse_tb<T, 16, 2>(L, nsweeps, s); return 1;
+    case 20: *rc = launch_coarse_tb<T, 20, 4>(L, nsweeps, s); return 1;
+    case 24: *rc = launch_coarse_tb<T, 24, 3>(L, nsweeps, s); return 1;
+    case 28: *rc = launch_coarse_tb<T, 28, 4>(L, nsweeps, s); return 1;
+    case 32: *rc = launch_coarse_tb<T, 32, 4>(L, nsweeps, s); return 1;
+    default: return 0;
+  }
+}
+
 // coarse strategy: 0 = one CTA (k_coarse_cols), 1 = cluster with a cluster
 // barrier per half-sweep (k_coarse_cluster), 2 = cluster with point-to-point
 // halo pushes (k_coarse_p2p).  Chosen per level size and precision from a
@@ -791,14 +1010,14 @@ static void strategy_defaults() {
 
 static int coarse_strategy(int n, bool fp32) {
   const char* e = getenv("WF_COARSE");
-  if (e && e[0] >= '0' && e[0] <= '2') return e[0] - '0';
+  if (e && e[0] >= '0' && e[0] <= '3') return e[0] - '0';
   if (!g_strategy_init) strategy_defaults();
   return (n >= 0 && n <= 64) ? g_strategy[fp32 ? 1 : 0][n] : 2;
 }
 
 int set_coarse_strategy(int n, int fp32, int strategy) {
-  if (n < 0 || n > 64 || strategy < 0 || strategy > 2)
-    return fail(WF_EINVAL, "wf_set_coarse_strategy: n in 0..64, strategy in 0..2");
+  if (n < 0 || n > 64 || strategy < 0 || strategy > 3)
+    return fail(WF_EINVAL, "wf_set_coarse_strategy: n in 0..64, strategy in 0..3");
   if (!g_strategy_init) strategy_defaults();
   g_strategy[fp32 ? 1 : 0][n] = strategy;
   return WF_OK;
@@ -1002,6 +1221,115 @@ static int launch_sweep2(const T* src, long sIs, long sJs, T* dst, long sId, lon
   return WF_OK;
 }
 
+// ---- a whole relax of a fine level in one cooperative launch --------------
+// The same half-sweep body as k_rbgs, all 2*nsweeps half-sweeps in one
+// launch with a grid barrier between them, so a 6-sweep relax costs one
+// launch instead of twelve.  The launch is cooperative (all CTAs resident);
+// the barrier is a sense-reversing counter in the case's scalar block whose
+// waits are bounded: a timeout records WF_ST_WAIT_TIMEOUT and the kernel
+// finishes its remaining half-sweeps without waiting (results then invalid,
+// the host raises).
+constexpr int GBAR_SPINS = 1 << 22;
+
+__device__ __forceinline__ void grid_barrier(unsigned* gbar, unsigned nblocks, int* err,
+                                             bool& timed_out) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* vgen = gbar + 1;
+    const unsigned gen = *vgen;
+    __threadfence();
+    if (atomicAdd(gbar, 1u) == nblocks - 1) {
+      gbar[0] = 0u;
+      __threadfence();
+      atomicAdd(gbar + 1, 1u);
+    } else if (!timed_out) {
+      int it = 0;
+      while (*vgen == gen) {
+        if (++it > GBAR_SPINS) {
+          timed_out = true;
+          if (err) atomicExch(err, (int)WF_ST_WAIT_TIMEOUT);
+          break;
+        }
+        __nanosleep(20);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+template <class T>
+__global__ void __launch_bounds__(MG_TPB) k_relax_persist(const Lvl<T> L, int nsweeps) {
+  const int n = L.n;
+  const int nh = (n + 1) >> 1;
+  const long tot = (long)n * n * nh;
+  bool timed_out = false;
+  for (int hs = 0; hs < 2 * nsweeps; ++hs) {
+    const int color = hs & 1;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
+         t += (long)gridDim.x * blockDim.x) {
+      const int kk = (int)(t % nh);
+      const int j = (int)((t / nh) % n);
+      const int i = (int)(t / ((long)nh * n));
+      const int k = 2 * kk + ((1 + i + j + color) & 1);
+      if (k >= n) continue;
+      const long c = lid(L, i + 1, j + 1, k + 1);
+      const T aw = i > 0 ? L.ax : T(0), ae = i < n - 1 ? L.ax : T(0);
+      const T as = j > 0 ? L.ay : T(0), an = j < n - 1 ? L.ay : T(0);
+      const T ab = k > 0 ? L.az : T(0), at = k < n - 1 ? L.az : T(0);
+      const T ap = -(aw + ae + as + an + ab + at);
+      const T* phi = L.phi;
+      const T s = aw * phi[c - L.sI] + ae * phi[c + L.sI] + as * phi[c - L.sJ] +
+                  an * phi[c + L.sJ] + ab * phi[c - 1] + at * phi[c + 1];
+      const T x = (L.rhs[c] - s) / ap;
+      L.phi[c] = x;
+      ring_mirror(L, i, j, k, c, x);
+    }
+    if (hs + 1 < 2 * nsweeps) grid_barrier(L.gbar, gridDim.x, L.err, timed_out);
+  }
+}
+
+template <class T>
+static int launch_relax_persist(const Lvl<T>& L, int nsweeps, cudaStream_t s, bool* done) {
+  *done = false;
+  static int blocks_per_sm[2] = {-1, -1};
+  int& bps = blocks_per_sm[sizeof(T) == 4 ? 1 : 0];
+  if (bps < 0) {
+    WF_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_relax_persist<T>, MG_TPB, 0));
+  }
+  int dev = 0, nsm = 0;
+  WF_CK(cudaGetDevice(&dev));
+  WF_CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const long half = (long)L.n * L.n * ((L.n + 1) / 2);
+  long want = (half + MG_TPB - 1) / MG_TPB;
+  const long cap = (long)nsm * std::max(1, std::min(bps, 4));
+  const int nb = (int)std::max(1L, std::min(want, cap));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nb, 1, 1);
+  cfg.blockDim = dim3(MG_TPB, 1, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  WF_CK(cudaLaunchKernelEx(&cfg, k_relax_persist<T>, L, nsweeps));
+  WF_CKL("k_relax_persist");
+  *done = true;
+  return WF_OK;
+}
+
+// smallest level edge that relaxes in one cooperative launch (WF_PERSIST_MIN)
+static int persist_min_n() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("WF_PERSIST_MIN");
+    v = e ? atoi(e) : 1 << 30;
+  }
+  return v;
+}
+
 // max |rhs - A phi| over a level (tests/test_mg.py:16-32)
 __global__ void k_resmax(const Lvl<double> L, double* out, unsigned int* ticket,
                          unsigned long long* acc) {
@@ -1054,9 +1382,11 @@ template <class T>
 static int relax(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
   if (nsweeps <= 0) return WF_OK;
   // small levels with many sweeps: the column kernel
-  if (nsweeps > 12 || L.n <= 12) {
+  if (nsweeps > 12 || L.n <= 24) {
+    // small levels: one CTA, or a cluster when there are many sweeps
     int rc = WF_OK;
     const int strat = coarse_strategy(L.n, sizeof(T) == 4);
+    if (nsweeps > 12 && strat == 3 && try_coarse_tb<T>(L, nsweeps, s, &rc)) return rc;
     if (nsweeps > 12 && strat == 2 && try_coarse_p2p<T>(L, nsweeps, s, &rc)) return rc;
     if (nsweeps > 12 && strat == 1 && try_coarse_cluster<T>(L, nsweeps, s, &rc)) return rc;
     if (try_coarse<T>(L, nsweeps, s, &rc)) return rc;
@@ -1078,6 +1408,11 @@ static int relax(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
       WF_CKL("k_rbgs");
     }
     return WF_OK;
+  }
+  if (L.gbar && nsweeps >= 1 && L.n >= persist_min_n()) {
+    bool done = false;
+    WF_TRY(launch_relax_persist<T>(L, nsweeps, s, &done));
+    if (done) return WF_OK;
   }
   const size_t sb = smem_bytes<T>(L.n);
   if (sb <= SMEM_CAP) {
@@ -1141,6 +1476,7 @@ static int build_levels(const wf_case& c, T* phi0, const T* rhs0, long sI, long 
     L.n = c.n >> l;
     L.err = c.sc ? &c.sc->status : nullptr;
     L.tmp = (T*)c.mg_tmp[l];
+    L.gbar = c.sc ? c.sc->gbar : nullptr;
     L.tJ = L.n + 2;
     L.tI = (long)(L.n + 2) * (L.n + 2);
     if ((L.n << l) != c.n || L.n < 1)
@@ -1222,6 +1558,7 @@ static int build_levels_f32(const wf_case& c, std::vector<Lvl<float>>& lv) {
     L.n = c.n >> l;
     L.err = c.sc ? &c.sc->status : nullptr;
     L.tmp = (float*)c.mg_tmp[l];
+    L.gbar = c.sc ? c.sc->gbar : nullptr;
     L.tJ = L.n + 2;
     L.tI = (long)(L.n + 2) * (L.n + 2);
     L.phi = (float*)c.mg_phi[l];
@@ -1256,6 +1593,7 @@ static Lvl<double> level0_view(const wf_case& c, double* phi, const double* rhs,
   L.sJ = sJ;
   L.err = c.sc ? &c.sc->status : nullptr;
   L.tmp = nullptr;
+  L.gbar = c.sc ? c.sc->gbar : nullptr;
   L.ax = 1.0 / (c.dx * c.dx);
   L.ay = 1.0 / (c.dy * c.dy);
   L.az = 1.0 / (c.dz * c.dz);
@@ -1441,6 +1779,7 @@ int mg_solve_noalloc(const double* su, double* pp, int n, int nlev, double dx, d
     Lvl<double>& L = lv[l];
     L.err = nullptr;
     L.tmp = nullptr;
+    L.gbar = nullptr;
     L.ax = 1.0 / (dxl * dxl);
     L.ay = 1.0 / (dyl * dyl);
     L.az = 1.0 / (dzl * dzl);

@@ -61,6 +61,7 @@ __global__ void k_scalars_init(wf_scalars* sc, double dt0) {
   sc->loop = 0;
   sc->ticket = 0u;
   sc->nmg = 0;
+  sc->gbar[0] = sc->gbar[1] = 0u;
 }
 
 int launch_scalars_init(wf_scalars* sc, double dt0, cudaStream_t s) {

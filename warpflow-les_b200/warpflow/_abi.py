@@ -38,6 +38,7 @@ class WfScalars(ctypes.Structure):
         ("loop", ctypes.c_int32),
         ("ticket", ctypes.c_uint32),
         ("nmg", ctypes.c_int32),
+        ("gbar", ctypes.c_uint32 * 2),
     ]
 
 
