@@ -180,7 +180,7 @@ def bench_ensemble(args):
 
     def run(precision, concurrent, steps, warm):
         cfgs = [cavity_case(sp.n, sp.re, sp.ulid, precision=precision) for sp in specs]
-        ens = Ensemble(cfgs, nstreams=16 if concurrent else 1)
+        ens = Ensemble(cfgs, nstreams=args.streams if concurrent else 1)
         for _ in range(warm):
             ens.step()
         torch.cuda.synchronize()
@@ -206,7 +206,8 @@ def bench_ensemble(args):
         "ms_per_batch_step": round(1e3 * dt / K, 3), "iters_mean": round(iters, 2),
         "plain_fp64_per_case_loop": round(plain, 2),
         "speedup_vs_plain": round(val / plain, 2),
-        "config": {"cases": args.cases, "sizes": sorted({sp.n for sp in specs}),
+        "config": {"cases": args.cases, "streams": args.streams,
+                   "sizes": sorted({sp.n for sp in specs}),
                    "seed": 0, "timing": "wall clock around whole batch steps, synced"}}),
         flush=True)
 
@@ -303,6 +304,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--mode", default="step", choices=["step", "ensemble", "serve", "poisson"])
     ap.add_argument("--cases", type=int, default=64)
+    ap.add_argument("--streams", type=int, default=16)
     ap.add_argument("--requests", type=int, default=48)
     ap.add_argument("--step-scale", type=float, default=0.05)
     args = ap.parse_args()

@@ -5,6 +5,15 @@
 
 namespace wf {
 
+// Programmatic dependent launch: every kernel of this library starts by
+// allowing its successor to begin launching, then waits until its
+// predecessor has completed and its memory is visible.  Without the launch
+// attribute both instructions are no-ops.
+__device__ __forceinline__ void pdl_entry() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 __device__ __forceinline__ unsigned long long dbits(double x) {
   return (unsigned long long)__double_as_longlong(x);
 }

@@ -7,6 +7,7 @@
 // ordered phases -- x faces, y faces, z faces -- and each phase runs as one
 // launch in which a thread owns one (a, b) line of every face op of that
 // phase and walks its layers in order.  Up to three fields share a launch.
+#include "wf_dev.cuh"
 #include "wf_internal.h"
 
 namespace wf {
@@ -35,6 +36,7 @@ struct PhaseArgs {
 };
 
 __global__ void k_fill_phase(const PhaseArgs args) {
+  pdl_entry();
   // b (k for x/y faces) is the fast lane index so stores coalesce
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   const int a = blockIdx.y * blockDim.y + threadIdx.y;
@@ -171,7 +173,7 @@ int launch_fills(const FillReq* reqs, int nreq, int n, cudaStream_t s) {
     }
     dim3 tb(32, 8);
     dim3 gb((a.bmax + 31) / 32, (a.amax + 7) / 8, nreq);
-    k_fill_phase<<<gb, tb, 0, s>>>(a);
+    WF_CK(launch_k(k_fill_phase, gb, tb, 0, s, a));
     WF_CKL("k_fill_phase");
   }
   return WF_OK;

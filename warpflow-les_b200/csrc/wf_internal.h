@@ -38,6 +38,31 @@ extern thread_local long g_launches;
 
 inline int64_t padded(int n) { return (int64_t)n + 2 * NPL; }
 
+// programmatic dependent launch on (default) or off (WF_PDL=0)
+bool pdl_enabled();
+
+// launch a kernel of this library, with the programmatic-serialization
+// attribute when enabled and an optional cluster shape
+template <typename... ExpTypes, typename... ActTypes>
+inline cudaError_t launch_k(void (*kernel)(ExpTypes...), dim3 grid, dim3 block, size_t smem,
+                            cudaStream_t s, ActTypes&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  int na = 0;
+  if (pdl_enabled()) {
+    at[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[na].val.programmaticStreamSerializationAllowed = 1;
+    ++na;
+  }
+  cfg.attrs = at;
+  cfg.numAttrs = na;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<ActTypes&&>(args)...);
+}
+
 int validate_case(const wf_case& c);
 
 // ---- ghost fills ---------------------------------------------------------

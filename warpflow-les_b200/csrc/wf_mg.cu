@@ -66,6 +66,7 @@ __device__ __forceinline__ void ring_mirror(const Lvl<T>& L, int i, int j, int k
 // one colour half-sweep (multigrid.py:70-90): update where (i+j+k+color)%2==1
 template <class T>
 __global__ void __launch_bounds__(MG_TPB) k_rbgs(const Lvl<T> L, int color) {
+  pdl_entry();
   const int n = L.n;
   const int nh = (n + 1) >> 1;
   const long tot = (long)n * n * nh;
@@ -93,6 +94,7 @@ __global__ void __launch_bounds__(MG_TPB) k_rbgs(const Lvl<T> L, int color) {
 // restriction (multigrid.py:93-119): rhs_c = 1/8 sum of the 8 fine residuals
 template <class T>
 __global__ void __launch_bounds__(MG_TPB) k_restrict(const Lvl<T> F, T* rhs_c, Lvl<T> C) {
+  pdl_entry();
   const int nc = C.n, n = F.n;
   const long tot = (long)nc * nc * nc;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
@@ -126,6 +128,7 @@ __global__ void __launch_bounds__(MG_TPB) k_restrict(const Lvl<T> F, T* rhs_c, L
 // zero a whole (n+2)^3 ring-layout level array
 template <class T>
 __global__ void k_zero(T* a, long cnt) {
+  pdl_entry();
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < cnt;
        t += (long)gridDim.x * blockDim.x)
     a[t] = T(0);
@@ -134,6 +137,7 @@ __global__ void k_zero(T* a, long cnt) {
 // zero a (n+2)^3 block embedded with strides (sI, sJ)
 template <class T>
 __global__ void k_zero_strided(T* a, int m, long sI, long sJ) {
+  pdl_entry();
   const long tot = (long)m * m * m;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
        t += (long)gridDim.x * blockDim.x) {
@@ -147,6 +151,7 @@ __global__ void k_zero_strided(T* a, int m, long sI, long sJ) {
 // prolongation (multigrid.py:122-146) + the ring refill that follows it
 template <class T>
 __global__ void __launch_bounds__(MG_TPB) k_prolong(const Lvl<T> C, Lvl<T> F) {
+  pdl_entry();
   const int n = F.n;
   const long tot = (long)n * n * n;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
@@ -187,6 +192,7 @@ __global__ void __launch_bounds__(MG_TPB) k_prolong(const Lvl<T> C, Lvl<T> F) {
 // After the last sweep the interior and the face rings go back to global.
 template <class T>
 __global__ void __launch_bounds__(1024) k_relax_smem(Lvl<T> L, int nsweeps) {
+  pdl_entry();
   extern __shared__ __align__(16) unsigned char smraw[];
   T* sphi = reinterpret_cast<T*>(smraw);
   const int n = L.n;
@@ -291,6 +297,7 @@ struct CoarseShape {
 template <class T, int NC, bool RHS_SMEM>
 __global__ void __launch_bounds__(CoarseShape<NC>::THREADS) k_coarse_cols(Lvl<T> L,
                                                                            int nsweeps) {
+  pdl_entry();
   constexpr int H = NC / 2;
   constexpr int HALF = NC * H;                  // columns per parity
   constexpr int GROUP = ((HALF + 31) / 32) * 32;
@@ -366,7 +373,7 @@ static int launch_coarse(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
   const size_t sb = (size_t)NC * NC * NC * sizeof(T) * (RHS_SMEM ? 2 : 1);
   WF_CK(cudaFuncSetAttribute(k_coarse_cols<T, NC, RHS_SMEM>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb));
-  k_coarse_cols<T, NC, RHS_SMEM><<<1, 2 * GROUP, sb, s>>>(L, nsweeps);
+  WF_CK(launch_k(k_coarse_cols<T, NC, RHS_SMEM>, 1, 2 * GROUP, sb, s, L, nsweeps));
   WF_CKL("k_coarse_cols");
   return WF_OK;
 }
@@ -406,6 +413,7 @@ struct ClusterShape {
 template <class T, int NC, int NCL>
 __global__ void __launch_bounds__(ClusterShape<NC, NCL>::THREADS)
     k_coarse_cluster(Lvl<T> L, int nsweeps) {
+  pdl_entry();
   using S = ClusterShape<NC, NCL>;
   constexpr int H = S::H, HALF = S::HALF, GROUP = S::GROUP, PL = S::PL, C = S::C;
   namespace cg = cooperative_groups;
@@ -507,13 +515,15 @@ static int launch_coarse_cluster(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
   cfg.blockDim = dim3(S::THREADS, 1, 1);
   cfg.dynamicSmemBytes = sb;
   cfg.stream = s;
-  cudaLaunchAttribute at[1];
+  cudaLaunchAttribute at[2];
   at[0].id = cudaLaunchAttributeClusterDimension;
   at[0].val.clusterDim.x = S::C;
   at[0].val.clusterDim.y = 1;
   at[0].val.clusterDim.z = 1;
+  at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[1].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = pdl_enabled() ? 2 : 1;
   WF_CK(cudaLaunchKernelEx(&cfg, kern, L, nsweeps));
   WF_CKL("k_coarse_cluster");
   return WF_OK;
@@ -594,6 +604,7 @@ constexpr int MBAR_WAIT_TRIES = 1 << 22;
 template <class T, int NC, int NCL>
 __global__ void __launch_bounds__(ClusterShape<NC, NCL>::THREADS)
     k_coarse_p2p(Lvl<T> L, int nsweeps, int wmode) {
+  pdl_entry();
   using S = ClusterShape<NC, NCL>;
   constexpr int H = S::H, HALF = S::HALF, GROUP = S::GROUP, PL = S::PL, C = S::C;
   namespace cg = cooperative_groups;
@@ -732,18 +743,21 @@ static int launch_coarse_p2p(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
   const size_t sb = 2ull * NC * S::PL * sizeof(T);
   auto kern = k_coarse_p2p<T, NC, NCL>;
   WF_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb));
+  if (S::C > 8) WF_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(S::C, 1, 1);
   cfg.blockDim = dim3(S::THREADS, 1, 1);
   cfg.dynamicSmemBytes = sb;
   cfg.stream = s;
-  cudaLaunchAttribute at[1];
+  cudaLaunchAttribute at[2];
   at[0].id = cudaLaunchAttributeClusterDimension;
   at[0].val.clusterDim.x = S::C;
   at[0].val.clusterDim.y = 1;
   at[0].val.clusterDim.z = 1;
+  at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[1].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = pdl_enabled() ? 2 : 1;
   static int wmode = -1;
   if (wmode < 0) {
     const char* e = getenv("WF_MBWAIT");
@@ -752,6 +766,20 @@ static int launch_coarse_p2p(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
   WF_CK(cudaLaunchKernelEx(&cfg, kern, L, nsweeps, wmode));
   WF_CKL("k_coarse_p2p");
   return WF_OK;
+}
+
+// thin slabs: more CTAs per cluster (up to 16, non-portable sizes)
+template <class T>
+static int try_coarse_p2p_thin(const Lvl<T>& L, int nsweeps, cudaStream_t s, int* rc) {
+  switch (L.n) {
+    case 12: *rc = launch_coarse_p2p<T, 12, 1>(L, nsweeps, s); return 1;
+    case 16: *rc = launch_coarse_p2p<T, 16, 1>(L, nsweeps, s); return 1;
+    case 20: *rc = launch_coarse_p2p<T, 20, 2>(L, nsweeps, s); return 1;
+    case 24: *rc = launch_coarse_p2p<T, 24, 2>(L, nsweeps, s); return 1;
+    case 28: *rc = launch_coarse_p2p<T, 28, 2>(L, nsweeps, s); return 1;
+    case 32: *rc = launch_coarse_p2p<T, 32, 2>(L, nsweeps, s); return 1;
+    default: return 0;
+  }
 }
 
 template <class T>
@@ -796,6 +824,7 @@ struct TbShape {
 template <class T, int NC, int NCL>
 __global__ void __launch_bounds__(TbShape<NC, NCL>::THREADS)
     k_coarse_tb(Lvl<T> L, int nsweeps, int wmode) {
+  pdl_entry();
   using S = TbShape<NC, NCL>;
   constexpr int H = S::H, HALF = S::HALF, GROUP = S::GROUP, PL = S::PL, C = S::C;
   constexpr int SIDE = S::SIDE;
@@ -961,13 +990,15 @@ static int launch_coarse_tb(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
   cfg.blockDim = dim3(S::THREADS, 1, 1);
   cfg.dynamicSmemBytes = sb;
   cfg.stream = s;
-  cudaLaunchAttribute at[1];
+  cudaLaunchAttribute at[2];
   at[0].id = cudaLaunchAttributeClusterDimension;
   at[0].val.clusterDim.x = S::C;
   at[0].val.clusterDim.y = 1;
   at[0].val.clusterDim.z = 1;
+  at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[1].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = pdl_enabled() ? 2 : 1;
   WF_CK(cudaLaunchKernelEx(&cfg, kern, L, nsweeps, 1));
   WF_CKL("k_coarse_tb");
   return WF_OK;
@@ -995,29 +1026,31 @@ static int try_coarse_tb(const Lvl<T>& L, int nsweeps, cudaStream_t s, int* rc) 
 // table that the autotuner (warpflow/autotune.py) can overwrite through
 // wf_set_coarse_strategy; WF_COARSE forces one strategy for every size.
 // Defaults measured on B200 (ns per half-sweep, FP64, 300-sweep relax):
-//   n:        8    12    16    20    24    32
-//   1 CTA:  133   263   407   903  1530  4090
-//   barrier 442   449   488   651   686   921
-//   p2p:    402   488   500   602   895   815
+//   n:             8    12    16    20    24    32
+//   0 one CTA:   133   263   407   903  1530  4090
+//   1 barrier:   442   449   488   651   686   921
+//   2 p2p:       402   487   501   596   905   860
+//   3 tb:        499   625  1143  1281  1962  3802
+//   4 p2p thin:    -   427   464   762   631   776
 static int g_strategy[2][65];
 static bool g_strategy_init = false;
 
 static void strategy_defaults() {
   for (int f = 0; f < 2; ++f)
-    for (int n = 0; n <= 64; ++n) g_strategy[f][n] = n <= 16 ? 0 : (n == 24 ? 1 : 2);
+    for (int n = 0; n <= 64; ++n) g_strategy[f][n] = n <= 16 ? 0 : (n == 20 ? 2 : 4);
   g_strategy_init = true;
 }
 
 static int coarse_strategy(int n, bool fp32) {
   const char* e = getenv("WF_COARSE");
-  if (e && e[0] >= '0' && e[0] <= '3') return e[0] - '0';
+  if (e && e[0] >= '0' && e[0] <= '4') return e[0] - '0';
   if (!g_strategy_init) strategy_defaults();
   return (n >= 0 && n <= 64) ? g_strategy[fp32 ? 1 : 0][n] : 2;
 }
 
 int set_coarse_strategy(int n, int fp32, int strategy) {
-  if (n < 0 || n > 64 || strategy < 0 || strategy > 3)
-    return fail(WF_EINVAL, "wf_set_coarse_strategy: n in 0..64, strategy in 0..3");
+  if (n < 0 || n > 64 || strategy < 0 || strategy > 4)
+    return fail(WF_EINVAL, "wf_set_coarse_strategy: n in 0..64, strategy in 0..4");
   if (!g_strategy_init) strategy_defaults();
   g_strategy[fp32 ? 1 : 0][n] = strategy;
   return WF_OK;
@@ -1058,18 +1091,29 @@ static int try_coarse_cluster(const Lvl<T>& L, int nsweeps, cudaStream_t s, int*
 template <int TJ, int TK>
 struct SweepTile {
   static constexpr int WJ = TJ + 4, WK = TK + 4;
+  static constexpr int WH = WK / 2;            // cells per parity half-row
   static constexpr int PLANE = WJ * WK;
-  static constexpr int THREADS = 320;
+  static constexpr int THREADS = 32 * (TJ + 2);  // one warp per row of the red region
 };
 
+// Window layout: [plane slot 4][k parity 2][row WJ][WH].  Cell (jj, kk) sits
+// in half-row kk&1 at index kk>>1; k k0 is even, so within a row of plane q
+// the red cells are exactly one parity half-row ((1 + q + j) & 1) and the
+// black cells the other.  A warp owns a row, lane = index in the half-row:
+// every access of a warp (its own cells, k+-1 in the other half-row, j+-1
+// in the same half-row of the adjacent rows, i+-1 in the adjacent planes)
+// is a contiguous run, free of bank conflicts.
 template <class T, int TJ, int TK>
 __global__ void __launch_bounds__(SweepTile<TJ, TK>::THREADS)
     k_sweep2(const T* __restrict__ src, long sIs, long sJs, T* __restrict__ dst, long sId,
              long sJd, const T* __restrict__ rhs, long sIr, long sJr, int n, T ax, T ay,
              T az, int seg, int write_ring) {
+  pdl_entry();
   using W = SweepTile<TJ, TK>;
-  constexpr int WK = W::WK, PLANE = W::PLANE, NT = W::THREADS;
-  constexpr int PER = (PLANE + NT - 1) / NT;  // window elements per thread
+  constexpr int WJ = W::WJ, WK = W::WK, WH = W::WH, PLANE = W::PLANE, NT = W::THREADS;
+  constexpr int HALF = WJ * WH;                // one parity of a plane
+  constexpr int PER = (PLANE + NT - 1) / NT;
+  static_assert(TK == 64, "lane mapping assumes 32 cells per parity half-row");
   __shared__ T win[4][PLANE];
   __shared__ T rb[2][PLANE];
   const int ntk = (n + TK - 1) / TK;
@@ -1078,8 +1122,10 @@ __global__ void __launch_bounds__(SweepTile<TJ, TK>::THREADS)
   const int i0 = blockIdx.y * seg;
   const int i1 = min(n, i0 + seg);
   const int tid = threadIdx.x;
-  // this thread's window elements: offsets into a plane of src / rhs
+  const int warp = tid >> 5, lane = tid & 31;
+  // loader mapping: element e of this thread = window cell (jj, kk), kk fastest
   long offs[PER], roff[PER];
+  int sidx[PER];
   bool okp[PER], okr[PER];
 #pragma unroll
   for (int e = 0; e < PER; ++e) {
@@ -1090,9 +1136,10 @@ __global__ void __launch_bounds__(SweepTile<TJ, TK>::THREADS)
     okr[e] = t < PLANE && j >= 0 && j < n && k >= 0 && k < n;
     offs[e] = okp[e] ? (long)(j + 1) * sJs + (k + 1) : 0;
     roff[e] = okr[e] ? (long)(j + 1) * sJr + (k + 1) : 0;
+    sidx[e] = t < PLANE ? (kk & 1) * HALF + jj * WH + (kk >> 1) : 0;
   }
-  T pf[PER], rf[PER];  // prefetched plane values (phi of plane q, rhs of plane q-1)
-  auto fetch = [&](int q) {
+  T pf[PER], rf[PER];
+  auto fetch = [&](int q) {  // phi of plane q and rhs of plane q-1 into registers
 #pragma unroll
     for (int e = 0; e < PER; ++e) {
       pf[e] = (okp[e] && q <= n) ? src[(long)(q + 1) * sIs + offs[e]] : T(0);
@@ -1104,15 +1151,30 @@ __global__ void __launch_bounds__(SweepTile<TJ, TK>::THREADS)
     T* r = rb[(q + 3) & 1];
 #pragma unroll
     for (int e = 0; e < PER; ++e) {
-      const int t = tid + e * NT;
-      if (t < PLANE) {
-        w[t] = pf[e];
-        r[t] = rf[e];
+      if (tid + e * NT < PLANE) {
+        w[sidx[e]] = pf[e];
+        r[sidx[e]] = rf[e];
       }
     }
   };
-  // loop invariant at plane p: the window holds planes p-2, p-1, p (and the
-  // rhs of p-1); plane p+1 with the rhs of p sits in registers
+  // one update of cell (row jj, parity par, index h) of plane pl (real index)
+  auto update = [&](int pl, int jj, int par, int h, T* wc, const T* wm, const T* wp,
+                    const T* rr) {
+    const int kk = 2 * h + par;
+    const int j = j0 - 2 + jj, k = k0 - 2 + kk;
+    if (j < 0 || j >= n || k < 0 || k >= n) return;
+    const int c = par * HALF + jj * WH + h;
+    const int ck = (1 - par) * HALF + jj * WH;          // other half-row of this row
+    const int km = ck + (par ? h : h - 1);              // kk-1
+    const int kp = ck + (par ? h + 1 : h);              // kk+1
+    const T aw = pl > 0 ? ax : T(0), ae = pl < n - 1 ? ax : T(0);
+    const T as = j > 0 ? ay : T(0), an = j < n - 1 ? ay : T(0);
+    const T ab = k > 0 ? az : T(0), at = k < n - 1 ? az : T(0);
+    const T ap = -(aw + ae + as + an + ab + at);
+    const T sum = aw * wm[c] + ae * wp[c] + as * wc[c - WH] + an * wc[c + WH] +
+                  ab * wc[km] + at * wc[kp];
+    wc[c] = (rr[c] - sum) / ap;
+  };
   if (i0 - 2 >= -1) {
     fetch(i0 - 2);
     deposit(i0 - 2);
@@ -1121,71 +1183,53 @@ __global__ void __launch_bounds__(SweepTile<TJ, TK>::THREADS)
   deposit(i0 - 1);
   fetch(i0);
   for (int p = i0 - 1; p <= i1; ++p) {
-    __syncthreads();  // previous plane's reads of the slots about to change are done
-    deposit(p + 1);   // plane p+1 and rhs of plane p
     __syncthreads();
-    if (p + 2 <= i1 + 1) fetch(p + 2);  // in flight during this plane's compute
-    // red on plane p over the tile plus a one-cell halo (real cells only)
+    deposit(p + 1);
+    __syncthreads();
+    if (p + 2 <= i1 + 1) fetch(p + 2);
+    // red on plane p over rows 1..TJ+2 (warp = row), cells kk in 1..TK+2
     if (p >= 0 && p < n) {
       T* wc = win[(p + 4) & 3];
       const T* wm = win[(p + 3) & 3];
       const T* wp = win[(p + 5) & 3];
       const T* rr = rb[p & 1];
-      constexpr int RJ = TJ + 2, RK = (TK + 2) / 2;
-      for (int t = tid; t < RJ * RK; t += NT) {
-        const int a = t / RK, b = t - a * RK;
-        const int j = j0 - 1 + a;
-        int k = k0 - 1 + 2 * b;
-        if (((p + j + k) & 1) == 0) ++k;  // the odd (red) cell of the pair
-        if (j < 0 || j >= n || k < 0 || k >= n || k > k0 + TK) continue;
-        const int c = (j - j0 + 2) * WK + (k - k0 + 2);
-        const T aw = p > 0 ? ax : T(0), ae = p < n - 1 ? ax : T(0);
-        const T as = j > 0 ? ay : T(0), an = j < n - 1 ? ay : T(0);
-        const T ab = k > 0 ? az : T(0), at = k < n - 1 ? az : T(0);
-        const T ap = -(aw + ae + as + an + ab + at);
-        const T sum = aw * wm[c] + ae * wp[c] + as * wc[c - WK] + an * wc[c + WK] +
-                      ab * wc[c - 1] + at * wc[c + 1];
-        wc[c] = (rr[c] - sum) / ap;
-      }
+      const int jj = 1 + warp;
+      const int j = j0 - 2 + jj;
+      const int par = (1 + p + j) & 1;  // half-row holding the red cells (k0 even)
+      // red kk range [1, TK+2]: parity 1 -> h 0..TK/2, parity 0 -> h 1..TK/2+1
+      const int hlo = par ? 0 : 1;
+      update(p, jj, par, hlo + lane, wc, wm, wp, rr);
+      if (lane == 0) update(p, jj, par, hlo + 32, wc, wm, wp, rr);
     }
     __syncthreads();
-    // black on plane q = p-1 of the tile, then store both colours of q
+    // black on plane q = p-1, rows 2..TJ+1, then store both colours of q
     const int q = p - 1;
-    if (q >= i0 && q < i1) {
+    if (q >= i0 && q < i1 && warp < TJ) {
       T* wc = win[(q + 4) & 3];
       const T* wm = win[(q + 3) & 3];
       const T* wp = win[(q + 5) & 3];
       const T* rr = rb[q & 1];
-      constexpr int BK = TK / 2;
-      for (int t = tid; t < TJ * BK; t += NT) {
-        const int a = t / BK, b = t - a * BK;
-        const int j = j0 + a;
-        const int kr = k0 + 2 * b;
-        if (j >= n || kr >= n) continue;
-        int k = kr;
-        if (((q + j + k) & 1) == 1) ++k;  // the even (black) cell of the pair
-        const int ck = (j - j0 + 2) * WK;
-        if (k < n) {
-          const int c = ck + (k - k0 + 2);
-          const T aw = q > 0 ? ax : T(0), ae = q < n - 1 ? ax : T(0);
-          const T as = j > 0 ? ay : T(0), an = j < n - 1 ? ay : T(0);
-          const T ab = k > 0 ? az : T(0), at = k < n - 1 ? az : T(0);
-          const T ap = -(aw + ae + as + an + ab + at);
-          const T sum = aw * wm[c] + ae * wp[c] + as * wc[c - WK] + an * wc[c + WK] +
-                        ab * wc[c - 1] + at * wc[c + 1];
-          wc[c] = (rr[c] - sum) / ap;
-        }
-        for (int kk = kr; kk < kr + 2 && kk < n; ++kk) {
-          const T x = wc[ck + (kk - k0 + 2)];
-          const long o = (long)(q + 1) * sId + (long)(j + 1) * sJd + (kk + 1);
+      const int jj = 2 + warp;
+      const int j = j0 - 2 + jj;
+      const int par = (q + j) & 1;      // half-row holding the black cells
+      update(q, jj, par, 1 + lane, wc, wm, wp, rr);
+      __syncwarp();
+      if (j < n) {
+#pragma unroll
+        for (int pp = 0; pp < 2; ++pp) {
+          const int kk = 2 * (1 + lane) + pp;   // tile cells kk 2..TK+1
+          const int k = k0 - 2 + kk;
+          if (k >= n) continue;
+          const T x = wc[pp * HALF + jj * WH + 1 + lane];
+          const long o = (long)(q + 1) * sId + (long)(j + 1) * sJd + (k + 1);
           dst[o] = x;
           if (write_ring) {
             if (q == 0) dst[o - sId] = x;
             if (q == n - 1) dst[o + sId] = x;
             if (j == 0) dst[o - sJd] = x;
             if (j == n - 1) dst[o + sJd] = x;
-            if (kk == 0) dst[o - 1] = x;
-            if (kk == n - 1) dst[o + 1] = x;
+            if (k == 0) dst[o - 1] = x;
+            if (k == n - 1) dst[o + 1] = x;
           }
         }
       }
@@ -1193,14 +1237,14 @@ __global__ void __launch_bounds__(SweepTile<TJ, TK>::THREADS)
   }
 }
 
-constexpr int SWEEP_TJ = 16, SWEEP_TK = 32;
+constexpr int SWEEP_TJ = 8, SWEEP_TK = 64;
 
 // smallest level edge that uses one-launch sweeps (WF_SWEEP2_MIN overrides)
 static int sweep2_min_n() {
   static int v = -1;
   if (v < 0) {
     const char* e = getenv("WF_SWEEP2_MIN");
-    v = e ? atoi(e) : 128;
+    v = e ? atoi(e) : 1 << 30;
   }
   return v;
 }
@@ -1214,9 +1258,8 @@ static int launch_sweep2(const T* src, long sIs, long sJs, T* dst, long sId, lon
   int nseg = std::max(1, (2 * 148 + ntj * ntk - 1) / (ntj * ntk));
   int seg = std::min(32, std::max(4, (n + nseg - 1) / nseg));
   nseg = (n + seg - 1) / seg;
-  k_sweep2<T, SWEEP_TJ, SWEEP_TK><<<dim3(ntj * ntk, nseg), SweepTile<SWEEP_TJ, SWEEP_TK>::THREADS,
-                                    0, s>>>(src, sIs, sJs, dst, sId, sJd, L.rhs, L.sI, L.sJ, n,
-                                            L.ax, L.ay, L.az, seg, write_ring);
+  WF_CK(launch_k(k_sweep2<T, SWEEP_TJ, SWEEP_TK>, dim3(ntj * ntk, nseg), SweepTile<SWEEP_TJ, SWEEP_TK>::THREADS, 0, s, src, sIs, sJs, dst, sId, sJd, L.rhs, L.sI, L.sJ, n,
+                                            L.ax, L.ay, L.az, seg, write_ring));
   WF_CKL("k_sweep2");
   return WF_OK;
 }
@@ -1260,6 +1303,7 @@ __device__ __forceinline__ void grid_barrier(unsigned* gbar, unsigned nblocks, i
 
 template <class T>
 __global__ void __launch_bounds__(MG_TPB) k_relax_persist(const Lvl<T> L, int nsweeps) {
+  pdl_entry();
   const int n = L.n;
   const int nh = (n + 1) >> 1;
   const long tot = (long)n * n * nh;
@@ -1333,6 +1377,7 @@ static int persist_min_n() {
 // max |rhs - A phi| over a level (tests/test_mg.py:16-32)
 __global__ void k_resmax(const Lvl<double> L, double* out, unsigned int* ticket,
                          unsigned long long* acc) {
+  pdl_entry();
   __shared__ double sm[32];
   const int n = L.n;
   const long tot = (long)n * n * n;
@@ -1386,6 +1431,7 @@ static int relax(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
     // small levels: one CTA, or a cluster when there are many sweeps
     int rc = WF_OK;
     const int strat = coarse_strategy(L.n, sizeof(T) == 4);
+    if (nsweeps > 12 && strat == 4 && try_coarse_p2p_thin<T>(L, nsweeps, s, &rc)) return rc;
     if (nsweeps > 12 && strat == 3 && try_coarse_tb<T>(L, nsweeps, s, &rc)) return rc;
     if (nsweeps > 12 && strat == 2 && try_coarse_p2p<T>(L, nsweeps, s, &rc)) return rc;
     if (nsweeps > 12 && strat == 1 && try_coarse_cluster<T>(L, nsweeps, s, &rc)) return rc;
@@ -1402,9 +1448,9 @@ static int relax(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
     if (nsweeps & 1) {
       const long half = (long)L.n * L.n * ((L.n + 1) / 2);
       const int nb = mg_blocks(half);
-      k_rbgs<T><<<nb, MG_TPB, 0, s>>>(L, 0);
+      WF_CK(launch_k(k_rbgs<T>, nb, MG_TPB, 0, s, L, 0));
       WF_CKL("k_rbgs");
-      k_rbgs<T><<<nb, MG_TPB, 0, s>>>(L, 1);
+      WF_CK(launch_k(k_rbgs<T>, nb, MG_TPB, 0, s, L, 1));
       WF_CKL("k_rbgs");
     }
     return WF_OK;
@@ -1421,16 +1467,16 @@ static int relax(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
     const int n3 = L.n * L.n * L.n;
     int tpb = 1024;
     if (n3 / 2 < 1024) tpb = std::max(32, ((n3 / 2 + 31) / 32) * 32);
-    k_relax_smem<T><<<1, tpb, sb, s>>>(L, nsweeps);
+    WF_CK(launch_k(k_relax_smem<T>, 1, tpb, sb, s, L, nsweeps));
     WF_CKL("k_relax_smem");
     return WF_OK;
   }
   const long half = (long)L.n * L.n * ((L.n + 1) / 2);
   const int nb = mg_blocks(half);
   for (int sw = 0; sw < nsweeps; ++sw) {
-    k_rbgs<T><<<nb, MG_TPB, 0, s>>>(L, 0);
+    WF_CK(launch_k(k_rbgs<T>, nb, MG_TPB, 0, s, L, 0));
     WF_CKL("k_rbgs");
-    k_rbgs<T><<<nb, MG_TPB, 0, s>>>(L, 1);
+    WF_CK(launch_k(k_rbgs<T>, nb, MG_TPB, 0, s, L, 1));
     WF_CKL("k_rbgs");
   }
   return WF_OK;
@@ -1443,17 +1489,17 @@ static int vcycle(std::vector<Lvl<T>>& lv, const wf_case& c, cudaStream_t s) {
     if (l > 0) {
       Lvl<T>& C = lv[l];
       const long m = (long)C.n + 2;
-      k_zero<T><<<mg_blocks(m * m * m), MG_TPB, 0, s>>>(C.phi, m * m * m);
+      WF_CK(launch_k(k_zero<T>, mg_blocks(m * m * m), MG_TPB, 0, s, C.phi, m * m * m));
       WF_CKL("k_zero");
-      k_restrict<T><<<mg_blocks((long)C.n * C.n * C.n), MG_TPB, 0, s>>>(
-          lv[l - 1], const_cast<T*>(C.rhs), C);
+      WF_CK(launch_k(k_restrict<T>, mg_blocks((long)C.n * C.n * C.n), MG_TPB, 0, s, 
+          lv[l - 1], const_cast<T*>(C.rhs), C));
       WF_CKL("k_restrict");
     }
     WF_TRY(relax(lv[l], l < L - 1 ? c.n_pre : c.n_coarse, s));
   }
   for (int l = L - 2; l >= 0; --l) {
-    k_prolong<T><<<mg_blocks((long)lv[l].n * lv[l].n * lv[l].n), MG_TPB, 0, s>>>(lv[l + 1],
-                                                                                 lv[l]);
+    WF_CK(launch_k(k_prolong<T>, mg_blocks((long)lv[l].n * lv[l].n * lv[l].n), MG_TPB, 0, s, lv[l + 1],
+                                                                                 lv[l]));
     WF_CKL("k_prolong");
     WF_TRY(relax(lv[l], c.n_post, s));
   }
@@ -1508,6 +1554,7 @@ static int build_levels(const wf_case& c, T* phi0, const T* rhs0, long sI, long 
 // corrections; residual and accumulation stay FP64.
 __global__ void __launch_bounds__(MG_TPB) k_defect(const Lvl<double> F, float* rhs_f,
                                                    float* phi_f, int n) {
+  pdl_entry();
   const long m = (long)n + 2;
   const long tot = (long)n * n * n;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
@@ -1534,6 +1581,7 @@ __global__ void __launch_bounds__(MG_TPB) k_defect(const Lvl<double> F, float* r
 }
 
 __global__ void k_correct(const Lvl<double> F, const float* __restrict__ phi_f, int n) {
+  pdl_entry();
   const long m = (long)n + 2;
   const long tot = m * m * m;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
@@ -1573,12 +1621,12 @@ static int build_levels_f32(const wf_case& c, std::vector<Lvl<float>>& lv) {
 static int dc_cycle(const Lvl<double>& F, std::vector<Lvl<float>>& lvf, const wf_case& c,
                     cudaStream_t s) {
   const int n = F.n;
-  k_defect<<<mg_blocks((long)n * n * n), MG_TPB, 0, s>>>(F, const_cast<float*>(lvf[0].rhs),
-                                                       lvf[0].phi, n);
+  WF_CK(launch_k(k_defect, mg_blocks((long)n * n * n), MG_TPB, 0, s, F, const_cast<float*>(lvf[0].rhs),
+                                                       lvf[0].phi, n));
   WF_CKL("k_defect");
   WF_TRY(vcycle<float>(lvf, c, s));
   const long m = (long)n + 2;
-  k_correct<<<mg_blocks(m * m * m), MG_TPB, 0, s>>>(F, lvf[0].phi, n);
+  WF_CK(launch_k(k_correct, mg_blocks(m * m * m), MG_TPB, 0, s, F, lvf[0].phi, n));
   WF_CKL("k_correct");
   return WF_OK;
 }
@@ -1615,7 +1663,7 @@ int mg_solve(const wf_case& c, cudaStream_t s) {
     std::vector<Lvl<float>> lvf;
     WF_TRY(build_levels_f32(c, lvf));
     const Lvl<double> F = level0_view(c, pp + off, c.fld[WF_SU] + off, P * P, P);
-    k_zero<double><<<mg_blocks(P * P * P), MG_TPB, 0, s>>>(pp, P * P * P);
+    WF_CK(launch_k(k_zero<double>, mg_blocks(P * P * P), MG_TPB, 0, s, pp, P * P * P));
     WF_CKL("k_zero pp");
     for (int cyc = 0; cyc < c.n_vcycles; ++cyc) WF_TRY(dc_cycle(F, lvf, c, s));
     return WF_OK;
@@ -1627,7 +1675,7 @@ int mg_solve(const wf_case& c, cudaStream_t s) {
   std::vector<Lvl<double>> lv;
   WF_TRY(build_levels<double>(c, pp + off, su + off, P * P, P, lv));
   // multigrid.py:332-333: pp and level-0 phi start from zero
-  k_zero<double><<<mg_blocks(P * P * P), MG_TPB, 0, s>>>(pp, P * P * P);
+  WF_CK(launch_k(k_zero<double>, mg_blocks(P * P * P), MG_TPB, 0, s, pp, P * P * P));
   WF_CKL("k_zero pp");
   for (int cyc = 0; cyc < c.n_vcycles; ++cyc) WF_TRY(vcycle<double>(lv, c, s));
   return WF_OK;
@@ -1649,6 +1697,7 @@ int mg_relax_pair(const wf_case& c, double* phi0, const double* rhs0, int nsweep
 }
 
 __global__ void k_refill(Lvl<double> L) {
+  pdl_entry();
   const int n = L.n;
   const long tot = (long)n * n;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
@@ -1668,7 +1717,7 @@ int mg_refill_pair(const wf_case& c, double* phi0, cudaStream_t s) {
   const long m = c.n + 2;
   std::vector<Lvl<double>> lv;
   WF_TRY(build_levels<double>(c, phi0, phi0, m * m, m, lv));
-  k_refill<<<mg_blocks((long)c.n * c.n), MG_TPB, 0, s>>>(lv[0]);
+  WF_CK(launch_k(k_refill, mg_blocks((long)c.n * c.n), MG_TPB, 0, s, lv[0]));
   WF_CKL("k_refill");
   return WF_OK;
 }
@@ -1679,8 +1728,8 @@ int mg_residual_max_pair(const wf_case& c, const double* phi0, const double* rhs
   const long m = c.n + 2;
   std::vector<Lvl<double>> lv;
   WF_TRY(build_levels<double>(c, const_cast<double*>(phi0), rhs0, m * m, m, lv));
-  k_resmax<<<mg_blocks((long)c.n * c.n * c.n), MG_TPB, 0, s>>>(lv[0], out, &c.sc->ticket,
-                                                               &c.sc->red[5]);
+  WF_CK(launch_k(k_resmax, mg_blocks((long)c.n * c.n * c.n), MG_TPB, 0, s, lv[0], out, &c.sc->ticket,
+                                                               &c.sc->red[5]));
   WF_CKL("k_resmax");
   return WF_OK;
 }
@@ -1732,17 +1781,17 @@ static int vcycle_fixed(Lvl<double>* lv, int L, const wf_case& c, cudaStream_t s
   for (int l = 0; l < L; ++l) {
     if (l > 0) {
       const long m = (long)lv[l].n + 2;
-      k_zero<double><<<mg_blocks(m * m * m), MG_TPB, 0, s>>>(lv[l].phi, m * m * m);
+      WF_CK(launch_k(k_zero<double>, mg_blocks(m * m * m), MG_TPB, 0, s, lv[l].phi, m * m * m));
       WF_CKL("k_zero");
-      k_restrict<double><<<mg_blocks((long)lv[l].n * lv[l].n * lv[l].n), MG_TPB, 0, s>>>(
-          lv[l - 1], const_cast<double*>(lv[l].rhs), lv[l]);
+      WF_CK(launch_k(k_restrict<double>, mg_blocks((long)lv[l].n * lv[l].n * lv[l].n), MG_TPB, 0, s, 
+          lv[l - 1], const_cast<double*>(lv[l].rhs), lv[l]));
       WF_CKL("k_restrict");
     }
     WF_TRY(relax(lv[l], l < L - 1 ? c.n_pre : c.n_coarse, s));
   }
   for (int l = L - 2; l >= 0; --l) {
-    k_prolong<double><<<mg_blocks((long)lv[l].n * lv[l].n * lv[l].n), MG_TPB, 0, s>>>(
-        lv[l + 1], lv[l]);
+    WF_CK(launch_k(k_prolong<double>, mg_blocks((long)lv[l].n * lv[l].n * lv[l].n), MG_TPB, 0, s, 
+        lv[l + 1], lv[l]));
     WF_CKL("k_prolong");
     WF_TRY(relax(lv[l], c.n_post, s));
   }
@@ -1804,7 +1853,7 @@ int mg_solve_noalloc(const double* su, double* pp, int n, int nlev, double dx, d
   c.n_post = 6;
   c.n_coarse = 300;
   c.n_vcycles = 4;
-  k_zero<double><<<mg_blocks(P * P * P), MG_TPB, 0, s>>>(pp, P * P * P);
+  WF_CK(launch_k(k_zero<double>, mg_blocks(P * P * P), MG_TPB, 0, s, pp, P * P * P));
   WF_CKL("k_zero pp");
   for (int cyc = 0; cyc < c.n_vcycles; ++cyc) WF_TRY(vcycle_fixed(lv, nlev, c, s));
   return WF_OK;

@@ -42,6 +42,7 @@ static inline int nblocks(long work, int tpb = TPB, int cap = 148 * 16) {
 // scalar block
 // --------------------------------------------------------------------------
 __global__ void k_scalars_init(wf_scalars* sc, double dt0) {
+  pdl_entry();
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   sc->dt = dt0;
   sc->ctime = 0.0;
@@ -66,7 +67,7 @@ __global__ void k_scalars_init(wf_scalars* sc, double dt0) {
 
 int launch_scalars_init(wf_scalars* sc, double dt0, cudaStream_t s) {
   if (!sc) return fail(WF_EINVAL, "null scalar block");
-  k_scalars_init<<<1, 32, 0, s>>>(sc, dt0);
+  WF_CK(launch_k(k_scalars_init, 1, 32, 0, s, sc, dt0));
   WF_CKL("k_scalars_init");
   return WF_OK;
 }
@@ -76,6 +77,7 @@ int launch_scalars_init(wf_scalars* sc, double dt0, cudaStream_t s) {
 // --------------------------------------------------------------------------
 __global__ void k_init_noise(double* u, double* v, double* w, Geo g, double amp,
                              int seed) {
+  pdl_entry();
   const long tot = (long)g.n * g.n * g.n;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
        t += (long)gridDim.x * blockDim.x) {
@@ -99,7 +101,7 @@ int launch_init_noise(double* u, double* v, double* w, int n, double amp, int se
                       cudaStream_t s) {
   if (!u || !v || !w || n < 1) return fail(WF_EINVAL, "init_noise: bad args");
   Geo g = geo_of(n);
-  k_init_noise<<<nblocks((long)n * n * n), TPB, 0, s>>>(u, v, w, g, amp, seed);
+  WF_CK(launch_k(k_init_noise, nblocks((long)n * n * n), TPB, 0, s, u, v, w, g, amp, seed));
   WF_CKL("k_init_noise");
   return WF_OK;
 }
@@ -110,6 +112,7 @@ int launch_init_noise(double* u, double* v, double* w, int n, double amp, int se
 // dt update on the device.
 // --------------------------------------------------------------------------
 __global__ void __launch_bounds__(TPB) k_checkdt(const wf_case c, Geo g) {
+  pdl_entry();
   __shared__ double sm[32];
   const double* u = c.fld[WF_U];
   const double* v = c.fld[WF_V];
@@ -180,7 +183,7 @@ __global__ void __launch_bounds__(TPB) k_checkdt(const wf_case c, Geo g) {
 
 int launch_checkdt(const wf_case& c, cudaStream_t s) {
   Geo g = geo_of(c.n);
-  k_checkdt<<<nblocks((long)c.n * c.n * c.n, TPB, 148 * 4), TPB, 0, s>>>(c, g);
+  WF_CK(launch_k(k_checkdt, nblocks((long)c.n * c.n * c.n, TPB, 148 * 4), TPB, 0, s, c, g));
   WF_CKL("k_checkdt");
   return WF_OK;
 }
@@ -192,6 +195,7 @@ __global__ void k_copy3(const double2* __restrict__ a0, double2* __restrict__ b0
                         const double2* __restrict__ a1, double2* __restrict__ b1,
                         const double2* __restrict__ a2, double2* __restrict__ b2,
                         long n2) {
+  pdl_entry();
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n2;
        t += (long)gridDim.x * blockDim.x) {
     b0[t] = __ldg(a0 + t);
@@ -201,6 +205,7 @@ __global__ void k_copy3(const double2* __restrict__ a0, double2* __restrict__ b0
 }
 __global__ void k_copy_tail(const double* a0, double* b0, const double* a1, double* b1,
                             const double* a2, double* b2, long idx) {
+  pdl_entry();
   b0[idx] = a0[idx];
   b1[idx] = a1[idx];
   b2[idx] = a2[idx];
@@ -209,13 +214,13 @@ __global__ void k_copy_tail(const double* a0, double* b0, const double* a1, doub
 int launch_copy_oo(const wf_case& c, cudaStream_t s) {
   const long tot = padded(c.n) * padded(c.n) * padded(c.n);
   const long n2 = tot / 2;
-  k_copy3<<<nblocks(n2, TPB, 148 * 8), TPB, 0, s>>>(
+  WF_CK(launch_k(k_copy3, nblocks(n2, TPB, 148 * 8), TPB, 0, s, 
       (const double2*)c.fld[WF_U], (double2*)c.fld[WF_UOO], (const double2*)c.fld[WF_V],
-      (double2*)c.fld[WF_VOO], (const double2*)c.fld[WF_W], (double2*)c.fld[WF_WOO], n2);
+      (double2*)c.fld[WF_VOO], (const double2*)c.fld[WF_W], (double2*)c.fld[WF_WOO], n2));
   WF_CKL("k_copy3");
   if (tot & 1) {
-    k_copy_tail<<<1, 1, 0, s>>>(c.fld[WF_U], c.fld[WF_UOO], c.fld[WF_V], c.fld[WF_VOO],
-                                c.fld[WF_W], c.fld[WF_WOO], tot - 1);
+    WF_CK(launch_k(k_copy_tail, 1, 1, 0, s, c.fld[WF_U], c.fld[WF_UOO], c.fld[WF_V], c.fld[WF_VOO],
+                                c.fld[WF_W], c.fld[WF_WOO], tot - 1));
     WF_CKL("k_copy_tail");
   }
   return WF_OK;
@@ -225,6 +230,7 @@ int launch_copy_oo(const wf_case& c, cudaStream_t s) {
 // WALE eddy viscosity (kernels.py:297-367)
 // --------------------------------------------------------------------------
 __global__ void __launch_bounds__(TPB) k_wale(const wf_case c, Geo g) {
+  pdl_entry();
   const double* u = c.fld[WF_U];
   const double* v = c.fld[WF_V];
   const double* w = c.fld[WF_W];
@@ -276,10 +282,14 @@ __global__ void __launch_bounds__(TPB) k_wale(const wf_case c, Geo g) {
     const double syz = 0.5 * (dvdz + dwdy);
     const double ss = dudx * dudx + dvdy * dvdy + dwdz * dwdz +
                       2.0 * (sxy * sxy + sxz * sxz + syz * syz);
+    // kernels.py:362-365 with x^1.5 = x sqrt(x), x^2.5 = x^2 sqrt(x) and
+    // x^1.25 = x sqrt(sqrt(x)) (correctly rounded sqrt; a few ulp from pow)
     double nut = 0.0;
     if (sdsd > 1.0e-8) {
-      const double sdsd15 = pow(sdsd, 1.5);
-      const double denom = pow(fabs(ss), 2.5) + pow(sdsd, 1.25);
+      const double rs = sqrt(sdsd);
+      const double sdsd15 = sdsd * rs;
+      const double as = fabs(ss);
+      const double denom = as * as * sqrt(as) + sdsd * sqrt(rs);
       nut = ls * ls * sdsd15 / denom;
     }
     vis[id] = c.rrey + nut;
@@ -288,6 +298,7 @@ __global__ void __launch_bounds__(TPB) k_wale(const wf_case c, Geo g) {
 
 // vis = 1/Re on real cells (kernels.py:442-449)
 __global__ void k_fill_real(double* f, Geo g, double val) {
+  pdl_entry();
   const long tot = (long)g.n * g.n * g.n;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
        t += (long)gridDim.x * blockDim.x) {
@@ -302,12 +313,12 @@ int launch_wale(const wf_case& c, cudaStream_t s) {
   Geo g = geo_of(c.n);
   const long tot = (long)c.n * c.n * c.n;
   if (c.sgs) {
-    k_wale<<<nblocks(tot), TPB, 0, s>>>(c, g);
+    WF_CK(launch_k(k_wale, nblocks(tot), TPB, 0, s, c, g));
     WF_CKL("k_wale");
     FillReq r{c.fld[WF_VIS], FILL_VIS, c.rrey};
     return launch_fills(&r, 1, c.n, s);
   }
-  k_fill_real<<<nblocks(tot), TPB, 0, s>>>(c.fld[WF_VIS], g, c.rrey);
+  WF_CK(launch_k(k_fill_real, nblocks(tot), TPB, 0, s, c.fld[WF_VIS], g, c.rrey));
   WF_CKL("k_fill_real");
   return WF_OK;
 }
@@ -331,6 +342,7 @@ __device__ __forceinline__ void op_dims(int comp, int n, int& ni, int& nj, int& 
 template <int COMP>
 __global__ void __launch_bounds__(TPB) k_conv(const wf_case c, Geo g, double alpha,
                                              const double* __restrict__ dtp) {
+  pdl_entry();
   const double* u = c.fld[WF_U];
   const double* v = c.fld[WF_V];
   const double* w = c.fld[WF_W];
@@ -417,6 +429,7 @@ __device__ __forceinline__ double lap1(const double* f, long id, long s, double 
 template <int COMP>
 __global__ void __launch_bounds__(TPB) k_diff(const wf_case c, Geo g, double alpha,
                                              const double* __restrict__ dtp) {
+  pdl_entry();
   const double* f = c.fld[WF_U + COMP];
   const double* vis = c.fld[WF_VIS];
   double* star = c.fld[WF_USTAR + COMP];
@@ -442,9 +455,9 @@ int launch_conv(const wf_case& c, int comp, double alpha, const double* dt,
   Geo g = geo_of(c.n);
   const long tot = (long)c.n * c.n * (c.n - 1);
   const int nb = nblocks(tot);
-  if (comp == 0) k_conv<0><<<nb, TPB, 0, s>>>(c, g, alpha, dt);
-  else if (comp == 1) k_conv<1><<<nb, TPB, 0, s>>>(c, g, alpha, dt);
-  else if (comp == 2) k_conv<2><<<nb, TPB, 0, s>>>(c, g, alpha, dt);
+  if (comp == 0) WF_CK(launch_k(k_conv<0>, nb, TPB, 0, s, c, g, alpha, dt));
+  else if (comp == 1) WF_CK(launch_k(k_conv<1>, nb, TPB, 0, s, c, g, alpha, dt));
+  else if (comp == 2) WF_CK(launch_k(k_conv<2>, nb, TPB, 0, s, c, g, alpha, dt));
   else return fail(WF_EINVAL, "conv: comp must be 0, 1 or 2");
   WF_CKL("k_conv");
   return WF_OK;
@@ -455,9 +468,9 @@ int launch_diff(const wf_case& c, int comp, double alpha, const double* dt,
   Geo g = geo_of(c.n);
   const long tot = (long)c.n * c.n * (c.n - 1);
   const int nb = nblocks(tot);
-  if (comp == 0) k_diff<0><<<nb, TPB, 0, s>>>(c, g, alpha, dt);
-  else if (comp == 1) k_diff<1><<<nb, TPB, 0, s>>>(c, g, alpha, dt);
-  else if (comp == 2) k_diff<2><<<nb, TPB, 0, s>>>(c, g, alpha, dt);
+  if (comp == 0) WF_CK(launch_k(k_diff<0>, nb, TPB, 0, s, c, g, alpha, dt));
+  else if (comp == 1) WF_CK(launch_k(k_diff<1>, nb, TPB, 0, s, c, g, alpha, dt));
+  else if (comp == 2) WF_CK(launch_k(k_diff<2>, nb, TPB, 0, s, c, g, alpha, dt));
   else return fail(WF_EINVAL, "diff: comp must be 0, 1 or 2");
   WF_CKL("k_diff");
   return WF_OK;
@@ -468,6 +481,7 @@ int launch_diff(const wf_case& c, int comp, double alpha, const double* dt,
 // --------------------------------------------------------------------------
 __global__ void __launch_bounds__(TPB) k_calvel(const wf_case c, Geo g, double alpha,
                                                const double* __restrict__ dtp) {
+  pdl_entry();
   const double* p = c.fld[WF_P];
   const double dt = *dtp;
   const long tot = (long)g.n * g.n * g.n;
@@ -490,7 +504,7 @@ __global__ void __launch_bounds__(TPB) k_calvel(const wf_case c, Geo g, double a
 
 int launch_calvel(const wf_case& c, double alpha, const double* dt, cudaStream_t s) {
   Geo g = geo_of(c.n);
-  k_calvel<<<nblocks((long)c.n * c.n * c.n), TPB, 0, s>>>(c, g, alpha, dt);
+  WF_CK(launch_k(k_calvel, nblocks((long)c.n * c.n * c.n), TPB, 0, s, c, g, alpha, dt));
   WF_CKL("k_calvel");
   return WF_OK;
 }
@@ -502,6 +516,7 @@ int launch_calvel(const wf_case& c, double alpha, const double* dt, cudaStream_t
 __global__ void __launch_bounds__(TPB) k_calmas(const wf_case c, Geo g,
                                                unsigned long long h_if,
                                                unsigned long long h_loop) {
+  pdl_entry();
   __shared__ double sm[32];
   const double* u = c.fld[WF_U];
   const double* v = c.fld[WF_V];
@@ -553,7 +568,7 @@ __global__ void __launch_bounds__(TPB) k_calmas(const wf_case c, Geo g,
 int launch_calmas(const wf_case& c, unsigned long long h_if, unsigned long long h_loop,
                   cudaStream_t s) {
   Geo g = geo_of(c.n);
-  k_calmas<<<nblocks((long)c.n * c.n * c.n, TPB, 148 * 4), TPB, 0, s>>>(c, g, h_if, h_loop);
+  WF_CK(launch_k(k_calmas, nblocks((long)c.n * c.n * c.n, TPB, 148 * 4), TPB, 0, s, c, g, h_if, h_loop));
   WF_CKL("k_calmas");
   return WF_OK;
 }
@@ -562,6 +577,7 @@ int launch_calmas(const wf_case& c, unsigned long long h_if, unsigned long long 
 // p += pp over real cells plus one ring (kernels.py:405-414)
 // --------------------------------------------------------------------------
 __global__ void k_add_ring(double* p, const double* pp, Geo g) {
+  pdl_entry();
   const int m = g.n + 2;
   const long tot = (long)m * m * m;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
@@ -576,7 +592,7 @@ __global__ void k_add_ring(double* p, const double* pp, Geo g) {
 
 int launch_add_ring(double* p, const double* pp, int n, cudaStream_t s) {
   Geo g = geo_of(n);
-  k_add_ring<<<nblocks((long)(n + 2) * (n + 2) * (n + 2)), TPB, 0, s>>>(p, pp, g);
+  WF_CK(launch_k(k_add_ring, nblocks((long)(n + 2) * (n + 2) * (n + 2)), TPB, 0, s, p, pp, g));
   WF_CKL("k_add_ring");
   return WF_OK;
 }

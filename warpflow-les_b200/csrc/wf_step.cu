@@ -13,6 +13,7 @@
 // calmas kernel's last block sets both conditions on the device, so a
 // whole step is one graph launch with no host round trip.
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 
@@ -22,6 +23,15 @@ namespace wf {
 
 static thread_local std::string g_err;
 thread_local long g_launches = 0;
+
+bool pdl_enabled() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("WF_PDL");
+    v = (e && e[0] == '0') ? 0 : 1;
+  }
+  return v == 1;
+}
 
 void set_error(const std::string& msg) { g_err = msg; }
 int fail(int code, const std::string& msg) {

@@ -3,7 +3,8 @@
 For each level size it times the implementations of libwfb200 (0: one CTA
 with the level in shared memory; 1: a thread-block cluster with a cluster
 barrier per half-sweep; 2: a cluster with point-to-point halo pushes; 3: the
-same with two halo planes and one exchange per sweep) on a 300-sweep relax
+same with two halo planes and one exchange per sweep; 4: point-to-point
+with thinner slabs, clusters of up to 16 CTAs) on a 300-sweep relax
 and installs the fastest through
 ``wf_set_coarse_strategy``.  Results can be cached as JSON and re-applied.
 The library's built-in table is the same measurement taken on a B200.
@@ -24,6 +25,7 @@ from .topology import build_topology
 SIZES = (6, 8, 10, 12, 14, 16, 20, 24, 28, 32)
 CLUSTER_SIZES = set(SIZES)   # sizes with cluster kernels
 TB_SIZES = {8, 10, 12, 14, 16, 20, 24, 28, 32}
+THIN_SIZES = {12, 16, 20, 24, 28, 32}
 SMEM_SIZES = {4, 8, 12, 16, 20, 24}
 
 
@@ -56,9 +58,9 @@ def tune(sizes=SIZES, sweeps=300, device="cuda:0"):
         mg = Multigrid(cfg, build_topology(cfg), device, 1.0 / n, 1.0 / n, 1.0 / n)
         lev = mg.levels[0]
         lev.rhs.assign(np.random.default_rng(n).standard_normal(lev.shape))
-        cands = [s for s in (0, 1, 2, 3)
+        cands = [s for s in (0, 1, 2, 3, 4)
                  if (s == 0 and n in SMEM_SIZES) or (s in (1, 2) and n in CLUSTER_SIZES)
-                 or (s == 3 and n in TB_SIZES)]
+                 or (s == 3 and n in TB_SIZES) or (s == 4 and n in THIN_SIZES)]
         times = {}
         for s in cands:
             set_strategy(n, s)
