@@ -219,7 +219,7 @@ def bench_serve(args):
     from warpflow.serve import CavityServer, poisson_stream
     reqs = poisson_stream(count=args.requests, rate=20.0, seed=0,
                           step_scale=args.step_scale)
-    srv = CavityServer(budget_bytes=150 * 10 ** 9, nstreams=16)
+    srv = CavityServer(budget_bytes=150 * 10 ** 9, nstreams=args.streams)
     srv.run(reqs)
     s = srv.summary()
     print(json.dumps({
@@ -229,7 +229,7 @@ def bench_serve(args):
         "wall_s": round(s["wall_s"], 2), "step_batches": s["step_batches"],
         "peak_resident_GB": round(s["peak_resident_bytes"] / 1e9, 3),
         "config": {"requests": args.requests, "rate_per_s": 20.0, "seed": 0,
-                   "step_scale": args.step_scale, "budget_GB": 150,
+                   "step_scale": args.step_scale, "budget_GB": 150, "streams": args.streams,
                    "latency": "arrival to end of last step, wall clock"}}), flush=True)
 
 

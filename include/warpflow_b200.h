@@ -200,7 +200,12 @@ typedef struct wf_stepper wf_stepper;
 /* Build the per-case step as one CUDA graph (device-side dt control and a
  * device-driven projection loop through conditional graph nodes).  `c` is
  * copied.  mode 0 = graph, 1 = plain stream launches with host-driven
- * projection loop (one 8-byte readback per outer iteration). */
+ * projection loop (one 8-byte readback per outer iteration).  OR-ing
+ * WF_STEP_SERIAL into the mode launches every kernel of the step without
+ * programmatic dependent launch: a kernel's CTAs then become resident only
+ * after its predecessor finished, which frees SMs for other streams when
+ * many steppers run concurrently (ensembles, serving). */
+#define WF_STEP_SERIAL 2
 WF_API int wf_stepper_create(const wf_case* c, int32_t mode, wf_stepper** out);
 /* One FlowSolver.step(): enqueue the step on `stream`.  No host sync. */
 WF_API int wf_stepper_step(wf_stepper* s, void* stream);

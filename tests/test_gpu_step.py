@@ -47,6 +47,20 @@ def test_step_matches_reference_golden(tag, mode):
                 assert d <= 1e-10, (tag, s, name, d)
 
 
+def test_serial_stepper_bit_identical():
+    """A stepper built without programmatic dependent launch (the form
+    ensembles and the server use) computes exactly the same step."""
+    from warpflow import FlowSolver, build_topology
+    cfg = make_cfg(24, levels=3)
+    a = _solver(cfg)
+    b = FlowSolver(cfg, build_topology(cfg), "cuda:0", serial=True)
+    for _ in range(3):
+        ra, rb = a.step(), b.step()
+        assert ra == rb
+    for name in FIELDS:
+        np.testing.assert_array_equal(a.f[name].numpy(), b.f[name].numpy())
+
+
 def _compare_run(cfg, nsteps, check_every=1):
     sol = _solver(cfg)
     ora = O.OracleSolver(cfg)

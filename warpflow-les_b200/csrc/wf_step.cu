@@ -23,6 +23,8 @@ namespace wf {
 
 static thread_local std::string g_err;
 thread_local long g_launches = 0;
+// Set while a stepper created with WF_STEP_SERIAL captures or launches.
+static thread_local int g_pdl_off = 0;
 
 bool pdl_enabled() {
   static int v = -1;
@@ -30,8 +32,15 @@ bool pdl_enabled() {
     const char* e = getenv("WF_PDL");
     v = (e && e[0] == '0') ? 0 : 1;
   }
-  return v == 1;
+  return v == 1 && !g_pdl_off;
 }
+
+// Turns programmatic dependent launch off on this thread for one scope.
+struct PdlOff {
+  int prev;
+  explicit PdlOff(bool on) : prev(g_pdl_off) { if (on) g_pdl_off = 1; }
+  ~PdlOff() { g_pdl_off = prev; }
+};
 
 void set_error(const std::string& msg) { g_err = msg; }
 int fail(int code, const std::string& msg) {
@@ -107,7 +116,8 @@ using namespace wf;
 
 struct wf_stepper {
   wf_case c;
-  int mode;
+  int mode;     // 0 graph, 1 host loop
+  int serial;   // WF_STEP_SERIAL: no programmatic dependent launch
   int32_t counts[4];  // launches: prologue, calmas pass, multigrid part, epilogue
   cudaGraph_t graph;
   cudaGraphExec_t exec;
@@ -336,16 +346,19 @@ int wf_stepper_create(const wf_case* c, int32_t mode, wf_stepper** out) {
   if (!c || !out) return fail(WF_EINVAL, "null argument");
   *out = nullptr;
   WF_TRY(validate_case(*c));
-  if (mode != 0 && mode != 1) return fail(WF_EINVAL, "mode must be 0 (graph) or 1 (host loop)");
+  if (mode & ~(1 | WF_STEP_SERIAL))
+    return fail(WF_EINVAL, "mode must be 0 (graph) or 1 (host loop), optionally | WF_STEP_SERIAL");
   wf_stepper* st = new wf_stepper();
   st->c = *c;
-  st->mode = mode;
+  st->mode = mode & 1;
+  st->serial = (mode & WF_STEP_SERIAL) != 0;
+  PdlOff guard(st->serial);
   st->graph = nullptr;
   st->exec = nullptr;
   st->hflag = nullptr;
   for (int i = 0; i < 4; ++i) st->counts[i] = 0;
   int rc = WF_OK;
-  if (mode == 0) {
+  if (st->mode == 0) {
     rc = build_graph(st);
   } else {
     cudaError_t e = cudaMallocHost((void**)&st->hflag, sizeof(int32_t));
@@ -367,6 +380,7 @@ int wf_stepper_step(wf_stepper* st, void* stream) {
     return WF_OK;
   }
   const wf_case& c = st->c;
+  PdlOff guard(st->serial);
   long l0 = g_launches;
   WF_TRY(step_prologue(c, s));
   st->counts[0] = (int32_t)(g_launches - l0);

@@ -67,7 +67,10 @@ class Ensemble:
 
     def __init__(self, cfgs, device="cuda:0", nstreams=16):
         self.device = cuda_device(device)
-        self.solvers = [FlowSolver(cfg, build_topology(cfg), self.device) for cfg in cfgs]
+        # Concurrent cases: kernels that wait for their predecessor while
+        # resident would hold SMs other streams could use.
+        self.solvers = [FlowSolver(cfg, build_topology(cfg), self.device,
+                                   serial=nstreams > 1) for cfg in cfgs]
         self.active = [True] * len(self.solvers)
         ns = max(1, min(nstreams, len(self.solvers)))
         self.streams = [torch.cuda.Stream(self.device) for _ in range(ns)]

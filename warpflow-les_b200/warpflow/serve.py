@@ -170,7 +170,8 @@ class CavityServer:
     def _build(self, req):
         cfg = cavity_case(req.n, req.re, req.ulid, levels=req.levels,
                           precision=req.precision, name="req%d" % req.rid)
-        return FlowSolver(cfg, build_topology(cfg), self.device)
+        return FlowSolver(cfg, build_topology(cfg), self.device,
+                          serial=len(self.streams) > 1)
 
     def run(self, requests, time_scale=1.0):
         """Serve `requests` (arrival times in seconds, compressed by

@@ -29,10 +29,15 @@ from .topology import NPL
 ALFARK = (0.5, 1.0)  # Heun RK2 stage coefficients (reference solver.py:26)
 
 STEP_MODES = {"graph": 0, "host": 1}
+STEP_SERIAL = 2   # WF_STEP_SERIAL: no programmatic dependent launch
 
 
 class FlowSolver:
-    def __init__(self, cfg, topo, device, step_mode=None):
+    def __init__(self, cfg, topo, device, step_mode=None, serial=False):
+        """`serial=True` builds the step without programmatic dependent
+        launch (each kernel's CTAs wait for the previous kernel to finish
+        before becoming resident); use it when many solvers step
+        concurrently on one GPU."""
         self.cfg = cfg
         self.topo = topo
         dev = cuda_device(device)
@@ -86,7 +91,9 @@ class FlowSolver:
             raise ValueError("step_mode must be one of %s" % sorted(STEP_MODES))
         self.step_mode = mode
         self._stepper = ctypes.c_void_p()
-        _abi.call("wf_stepper_create", ctypes.byref(self.case), STEP_MODES[mode],
+        self.serial = bool(serial)
+        _abi.call("wf_stepper_create", ctypes.byref(self.case),
+                  STEP_MODES[mode] | (STEP_SERIAL if serial else 0),
                   ctypes.byref(self._stepper))
 
     # ------------------------------------------------------------------ #
