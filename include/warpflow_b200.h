@@ -101,9 +101,10 @@ typedef struct wf_case {
   double* fld[WF_NFIELDS];        /* (n+6)^3 each, order of enum wf_field */
   void* mg_phi[WF_MAX_LEVELS];    /* level l >= 1 (entry 0 unused in FP64) */
   void* mg_rhs[WF_MAX_LEVELS];    /* level l >= 1; in FP32 mode entry 0 is the FP32 level-0 pair */
-  void* mg_tmp[WF_MAX_LEVELS];    /* optional (n_l+2)^3 second buffer per level (level 0
-                                     included, element type of the level): with it a whole
-                                     red-black sweep is one launch; NULL = two launches */
+  void* mg_tmp[WF_MAX_LEVELS];    /* optional scratch of 2*(n_l+2)^3 elements per level
+                                     (level 0 included, element type of the level): large
+                                     levels relax on row-parity-split copies of phi and rhs
+                                     held there; NULL = relax in place */
   wf_scalars* sc;                 /* device scalar block */
 } wf_case;
 

@@ -1,6 +1,9 @@
-"""One-launch red-black sweeps (used by default for levels >= 128) forced
-on at small sizes in a child process: multigrid solves must match the FP64
-oracle, and the mixed form must stay within its tolerance."""
+"""The alternative fine-level relax paths forced on at small sizes in child
+processes -- sweeps on row-parity-split copies (used by default for large
+levels) and one-launch red-black sweeps (off by default): multigrid solves
+must match the FP64 oracle, the mixed form must stay within its tolerance,
+and every result must be bit-identical to the in-place one-colour path."""
+import hashlib
 import json
 import os
 import subprocess
@@ -13,7 +16,7 @@ from conftest import PKG, ROOT
 pytestmark = pytest.mark.gpu
 
 SCRIPT = r"""
-import json, sys
+import hashlib, json, sys
 sys.path[:0] = [%r, %r]
 import numpy as np
 from oracle import wf_oracle as O
@@ -34,6 +37,7 @@ for n, L, prec in ((20, 2, "fp64"), (24, 3, "fp64"), (40, 3, "fp64"), (40, 3, "m
     ref = np.zeros(shape)
     O.Multigrid(n, L, h, h, h).solve(rhs, ref, n)
     out["%%d_%%d_%%s" %% (n, L, prec)] = float(np.abs(pp.numpy() - ref).max() / np.abs(ref).max())
+    out["hash_%%d_%%d_%%s" %% (n, L, prec)] = hashlib.sha1(pp.numpy().tobytes()).hexdigest()
     # harness relax with an odd sweep count on level 0 (fp64 only)
     if prec == "fp64":
         lev = mg.levels[0]
@@ -45,16 +49,36 @@ for n, L, prec in ((20, 2, "fp64"), (24, 3, "fp64"), (40, 3, "fp64"), (40, 3, "m
         for _ in range(5):
             O.rbgs(ol, 0); O.rbgs(ol, 1); O.mg_refill(ol.phi, n)
         out["relax_%%d" %% n] = float(np.abs(lev.phi.numpy() - ol.phi).max() / np.abs(ol.phi).max())
+        out["hash_relax_%%d" %% n] = hashlib.sha1(lev.phi.numpy().tobytes()).hexdigest()
 print(json.dumps(out))
 """ % (ROOT, PKG)
 
 
-def test_one_launch_sweeps_match_oracle():
-    env = dict(os.environ, WF_SWEEP2_MIN="8")
+OFF = str(1 << 30)
+
+
+def _run(env_extra):
+    env = dict(os.environ, **env_extra)
     r = subprocess.run([sys.executable, "-c", SCRIPT], capture_output=True, text=True,
                        env=env, timeout=600)
     assert r.returncode == 0, r.stderr[-3000:]
-    res = json.loads(r.stdout.strip().splitlines()[-1])
-    for key, rel in res.items():
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+@pytest.fixture(scope="module")
+def in_place():
+    return _run({"WF_SPLIT_MIN": OFF, "WF_SWEEP2_MIN": OFF})
+
+
+@pytest.mark.parametrize("env", [{"WF_SPLIT_MIN": "8", "WF_SWEEP2_MIN": OFF},
+                                 {"WF_SPLIT_MIN": OFF, "WF_SWEEP2_MIN": "8"}],
+                         ids=["split", "one_launch"])
+def test_relax_paths_match_oracle_and_in_place(env, in_place):
+    res = _run(env)
+    for key, val in res.items():
+        if key.startswith("hash_"):
+            assert val == in_place[key], key
+            continue
         tol = 1e-5 if key.endswith("mixed") else 1e-11
-        assert rel <= tol, (key, rel)
+        assert val <= tol, (key, val)
+        assert in_place[key] <= tol, (key, in_place[key])

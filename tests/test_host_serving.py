@@ -71,8 +71,8 @@ def test_case_bytes_formula():
     n = 80
     f = 13 * 86 ** 3 * 8
     vol = 82 ** 3 + 42 ** 3 + 22 ** 3
-    mg64 = 2 * 8 * vol + 8 * vol          # phi, rhs + sweep buffer
-    mg32 = 2 * 4 * vol + 4 * vol
+    mg64 = 2 * 8 * vol + 2 * 8 * vol      # phi, rhs + two-array scratch
+    mg32 = 2 * 4 * vol + 2 * 4 * vol
     assert case_bytes(n, 3, "fp64") - f - mg64 < 4096
     assert case_bytes(n, 3, "mixed") - f - 2 * 8 * vol - mg32 < 4096
 

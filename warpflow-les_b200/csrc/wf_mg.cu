@@ -40,7 +40,7 @@ struct Lvl {
   long sI, sJ;   // strides (k stride 1)
   T ax, ay, az;  // 1/h^2 per axis of this level
   int* err;      // where a device-side wait records a timeout (may be null)
-  T* tmp;        // second buffer for one-launch sweeps (may be null)
+  T* tmp;        // scratch of two level arrays: split copies / one-launch sweeps (may be null)
   long tI, tJ;   // its strides
   unsigned* gbar;  // two words of grid-barrier state (may be null)
 };
@@ -1073,6 +1073,192 @@ static int try_coarse_cluster(const Lvl<T>& L, int nsweeps, cudaStream_t s, int*
   }
 }
 
+// ---- red-black sweeps on a row-parity-split copy (large levels) -----------
+// A large level relaxes on a scratch copy whose rows are stored split by the
+// parity of the array index a = k+1: position of a in its row is
+// (a&1)*H + (a>>1), H = (n+2)/2.  Within a row the cells of one colour then
+// form one contiguous half-row, so a half-sweep reads the other colour (half
+// the level), the rhs of its own colour (from a split copy of rhs) and writes
+// its own colour: 1.5 words per cell, against 3 words of whole cache lines in
+// the interleaved layout.  Every cell keeps k_rbgs's arithmetic (same terms,
+// same order, division by ap), so results are bit-identical to it.  The copy
+// has the ring of the original (face-ring values only ever meet a zero
+// coefficient); copying back writes the real cells and their face-ring
+// mirrors, which is what k_rbgs leaves in the ring after the last sweep.
+__device__ __forceinline__ int spos(int a, int H) { return (a & 1) * H + (a >> 1); }
+
+constexpr int SPLIT_ROWS = 8;  // rows (one warp each) per CTA
+
+// level phi (all (n+2)^3 cells) and rhs -> split copies sp, sr (dense strides)
+template <class T>
+__global__ void __launch_bounds__(32 * SPLIT_ROWS)
+    k_split_in(const Lvl<T> L, T* __restrict__ sp, T* __restrict__ sr) {
+  pdl_entry();
+  const int m = L.n + 2, H = m >> 1;
+  const int row = blockIdx.x * SPLIT_ROWS + (threadIdx.x >> 5);
+  if (row >= m * m) return;
+  const int i = row / m, j = row - i * m;
+  const long src = (long)i * L.sI + (long)j * L.sJ;
+  const long dst = (long)i * L.tI + (long)j * L.tJ;
+  for (int a = threadIdx.x & 31; a < m; a += 32) {
+    const int q = spos(a, H);
+    sp[dst + q] = L.phi[src + a];
+    sr[dst + q] = L.rhs[src + a];
+  }
+}
+
+// x / d, correctly rounded, from y = RN(1/d): one residual correction makes
+// the quotient faithful, a second rounds it correctly (P. Markstein,
+// "Computation of elementary functions on the IBM RISC System/6000
+// processor", IBM J. Res. Dev. 34(1), 1990).  Valid away from overflow and
+// underflow, which the multigrid's values stay far from; four FMAs and a
+// multiply in place of a full division.
+template <class T>
+__device__ __forceinline__ T div_by_recip(T x, T d, T y) {
+  T q = x * y;
+  T r = fma(-q, d, x);
+  q = fma(r, y, q);
+  r = fma(-q, d, x);
+  return fma(r, y, q);
+}
+
+// RN(1/ap) for every boundary pattern of a cell: index 9*cx + 3*cy + cz,
+// c = number of non-zero coefficients along the axis (0, 1 or 2).  ap is
+// summed in the kernels' order; zero terms do not change an IEEE sum, so
+// the pattern counts fix ap exactly.
+template <class T>
+struct ApRecip {
+  T y[27];
+};
+
+template <class T>
+static ApRecip<T> ap_recip(const Lvl<T>& L) {
+  ApRecip<T> t;
+  for (int cx = 0; cx < 3; ++cx)
+    for (int cy = 0; cy < 3; ++cy)
+      for (int cz = 0; cz < 3; ++cz) {
+        const T aw = cx > 0 ? L.ax : T(0), ae = cx > 1 ? L.ax : T(0);
+        const T as = cy > 0 ? L.ay : T(0), an = cy > 1 ? L.ay : T(0);
+        const T ab = cz > 0 ? L.az : T(0), at = cz > 1 ? L.az : T(0);
+        const T ap = -(aw + ae + as + an + ab + at);
+        t.y[9 * cx + 3 * cy + cz] = ap != T(0) ? T(1) / ap : T(0);
+      }
+  return t;
+}
+
+// one colour half-sweep on the split copy: a warp updates CPT runs of 32
+// consecutive cells of one colour in one real row (cells h, h+32, ...); grid
+// x = chunk of 32*CPT cells of the half-row, y = group of SPLIT_ROWS rows j,
+// z = plane i.  All loads of a thread come before its stores: a half-sweep
+// reads only the other colour and rhs, which it does not write.
+template <class T, int CPT>
+__global__ void __launch_bounds__(32 * SPLIT_ROWS)
+    k_rbgs_split(const Lvl<T> L, T* __restrict__ sp, const T* __restrict__ sr, int color,
+                 const __grid_constant__ ApRecip<T> rt) {
+  pdl_entry();
+  const int n = L.n, nh = n >> 1;
+  const int h0 = blockIdx.x * 32 * CPT + threadIdx.x;
+  const int j = blockIdx.y * SPLIT_ROWS + threadIdx.y;
+  const int i = blockIdx.z;
+  if (j >= n || h0 >= nh) return;
+  const int H = (n + 2) >> 1, tI = (int)L.tI, tJ = (int)L.tJ;
+  const int pr = (i + j + color) & 1;       // parity of a = k+1 of this row's colour
+  const long r = (long)(i + 1) * L.tI + (long)(j + 1) * L.tJ;
+  T* own = sp + r + (pr * H + 1 - pr + h0);  // a = 2*(h+1-pr) + pr
+  const T* oth = sp + r + ((1 - pr) * H + h0);  // a-1, a+1
+  const T* rr = sr + r + (pr * H + 1 - pr + h0);
+  const T aw = i > 0 ? L.ax : T(0), ae = i < n - 1 ? L.ax : T(0);
+  const T as = j > 0 ? L.ay : T(0), an = j < n - 1 ? L.ay : T(0);
+  const int pij = 9 * ((i > 0) + (i < n - 1)) + 3 * ((j > 0) + (j < n - 1));
+  T vw[CPT], ve[CPT], vs[CPT], vn[CPT], vb[CPT], vt[CPT], vr[CPT];
+#pragma unroll
+  for (int u = 0; u < CPT; ++u) {
+    if (u == 0 || h0 + 32 * u < nh) {
+      vw[u] = own[32 * u - tI];
+      ve[u] = own[32 * u + tI];
+      vs[u] = own[32 * u - tJ];
+      vn[u] = own[32 * u + tJ];
+      vb[u] = oth[32 * u];
+      vt[u] = oth[32 * u + 1];
+      vr[u] = rr[32 * u];
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < CPT; ++u) {
+    if (u == 0 || h0 + 32 * u < nh) {
+      const int k = 2 * (h0 + 32 * u) + 1 - pr;
+      const T ab = k > 0 ? L.az : T(0), at = k < n - 1 ? L.az : T(0);
+      const T ap = -(aw + ae + as + an + ab + at);
+      const T s = aw * vw[u] + ae * ve[u] + as * vs[u] + an * vn[u] + ab * vb[u] + at * vt[u];
+      own[32 * u] = div_by_recip(vr[u] - s, ap, rt.y[pij + (k > 0) + (k < n - 1)]);
+    }
+  }
+}
+
+// cells per thread of the split half-sweep (WF_SPLIT_CPT = 1, 2 or 4 overrides)
+static int split_cpt() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("WF_SPLIT_CPT");
+    v = e ? atoi(e) : 2;
+    if (v != 1 && v != 2 && v != 4) v = 2;
+  }
+  return v;
+}
+
+// split copy -> real cells of the level and their face-ring mirrors
+template <class T>
+__global__ void __launch_bounds__(32 * SPLIT_ROWS)
+    k_split_out(const Lvl<T> L, const T* __restrict__ sp) {
+  pdl_entry();
+  const int n = L.n, H = (n + 2) >> 1;
+  const int row = blockIdx.x * SPLIT_ROWS + (threadIdx.x >> 5);
+  if (row >= n * n) return;
+  const int i = row / n, j = row - i * n;
+  const long r = (long)(i + 1) * L.tI + (long)(j + 1) * L.tJ;
+  for (int k = threadIdx.x & 31; k < n; k += 32) {
+    const T x = sp[r + spos(k + 1, H)];
+    const long c = lid(L, i + 1, j + 1, k + 1);
+    L.phi[c] = x;
+    ring_mirror(L, i, j, k, c, x);
+  }
+}
+
+// smallest even level edge that relaxes on the split copy (WF_SPLIT_MIN overrides)
+static int split_min_n() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("WF_SPLIT_MIN");
+    v = e ? atoi(e) : 128;
+  }
+  return v;
+}
+
+template <class T>
+static int relax_split(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
+  const int m = L.n + 2;
+  T* sp = L.tmp;
+  T* sr = L.tmp + (long)m * m * m;
+  const int nb_all = (m * m + SPLIT_ROWS - 1) / SPLIT_ROWS;
+  const int nb = (L.n * L.n + SPLIT_ROWS - 1) / SPLIT_ROWS;
+  const int cpt = split_cpt();
+  const dim3 grid((L.n / 2 + 32 * cpt - 1) / (32 * cpt), (L.n + SPLIT_ROWS - 1) / SPLIT_ROWS,
+                  L.n);
+  const ApRecip<T> rt = ap_recip(L);
+  auto kern = cpt == 4 ? k_rbgs_split<T, 4> : cpt == 2 ? k_rbgs_split<T, 2> : k_rbgs_split<T, 1>;
+  WF_CK(launch_k(k_split_in<T>, nb_all, 32 * SPLIT_ROWS, 0, s, L, sp, sr));
+  WF_CKL("k_split_in");
+  for (int it = 0; it < nsweeps; ++it) {
+    for (int color = 0; color < 2; ++color) {
+      WF_CK(launch_k(kern, grid, dim3(32, SPLIT_ROWS), 0, s, L, sp, (const T*)sr, color, rt));
+      WF_CKL("k_rbgs_split");
+    }
+  }
+  WF_CK(launch_k(k_split_out<T>, nb, 32 * SPLIT_ROWS, 0, s, L, (const T*)sp));
+  WF_CKL("k_split_out");
+  return WF_OK;
+}
+
 // ---- one whole red-black sweep per launch (fine levels) -------------------
 // Red values depend only on the old black values, so a sweep can run as one
 // launch if every CTA reads the old state from `src` and writes the new
@@ -1437,6 +1623,7 @@ static int relax(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
     if (nsweeps > 12 && strat == 1 && try_coarse_cluster<T>(L, nsweeps, s, &rc)) return rc;
     if (try_coarse<T>(L, nsweeps, s, &rc)) return rc;
   }
+  if (L.tmp && (L.n & 1) == 0 && L.n >= split_min_n()) return relax_split<T>(L, nsweeps, s);
   if (L.tmp && nsweeps >= 2 && L.n >= sweep2_min_n()) {
     // pairs of one-launch sweeps: phi -> tmp -> phi
     const int pairs = nsweeps / 2;

@@ -97,9 +97,11 @@ class Multigrid:
             for lev in self.levels:
                 self._f32.append((DeviceField.zeros(lev.shape, self.device, torch.float32),
                                   DeviceField.zeros(lev.shape, self.device, torch.float32)))
-        # second buffer per level: a whole red-black sweep becomes one launch
+        # scratch of two level arrays per level: the row-parity-split copies
+        # of phi and rhs that large levels relax on
         dt = torch.float32 if self.precision == "mixed" else torch.float64
-        self._tmp = [DeviceField.zeros(lev.shape, self.device, dt) for lev in self.levels]
+        self._tmp = [DeviceField.zeros((2 * lev.shape[0],) + lev.shape[1:], self.device, dt)
+                     for lev in self.levels]
         self._tmp64 = self._tmp if dt == torch.float64 else None
         self.n_pre = 6       # multigrid.py:257-260
         self.n_post = 6

@@ -44,9 +44,9 @@ def case_bytes(n, levels=3, precision="mixed"):
         m = (n >> l) + 2
         mg += 2 * m ** 3 * 8
         if precision == "mixed":
-            mg += 2 * m ** 3 * 4 + m ** 3 * 4
+            mg += 2 * m ** 3 * 4 + 2 * m ** 3 * 4
         else:
-            mg += m ** 3 * 8
+            mg += 2 * m ** 3 * 8
     return fields + mg + 2 * ctypes.sizeof(_abi.WfScalars) + 8
 
 
