@@ -1092,7 +1092,7 @@ constexpr int SPLIT_ROWS = 8;  // rows (one warp each) per CTA
 // level phi (all (n+2)^3 cells) and rhs -> split copies sp, sr (dense strides)
 template <class T>
 __global__ void __launch_bounds__(32 * SPLIT_ROWS)
-    k_split_in(const Lvl<T> L, T* __restrict__ sp, T* __restrict__ sr) {
+    k_split_in(const Lvl<T> L, T* __restrict__ sp, T* __restrict__ sr, int with_rhs) {
   pdl_entry();
   const int m = L.n + 2, H = m >> 1;
   const int row = blockIdx.x * SPLIT_ROWS + (threadIdx.x >> 5);
@@ -1103,7 +1103,7 @@ __global__ void __launch_bounds__(32 * SPLIT_ROWS)
   for (int a = threadIdx.x & 31; a < m; a += 32) {
     const int q = spos(a, H);
     sp[dst + q] = L.phi[src + a];
-    sr[dst + q] = L.rhs[src + a];
+    if (with_rhs) sr[dst + q] = L.rhs[src + a];
   }
 }
 
@@ -1234,8 +1234,10 @@ static int split_min_n() {
   return v;
 }
 
+// rhs_ready: the scratch already holds the split rhs of this level (the
+// level's rhs has not changed since the last split relax of it)
 template <class T>
-static int relax_split(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
+static int relax_split(const Lvl<T>& L, int nsweeps, bool rhs_ready, cudaStream_t s) {
   const int m = L.n + 2;
   T* sp = L.tmp;
   T* sr = L.tmp + (long)m * m * m;
@@ -1246,7 +1248,7 @@ static int relax_split(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
                   L.n);
   const ApRecip<T> rt = ap_recip(L);
   auto kern = cpt == 4 ? k_rbgs_split<T, 4> : cpt == 2 ? k_rbgs_split<T, 2> : k_rbgs_split<T, 1>;
-  WF_CK(launch_k(k_split_in<T>, nb_all, 32 * SPLIT_ROWS, 0, s, L, sp, sr));
+  WF_CK(launch_k(k_split_in<T>, nb_all, 32 * SPLIT_ROWS, 0, s, L, sp, sr, rhs_ready ? 0 : 1));
   WF_CKL("k_split_in");
   for (int it = 0; it < nsweeps; ++it) {
     for (int color = 0; color < 2; ++color) {
@@ -1609,8 +1611,10 @@ static size_t smem_bytes(int n) {
 
 constexpr size_t SMEM_CAP = 220 * 1024;
 
+// rhs_ready: the level's rhs is unchanged since its last relax, so a split
+// copy of it made then can be reused
 template <class T>
-static int relax(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
+static int relax(const Lvl<T>& L, int nsweeps, cudaStream_t s, bool rhs_ready = false) {
   if (nsweeps <= 0) return WF_OK;
   // small levels with many sweeps: the column kernel
   if (nsweeps > 12 || L.n <= 24) {
@@ -1623,7 +1627,8 @@ static int relax(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
     if (nsweeps > 12 && strat == 1 && try_coarse_cluster<T>(L, nsweeps, s, &rc)) return rc;
     if (try_coarse<T>(L, nsweeps, s, &rc)) return rc;
   }
-  if (L.tmp && (L.n & 1) == 0 && L.n >= split_min_n()) return relax_split<T>(L, nsweeps, s);
+  if (L.tmp && (L.n & 1) == 0 && L.n >= split_min_n())
+    return relax_split<T>(L, nsweeps, rhs_ready, s);
   if (L.tmp && nsweeps >= 2 && L.n >= sweep2_min_n()) {
     // pairs of one-launch sweeps: phi -> tmp -> phi
     const int pairs = nsweeps / 2;
@@ -1669,8 +1674,11 @@ static int relax(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
   return WF_OK;
 }
 
+// rhs0_ready: level 0's rhs is unchanged since the previous V-cycle relaxed
+// it (a solve's V-cycles share rhs = su)
 template <class T>
-static int vcycle(std::vector<Lvl<T>>& lv, const wf_case& c, cudaStream_t s) {
+static int vcycle(std::vector<Lvl<T>>& lv, const wf_case& c, cudaStream_t s,
+                  bool rhs0_ready = false) {
   const int L = (int)lv.size();
   for (int l = 0; l < L; ++l) {
     if (l > 0) {
@@ -1682,13 +1690,14 @@ static int vcycle(std::vector<Lvl<T>>& lv, const wf_case& c, cudaStream_t s) {
           lv[l - 1], const_cast<T*>(C.rhs), C));
       WF_CKL("k_restrict");
     }
-    WF_TRY(relax(lv[l], l < L - 1 ? c.n_pre : c.n_coarse, s));
+    WF_TRY(relax(lv[l], l < L - 1 ? c.n_pre : c.n_coarse, s, l == 0 && rhs0_ready));
   }
   for (int l = L - 2; l >= 0; --l) {
     WF_CK(launch_k(k_prolong<T>, mg_blocks((long)lv[l].n * lv[l].n * lv[l].n), MG_TPB, 0, s, lv[l + 1],
                                                                                  lv[l]));
     WF_CKL("k_prolong");
-    WF_TRY(relax(lv[l], c.n_post, s));
+    // the rhs of level l is the one its pre-smoothing saw
+    WF_TRY(relax(lv[l], c.n_post, s, c.n_pre > 0 || (l == 0 && rhs0_ready)));
   }
   return WF_OK;
 }
@@ -1864,7 +1873,8 @@ int mg_solve(const wf_case& c, cudaStream_t s) {
   // multigrid.py:332-333: pp and level-0 phi start from zero
   WF_CK(launch_k(k_zero<double>, mg_blocks(P * P * P), MG_TPB, 0, s, pp, P * P * P));
   WF_CKL("k_zero pp");
-  for (int cyc = 0; cyc < c.n_vcycles; ++cyc) WF_TRY(vcycle<double>(lv, c, s));
+  for (int cyc = 0; cyc < c.n_vcycles; ++cyc)
+    WF_TRY(vcycle<double>(lv, c, s, cyc > 0 && (c.n_pre > 0 || c.n_post > 0)));
   return WF_OK;
 }
 
