@@ -98,8 +98,8 @@ def _randomise(sol, names, seed, scale=1.0):
 
 @pytest.mark.parametrize("comp", [0, 1, 2])
 @pytest.mark.parametrize("alpha", [0.5, 1.0])
-def test_conv_diff(comp, alpha):
-    n = 16
+@pytest.mark.parametrize("n", [16, 40, 72])   # one, two and three marching segments
+def test_conv_diff(comp, alpha, n):
     sol = _solver(n=n)
     sol.dt = 3.3e-4
     f = _randomise(sol, ["u", "v", "w", "uoo", "voo", "woo", "vis", "ustar", "vstar",

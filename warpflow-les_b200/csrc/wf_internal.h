@@ -41,6 +41,11 @@ inline int64_t padded(int n) { return (int64_t)n + 2 * NPL; }
 // programmatic dependent launch on (default) or off (WF_PDL=0)
 bool pdl_enabled();
 
+// one thread per cell of an ni x nj x nk box: CTAs of 32 (k) x 8 (j) threads,
+// grid z = i
+inline dim3 cells3(int ni, int nj, int nk) { return dim3((nk + 31) / 32, (nj + 7) / 8, ni); }
+inline dim3 cell_block() { return dim3(32, 8); }
+
 // launch a kernel of this library, with the programmatic-serialization
 // attribute when enabled and an optional cluster shape
 template <typename... ExpTypes, typename... ActTypes>

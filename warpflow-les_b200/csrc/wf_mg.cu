@@ -69,14 +69,14 @@ __global__ void __launch_bounds__(MG_TPB) k_rbgs(const Lvl<T> L, int color) {
   pdl_entry();
   const int n = L.n;
   const int nh = (n + 1) >> 1;
-  const long tot = (long)n * n * nh;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
-       t += (long)gridDim.x * blockDim.x) {
-    const int kk = (int)(t % nh);
-    const int j = (int)((t / nh) % n);
-    const int i = (int)(t / ((long)nh * n));
+  {  // one thread per cell: x = kk (runs of 32), y = j (groups of 8), z = i
+    const int kx_ = blockIdx.x * 32 + threadIdx.x, jy_ = blockIdx.y * 8 + threadIdx.y;
+    if (kx_ >= nh || jy_ >= n) return;
+    const int kk = kx_;
+    const int j = jy_;
+    const int i = (int)blockIdx.z;
     const int k = 2 * kk + ((1 + i + j + color) & 1);
-    if (k >= n) continue;
+    if (k >= n) return;
     const long c = lid(L, i + 1, j + 1, k + 1);
     const T aw = i > 0 ? L.ax : T(0), ae = i < n - 1 ? L.ax : T(0);
     const T as = j > 0 ? L.ay : T(0), an = j < n - 1 ? L.ay : T(0);
@@ -96,12 +96,12 @@ template <class T>
 __global__ void __launch_bounds__(MG_TPB) k_restrict(const Lvl<T> F, T* rhs_c, Lvl<T> C) {
   pdl_entry();
   const int nc = C.n, n = F.n;
-  const long tot = (long)nc * nc * nc;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
-       t += (long)gridDim.x * blockDim.x) {
-    const int ck = (int)(t % nc);
-    const int cj = (int)((t / nc) % nc);
-    const int ci = (int)(t / ((long)nc * nc));
+  {  // one thread per cell: x = ck (runs of 32), y = cj (groups of 8), z = ci
+    const int kx_ = blockIdx.x * 32 + threadIdx.x, jy_ = blockIdx.y * 8 + threadIdx.y;
+    if (kx_ >= nc || jy_ >= nc) return;
+    const int ck = kx_;
+    const int cj = jy_;
+    const int ci = (int)blockIdx.z;
     T acc = T(0);
 #pragma unroll
     for (int di = 0; di < 2; ++di)
@@ -153,12 +153,12 @@ template <class T>
 __global__ void __launch_bounds__(MG_TPB) k_prolong(const Lvl<T> C, Lvl<T> F) {
   pdl_entry();
   const int n = F.n;
-  const long tot = (long)n * n * n;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
-       t += (long)gridDim.x * blockDim.x) {
-    const int k = (int)(t % n);
-    const int j = (int)((t / n) % n);
-    const int i = (int)(t / ((long)n * n));
+  {  // one thread per cell: x = k (runs of 32), y = j (groups of 8), z = i
+    const int kx_ = blockIdx.x * 32 + threadIdx.x, jy_ = blockIdx.y * 8 + threadIdx.y;
+    if (kx_ >= n || jy_ >= n) return;
+    const int k = kx_;
+    const int j = jy_;
+    const int i = (int)blockIdx.z;
     const int c0x = (i % 2 == 0) ? i / 2 - 1 : i / 2;
     const T wx0 = (i % 2 == 0) ? T(0.25) : T(0.75);
     const int c0y = (j % 2 == 0) ? j / 2 - 1 : j / 2;
@@ -1640,9 +1640,9 @@ static int relax(const Lvl<T>& L, int nsweeps, cudaStream_t s, bool rhs_ready = 
     if (nsweeps & 1) {
       const long half = (long)L.n * L.n * ((L.n + 1) / 2);
       const int nb = mg_blocks(half);
-      WF_CK(launch_k(k_rbgs<T>, nb, MG_TPB, 0, s, L, 0));
+      WF_CK(launch_k(k_rbgs<T>, cells3(L.n, L.n, (L.n + 1) / 2), cell_block(), 0, s, L, 0));
       WF_CKL("k_rbgs");
-      WF_CK(launch_k(k_rbgs<T>, nb, MG_TPB, 0, s, L, 1));
+      WF_CK(launch_k(k_rbgs<T>, cells3(L.n, L.n, (L.n + 1) / 2), cell_block(), 0, s, L, 1));
       WF_CKL("k_rbgs");
     }
     return WF_OK;
@@ -1666,9 +1666,9 @@ static int relax(const Lvl<T>& L, int nsweeps, cudaStream_t s, bool rhs_ready = 
   const long half = (long)L.n * L.n * ((L.n + 1) / 2);
   const int nb = mg_blocks(half);
   for (int sw = 0; sw < nsweeps; ++sw) {
-    WF_CK(launch_k(k_rbgs<T>, nb, MG_TPB, 0, s, L, 0));
+    WF_CK(launch_k(k_rbgs<T>, cells3(L.n, L.n, (L.n + 1) / 2), cell_block(), 0, s, L, 0));
     WF_CKL("k_rbgs");
-    WF_CK(launch_k(k_rbgs<T>, nb, MG_TPB, 0, s, L, 1));
+    WF_CK(launch_k(k_rbgs<T>, cells3(L.n, L.n, (L.n + 1) / 2), cell_block(), 0, s, L, 1));
     WF_CKL("k_rbgs");
   }
   return WF_OK;
@@ -1686,14 +1686,14 @@ static int vcycle(std::vector<Lvl<T>>& lv, const wf_case& c, cudaStream_t s,
       const long m = (long)C.n + 2;
       WF_CK(launch_k(k_zero<T>, mg_blocks(m * m * m), MG_TPB, 0, s, C.phi, m * m * m));
       WF_CKL("k_zero");
-      WF_CK(launch_k(k_restrict<T>, mg_blocks((long)C.n * C.n * C.n), MG_TPB, 0, s, 
+      WF_CK(launch_k(k_restrict<T>, cells3(C.n, C.n, C.n), cell_block(), 0, s,
           lv[l - 1], const_cast<T*>(C.rhs), C));
       WF_CKL("k_restrict");
     }
     WF_TRY(relax(lv[l], l < L - 1 ? c.n_pre : c.n_coarse, s, l == 0 && rhs0_ready));
   }
   for (int l = L - 2; l >= 0; --l) {
-    WF_CK(launch_k(k_prolong<T>, mg_blocks((long)lv[l].n * lv[l].n * lv[l].n), MG_TPB, 0, s, lv[l + 1],
+    WF_CK(launch_k(k_prolong<T>, cells3(lv[l].n, lv[l].n, lv[l].n), cell_block(), 0, s, lv[l + 1],
                                                                                  lv[l]));
     WF_CKL("k_prolong");
     // the rhs of level l is the one its pre-smoothing saw
@@ -1980,14 +1980,14 @@ static int vcycle_fixed(Lvl<double>* lv, int L, const wf_case& c, cudaStream_t s
       const long m = (long)lv[l].n + 2;
       WF_CK(launch_k(k_zero<double>, mg_blocks(m * m * m), MG_TPB, 0, s, lv[l].phi, m * m * m));
       WF_CKL("k_zero");
-      WF_CK(launch_k(k_restrict<double>, mg_blocks((long)lv[l].n * lv[l].n * lv[l].n), MG_TPB, 0, s, 
+      WF_CK(launch_k(k_restrict<double>, cells3(lv[l].n, lv[l].n, lv[l].n), cell_block(), 0, s,
           lv[l - 1], const_cast<double*>(lv[l].rhs), lv[l]));
       WF_CKL("k_restrict");
     }
     WF_TRY(relax(lv[l], l < L - 1 ? c.n_pre : c.n_coarse, s));
   }
   for (int l = L - 2; l >= 0; --l) {
-    WF_CK(launch_k(k_prolong<double>, mg_blocks((long)lv[l].n * lv[l].n * lv[l].n), MG_TPB, 0, s, 
+    WF_CK(launch_k(k_prolong<double>, cells3(lv[l].n, lv[l].n, lv[l].n), cell_block(), 0, s, 
         lv[l + 1], lv[l]));
     WF_CKL("k_prolong");
     WF_TRY(relax(lv[l], c.n_post, s));

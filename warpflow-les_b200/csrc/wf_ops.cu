@@ -239,12 +239,12 @@ __global__ void __launch_bounds__(TPB) k_wale(const wf_case c, Geo g) {
   const double delta = pow(dx * dy * dz, 1.0 / 3.0);
   const double ls = c.cw * delta;
   const long sI = g.sI, sJ = g.sJ;
-  const long tot = (long)g.n * g.n * g.n;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
-       t += (long)gridDim.x * blockDim.x) {
-    const int k = NPL + (int)(t % g.n);
-    const int j = NPL + (int)((t / g.n) % g.n);
-    const int i = NPL + (int)(t / ((long)g.n * g.n));
+  {  // one thread per cell: x = k (runs of 32), y = j (groups of 8), z = i
+    const int kx_ = blockIdx.x * 32 + threadIdx.x, jy_ = blockIdx.y * 8 + threadIdx.y;
+    if (kx_ >= g.n || jy_ >= g.n) return;
+    const int k = NPL + kx_;
+    const int j = NPL + jy_;
+    const int i = NPL + (int)blockIdx.z;
     const long id = g.at(i, j, k);
 #define U_(a) LD(u, id + (a))
 #define V_(a) LD(v, id + (a))
@@ -313,7 +313,7 @@ int launch_wale(const wf_case& c, cudaStream_t s) {
   Geo g = geo_of(c.n);
   const long tot = (long)c.n * c.n * c.n;
   if (c.sgs) {
-    WF_CK(launch_k(k_wale, nblocks(tot), TPB, 0, s, c, g));
+    WF_CK(launch_k(k_wale, cells3(c.n, c.n, c.n), cell_block(), 0, s, c, g));
     WF_CKL("k_wale");
     FillReq r{c.fld[WF_VIS], FILL_VIS, c.rrey};
     return launch_fills(&r, 1, c.n, s);
@@ -332,7 +332,7 @@ __device__ __forceinline__ double I4(const double* f, long id, long s) {
 }
 
 // op-range dims (solver.py:99-110): the component's own axis is n-1 long
-__device__ __forceinline__ void op_dims(int comp, int n, int& ni, int& nj, int& nk) {
+__host__ __device__ __forceinline__ void op_dims(int comp, int n, int& ni, int& nj, int& nk) {
   ni = nj = nk = n;
   if (comp == 0) ni = n - 1;
   if (comp == 1) nj = n - 1;
@@ -354,11 +354,12 @@ __global__ void __launch_bounds__(TPB) k_conv(const wf_case c, Geo g, double alp
   int ni, nj, nk;
   op_dims(COMP, g.n, ni, nj, nk);
   const long tot = (long)ni * nj * nk;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
-       t += (long)gridDim.x * blockDim.x) {
-    const int k = NPL + (int)(t % nk);
-    const int j = NPL + (int)((t / nk) % nj);
-    const int i = NPL + (int)(t / ((long)nk * nj));
+  {  // one thread per cell: x = k (runs of 32), y = j (groups of 8), z = i
+    const int kx_ = blockIdx.x * 32 + threadIdx.x, jy_ = blockIdx.y * 8 + threadIdx.y;
+    if (kx_ >= nk || jy_ >= nj) return;
+    const int k = NPL + kx_;
+    const int j = NPL + jy_;
+    const int i = NPL + (int)blockIdx.z;
     const long id = g.at(i, j, k);
     double tot3;
     if (COMP == 0) {
@@ -438,11 +439,12 @@ __global__ void __launch_bounds__(TPB) k_diff(const wf_case c, Geo g, double alp
   int ni, nj, nk;
   op_dims(COMP, g.n, ni, nj, nk);
   const long tot = (long)ni * nj * nk;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
-       t += (long)gridDim.x * blockDim.x) {
-    const int k = NPL + (int)(t % nk);
-    const int j = NPL + (int)((t / nk) % nj);
-    const int i = NPL + (int)(t / ((long)nk * nj));
+  {  // one thread per cell: x = k (runs of 32), y = j (groups of 8), z = i
+    const int kx_ = blockIdx.x * 32 + threadIdx.x, jy_ = blockIdx.y * 8 + threadIdx.y;
+    if (kx_ >= nk || jy_ >= nj) return;
+    const int k = NPL + kx_;
+    const int j = NPL + jy_;
+    const int i = NPL + (int)blockIdx.z;
     const long id = g.at(i, j, k);
     const double l4 = lap1(f, id, g.sI, c.dx) + lap1(f, id, g.sJ, c.dy) + lap1(f, id, 1, c.dz);
     const double diff = LD(vis, id + vofs) * l4;
@@ -455,9 +457,12 @@ int launch_conv(const wf_case& c, int comp, double alpha, const double* dt,
   Geo g = geo_of(c.n);
   const long tot = (long)c.n * c.n * (c.n - 1);
   const int nb = nblocks(tot);
-  if (comp == 0) WF_CK(launch_k(k_conv<0>, nb, TPB, 0, s, c, g, alpha, dt));
-  else if (comp == 1) WF_CK(launch_k(k_conv<1>, nb, TPB, 0, s, c, g, alpha, dt));
-  else if (comp == 2) WF_CK(launch_k(k_conv<2>, nb, TPB, 0, s, c, g, alpha, dt));
+  int ni, nj, nk;
+  op_dims(comp, c.n, ni, nj, nk);
+  const dim3 gr = cells3(ni, nj, nk), bl = cell_block();
+  if (comp == 0) WF_CK(launch_k(k_conv<0>, gr, bl, 0, s, c, g, alpha, dt));
+  else if (comp == 1) WF_CK(launch_k(k_conv<1>, gr, bl, 0, s, c, g, alpha, dt));
+  else if (comp == 2) WF_CK(launch_k(k_conv<2>, gr, bl, 0, s, c, g, alpha, dt));
   else return fail(WF_EINVAL, "conv: comp must be 0, 1 or 2");
   WF_CKL("k_conv");
   return WF_OK;
@@ -468,9 +473,12 @@ int launch_diff(const wf_case& c, int comp, double alpha, const double* dt,
   Geo g = geo_of(c.n);
   const long tot = (long)c.n * c.n * (c.n - 1);
   const int nb = nblocks(tot);
-  if (comp == 0) WF_CK(launch_k(k_diff<0>, nb, TPB, 0, s, c, g, alpha, dt));
-  else if (comp == 1) WF_CK(launch_k(k_diff<1>, nb, TPB, 0, s, c, g, alpha, dt));
-  else if (comp == 2) WF_CK(launch_k(k_diff<2>, nb, TPB, 0, s, c, g, alpha, dt));
+  int ni, nj, nk;
+  op_dims(comp, c.n, ni, nj, nk);
+  const dim3 gr = cells3(ni, nj, nk), bl = cell_block();
+  if (comp == 0) WF_CK(launch_k(k_diff<0>, gr, bl, 0, s, c, g, alpha, dt));
+  else if (comp == 1) WF_CK(launch_k(k_diff<1>, gr, bl, 0, s, c, g, alpha, dt));
+  else if (comp == 2) WF_CK(launch_k(k_diff<2>, gr, bl, 0, s, c, g, alpha, dt));
   else return fail(WF_EINVAL, "diff: comp must be 0, 1 or 2");
   WF_CKL("k_diff");
   return WF_OK;
@@ -484,13 +492,13 @@ __global__ void __launch_bounds__(TPB) k_calvel(const wf_case c, Geo g, double a
   pdl_entry();
   const double* p = c.fld[WF_P];
   const double dt = *dtp;
-  const long tot = (long)g.n * g.n * g.n;
   const int hi = NPL + g.n - 1;  // last real index; the component's own axis stops before it
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
-       t += (long)gridDim.x * blockDim.x) {
-    const int k = NPL + (int)(t % g.n);
-    const int j = NPL + (int)((t / g.n) % g.n);
-    const int i = NPL + (int)(t / ((long)g.n * g.n));
+  {  // one thread per cell: x = k (runs of 32), y = j (groups of 8), z = i
+    const int kx_ = blockIdx.x * 32 + threadIdx.x, jy_ = blockIdx.y * 8 + threadIdx.y;
+    if (kx_ >= g.n || jy_ >= g.n) return;
+    const int k = NPL + kx_;
+    const int j = NPL + jy_;
+    const int i = NPL + (int)blockIdx.z;
     const long id = g.at(i, j, k);
     const double p0 = LD(p, id);
     if (i < hi)
@@ -504,7 +512,7 @@ __global__ void __launch_bounds__(TPB) k_calvel(const wf_case c, Geo g, double a
 
 int launch_calvel(const wf_case& c, double alpha, const double* dt, cudaStream_t s) {
   Geo g = geo_of(c.n);
-  WF_CK(launch_k(k_calvel, nblocks((long)c.n * c.n * c.n), TPB, 0, s, c, g, alpha, dt));
+  WF_CK(launch_k(k_calvel, cells3(c.n, c.n, c.n), cell_block(), 0, s, c, g, alpha, dt));
   WF_CKL("k_calvel");
   return WF_OK;
 }
