@@ -98,7 +98,7 @@ def _randomise(sol, names, seed, scale=1.0):
 
 @pytest.mark.parametrize("comp", [0, 1, 2])
 @pytest.mark.parametrize("alpha", [0.5, 1.0])
-@pytest.mark.parametrize("n", [16, 40, 72])   # one, two and three marching segments
+@pytest.mark.parametrize("n", [16, 40, 72])   # whole and partial 32-cell runs along k
 def test_conv_diff(comp, alpha, n):
     sol = _solver(n=n)
     sol.dt = 3.3e-4

@@ -1568,13 +1568,12 @@ __global__ void k_resmax(const Lvl<double> L, double* out, unsigned int* ticket,
   pdl_entry();
   __shared__ double sm[32];
   const int n = L.n;
-  const long tot = (long)n * n * n;
   double m = 0.0;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
-       t += (long)gridDim.x * blockDim.x) {
-    const int k = (int)(t % n);
-    const int j = (int)((t / n) % n);
-    const int i = (int)(t / ((long)n * n));
+  // 1-D CTAs of 32 (k) x 8 (j) threads stepping through planes i by gridDim.z
+  const int k = blockIdx.x * 32 + (threadIdx.x & 31);
+  const int j = blockIdx.y * 8 + (threadIdx.x >> 5);
+  const bool in = k < n && j < n;
+  for (int i = blockIdx.z; in && i < n; i += gridDim.z) {
     const long c = lid(L, i + 1, j + 1, k + 1);
     const double aw = i > 0 ? L.ax : 0.0, ae = i < n - 1 ? L.ax : 0.0;
     const double as = j > 0 ? L.ay : 0.0, an = j < n - 1 ? L.ay : 0.0;
@@ -1925,7 +1924,9 @@ int mg_residual_max_pair(const wf_case& c, const double* phi0, const double* rhs
   const long m = c.n + 2;
   std::vector<Lvl<double>> lv;
   WF_TRY(build_levels<double>(c, const_cast<double*>(phi0), rhs0, m * m, m, lv));
-  WF_CK(launch_k(k_resmax, mg_blocks((long)c.n * c.n * c.n), MG_TPB, 0, s, lv[0], out, &c.sc->ticket,
+  const int gx = (c.n + 31) / 32, gy = (c.n + 7) / 8;
+  const dim3 rg(gx, gy, std::max(1, std::min(c.n, (148 * 8) / (gx * gy))));
+  WF_CK(launch_k(k_resmax, rg, MG_TPB, 0, s, lv[0], out, &c.sc->ticket,
                                                                &c.sc->red[5]));
   WF_CKL("k_resmax");
   return WF_OK;

@@ -5,6 +5,8 @@
 // Field layout: (n+6)^3 doubles, [i][j][k] with k contiguous, real cells
 // NPL..NPL+n-1.  One thread per output cell; consecutive threads walk k so
 // every access of a warp is a contiguous run.
+#include <algorithm>
+
 #include "wf_dev.cuh"
 #include "wf_internal.h"
 
@@ -27,6 +29,16 @@ static inline Geo geo_of(int n) {
   g.sJ = g.P;
   g.sI = g.P * g.P;
   return g;
+}
+
+// reductions over the n^3 real cells: 1-D CTAs of 32 (k) x 8 (j) threads,
+// grid (k runs, j groups, G) with each CTA stepping through planes i by G;
+// G keeps the grid near 8 CTAs per SM, so that few CTAs meet at the
+// reduction atomics
+static inline dim3 reduce_grid(int n) {
+  const int gx = (n + 31) / 32, gy = (n + 7) / 8;
+  const int g = std::max(1, std::min(n, (148 * 8) / (gx * gy)));
+  return dim3(gx, gy, g);
 }
 
 static inline int nblocks(long work, int tpb = TPB, int cap = 148 * 16) {
@@ -121,12 +133,10 @@ __global__ void __launch_bounds__(TPB) k_checkdt(const wf_case c, Geo g) {
   const double dx = c.dx, dy = c.dy, dz = c.dz;
   const double inv2 = 1.0 / (dx * dx) + 1.0 / (dy * dy) + 1.0 / (dz * dz);
   double mu = 0.0, mv = 0.0, mw = 0.0, mdt = 1.0e10;
-  const long tot = (long)g.n * g.n * g.n;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
-       t += (long)gridDim.x * blockDim.x) {
-    const int k = NPL + (int)(t % g.n);
-    const int j = NPL + (int)((t / g.n) % g.n);
-    const int i = NPL + (int)(t / ((long)g.n * g.n));
+  const int k = NPL + blockIdx.x * 32 + (threadIdx.x & 31);
+  const int j = NPL + blockIdx.y * 8 + (threadIdx.x >> 5);
+  const bool in = k < NPL + g.n && j < NPL + g.n;
+  for (int i = NPL + blockIdx.z; in && i < NPL + g.n; i += gridDim.z) {
     const long id = g.at(i, j, k);
     const double uu = LD(u, id), vv = LD(v, id), ww = LD(w, id);
     mu = fmax(mu, fabs(uu));
@@ -183,7 +193,7 @@ __global__ void __launch_bounds__(TPB) k_checkdt(const wf_case c, Geo g) {
 
 int launch_checkdt(const wf_case& c, cudaStream_t s) {
   Geo g = geo_of(c.n);
-  WF_CK(launch_k(k_checkdt, nblocks((long)c.n * c.n * c.n, TPB, 148 * 4), TPB, 0, s, c, g));
+  WF_CK(launch_k(k_checkdt, reduce_grid(c.n), TPB, 0, s, c, g));
   WF_CKL("k_checkdt");
   return WF_OK;
 }
@@ -534,12 +544,10 @@ __global__ void __launch_bounds__(TPB) k_calmas(const wf_case c, Geo g,
   const double dt = sc->dt;
   const double dx = c.dx, dy = c.dy, dz = c.dz;
   double mloc = 0.0;
-  const long tot = (long)g.n * g.n * g.n;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
-       t += (long)gridDim.x * blockDim.x) {
-    const int k = NPL + (int)(t % g.n);
-    const int j = NPL + (int)((t / g.n) % g.n);
-    const int i = NPL + (int)(t / ((long)g.n * g.n));
+  const int k = NPL + blockIdx.x * 32 + (threadIdx.x & 31);
+  const int j = NPL + blockIdx.y * 8 + (threadIdx.x >> 5);
+  const bool in = k < NPL + g.n && j < NPL + g.n;
+  for (int i = NPL + blockIdx.z; in && i < NPL + g.n; i += gridDim.z) {
     const long id = g.at(i, j, k);
     const long X = g.sI, Y = g.sJ;
     const double dudx = (-LD(u, id + X) + 27.0 * LD(u, id) - 27.0 * LD(u, id - X) +
@@ -576,7 +584,7 @@ __global__ void __launch_bounds__(TPB) k_calmas(const wf_case c, Geo g,
 int launch_calmas(const wf_case& c, unsigned long long h_if, unsigned long long h_loop,
                   cudaStream_t s) {
   Geo g = geo_of(c.n);
-  WF_CK(launch_k(k_calmas, nblocks((long)c.n * c.n * c.n, TPB, 148 * 4), TPB, 0, s, c, g, h_if, h_loop));
+  WF_CK(launch_k(k_calmas, reduce_grid(c.n), TPB, 0, s, c, g, h_if, h_loop));
   WF_CKL("k_calmas");
   return WF_OK;
 }
@@ -587,12 +595,12 @@ int launch_calmas(const wf_case& c, unsigned long long h_if, unsigned long long 
 __global__ void k_add_ring(double* p, const double* pp, Geo g) {
   pdl_entry();
   const int m = g.n + 2;
-  const long tot = (long)m * m * m;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
-       t += (long)gridDim.x * blockDim.x) {
-    const int k = NPL - 1 + (int)(t % m);
-    const int j = NPL - 1 + (int)((t / m) % m);
-    const int i = NPL - 1 + (int)(t / ((long)m * m));
+  {  // one thread per cell: x = k (runs of 32), y = j (groups of 8), z = i
+    const int kx_ = blockIdx.x * 32 + threadIdx.x, jy_ = blockIdx.y * 8 + threadIdx.y;
+    if (kx_ >= m || jy_ >= m) return;
+    const int k = NPL - 1 + kx_;
+    const int j = NPL - 1 + jy_;
+    const int i = NPL - 1 + (int)blockIdx.z;
     const long id = g.at(i, j, k);
     p[id] = p[id] + pp[id];
   }
@@ -600,7 +608,7 @@ __global__ void k_add_ring(double* p, const double* pp, Geo g) {
 
 int launch_add_ring(double* p, const double* pp, int n, cudaStream_t s) {
   Geo g = geo_of(n);
-  WF_CK(launch_k(k_add_ring, nblocks((long)(n + 2) * (n + 2) * (n + 2)), TPB, 0, s, p, pp, g));
+  WF_CK(launch_k(k_add_ring, cells3(n + 2, n + 2, n + 2), cell_block(), 0, s, p, pp, g));
   WF_CKL("k_add_ring");
   return WF_OK;
 }
