@@ -1925,7 +1925,7 @@ int mg_residual_max_pair(const wf_case& c, const double* phi0, const double* rhs
   std::vector<Lvl<double>> lv;
   WF_TRY(build_levels<double>(c, const_cast<double*>(phi0), rhs0, m * m, m, lv));
   const int gx = (c.n + 31) / 32, gy = (c.n + 7) / 8;
-  const dim3 rg(gx, gy, std::max(1, std::min(c.n, (148 * 8) / (gx * gy))));
+  const dim3 rg(gx, gy, std::max(1, std::min(c.n, (148 * 32) / (gx * gy))));
   WF_CK(launch_k(k_resmax, rg, MG_TPB, 0, s, lv[0], out, &c.sc->ticket,
                                                                &c.sc->red[5]));
   WF_CKL("k_resmax");

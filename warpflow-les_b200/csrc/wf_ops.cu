@@ -33,11 +33,11 @@ static inline Geo geo_of(int n) {
 
 // reductions over the n^3 real cells: 1-D CTAs of 32 (k) x 8 (j) threads,
 // grid (k runs, j groups, G) with each CTA stepping through planes i by G;
-// G keeps the grid near 8 CTAs per SM, so that few CTAs meet at the
-// reduction atomics
+// G keeps the grid near 32 CTAs per SM: enough independent planes in flight,
+// few enough CTAs meeting at the reduction atomics
 static inline dim3 reduce_grid(int n) {
   const int gx = (n + 31) / 32, gy = (n + 7) / 8;
-  const int g = std::max(1, std::min(n, (148 * 8) / (gx * gy)));
+  const int g = std::max(1, std::min(n, (148 * 32) / (gx * gy)));
   return dim3(gx, gy, g);
 }
 
