@@ -145,6 +145,67 @@ def load_peaks():
     return PEAKS_FALLBACK["hbm_gbs"], "fallback"
 
 
+# DRAM bytes per launch of the dominant kernels, from the ncu captures
+# summarised under profiles/ (dram__bytes_read.sum + dram__bytes_write.sum)
+NCU_TRAFFIC = {("k_rbgs_split", 256): (189055488, "profiles/rbgs_split_256_full.md"),
+               ("coarse", 20): (172032, "profiles/coarse_p2p_20_full.md")}
+
+
+def kernel_roofline(sol, args, peak, peak_kind):
+    """The dominant kernel of the step, timed live with CUDA events on the
+    launching stream after the timed region.  Levels >= 128 (FP64): the
+    split half-sweep of level 0 -- relax(6) and relax(12) differ by exactly
+    12 half-sweep launches, so their difference isolates the kernel; its
+    algorithmic bytes are 1.5 words per cell (read the other colour, read the
+    own colour's rhs, write the own colour).  Smaller cases: the coarse-level
+    relax (300 sweeps in one launch, the largest share of the step), whose
+    global traffic is reading phi and rhs and writing phi once."""
+    import numpy as np
+    import torch
+    if args.precision != "fp64":
+        return {"bound": "hbm", "kernel": None, "achieved": None, "peak": peak,
+                "unit": "GB/s", "frac": None, "traffic": None,
+                "note": "mixed precision relaxes FP32 levels outside the FP64 harness; "
+                        "see roofline_step"}
+    mg = sol.mg
+
+    def timed(l, sweeps, reps):
+        mg._relax(l, sweeps)
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            mg._relax(l, sweeps)
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps / 1e3   # s per relax
+
+    n = args.n
+    lev0 = mg.levels[0]
+    lev0.rhs.assign(np.random.default_rng(7).standard_normal(lev0.shape))
+    if n >= 128:
+        t = (timed(0, 12, 5) - timed(0, 6, 5)) / 12
+        alg = 1.5 * n ** 3 * 8
+        name = "k_rbgs_split (level-0 half-sweep, FP64)"
+        key = ("k_rbgs_split", n)
+    else:
+        lc = args.levels - 1
+        nc = n >> lc
+        lv = mg.levels[lc]
+        lv.rhs.assign(np.random.default_rng(8).standard_normal(lv.shape))
+        t = timed(lc, 300, 5)
+        alg = 3 * (nc + 2) ** 3 * 8
+        name = "coarse relax %d^3, 300 sweeps in one launch (latency-bound)" % nc
+        key = ("coarse", nc)
+    traffic, src = NCU_TRAFFIC.get(key, (None, None))
+    ach = alg / t / 1e9
+    return {"bound": "hbm", "kernel": name, "achieved": round(ach, 2), "peak": peak,
+            "peak_kind": peak_kind, "unit": "GB/s", "frac": round(ach / peak, 5),
+            "traffic": traffic, "traffic_source": src, "alg_bytes_per_launch": round(alg),
+            "us_per_launch": round(t * 1e6, 2)}
+
+
 # ---------------------------------------------------------------------------
 def run_oracle(n, levels, steps, warmup):
     """The reference algorithm on the host cores (NumPy FP64 oracle port;
@@ -413,13 +474,13 @@ def main():
                     for it, m in zip(iters, nmgs))
     peak, peak_kind = load_peaks()
     achieved = bytes_tot / (sum(step_ms) / 1e3) / 1e9
-    roofline = {"bound": "hbm", "kernel": "whole step (one CUDA graph launch)",
-                "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind,
-                "unit": "GB/s", "frac": round(achieved / peak, 4),
-                "traffic": None,
-                "alg_bytes_per_step": round(bytes_tot / K),
-                "note": "achieved = algorithmic bytes of the reference passes (measured "
-                        "iters per step) / device step time; frac of measured copy peak"}
+    roofline_step = {"bound": "hbm", "kernel": "whole step (one CUDA graph launch)",
+                     "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "alg_bytes_per_step": round(bytes_tot / K),
+                     "note": "algorithmic bytes of the reference passes (measured iters per "
+                             "step) / device step time; frac of the measured copy peak"}
+    roofline = kernel_roofline(sol, args, peak, peak_kind)
 
     # ---- end to end through the public API with host buffers ---------------
     e2e = None
@@ -479,7 +540,8 @@ def main():
                 "config": cfg_desc, "iters_mean": round(sum(iters) / K, 3),
                 "wall_s": round(wall, 3), "gpu_launches": int(launches),
                 "launches_per_step": round(launches / K, 1),
-                "clocks": clocks, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e}
+                "clocks": clocks, "roofline": roofline, "roofline_step": roofline_step,
+                "cpu_baseline": cpu, "e2e": e2e}
         print(json.dumps(line), flush=True)
     sol.close()
     if world > 1:
