@@ -1,8 +1,11 @@
-"""The alternative fine-level relax paths forced on at small sizes in child
-processes -- sweeps on row-parity-split copies (used by default for large
-levels) and one-launch red-black sweeps (off by default): multigrid solves
-must match the FP64 oracle, the mixed form must stay within its tolerance,
-and every result must be bit-identical to the in-place one-colour path."""
+"""The alternative relax paths of the fine and mid-size levels, each forced on
+or off in child processes -- sweeps on row-parity-split copies (default for
+levels >= 128), cluster-resident relaxes of 28..48^3 levels (default), and
+one-launch red-black sweeps (off by default): multigrid solves must match
+the FP64 oracle and the mixed form must stay within its tolerance.  The
+split and one-launch paths divide exactly like the in-place one-colour path
+and must equal it bit for bit; the cluster kernels multiply by the
+reciprocal of the diagonal (one rounding away) and must agree to 1e-12."""
 import hashlib
 import json
 import os
@@ -24,7 +27,8 @@ from warpflow import Multigrid, build_topology
 from warpflow.config import case_from_dict
 from warpflow.fields import DeviceField
 out = {}
-for n, L, prec in ((20, 2, "fp64"), (24, 3, "fp64"), (40, 3, "fp64"), (40, 3, "mixed"), (70, 2, "fp64")):
+for n, L, prec in ((20, 2, "fp64"), (24, 3, "fp64"), (40, 3, "fp64"), (40, 3, "mixed"),
+                   (70, 2, "fp64"), (64, 3, "fp64"), (96, 3, "fp64"), (96, 3, "mixed")):
     cfg = case_from_dict({"grid": {"nx": n, "ny": n, "nz": n},
                           "numerics": {"mg_levels": L, "mg_precision": prec}})
     h = 1.0 / n
@@ -67,18 +71,24 @@ def _run(env_extra):
 
 @pytest.fixture(scope="module")
 def in_place():
-    return _run({"WF_SPLIT_MIN": OFF, "WF_SWEEP2_MIN": OFF})
+    return _run({"WF_SPLIT_MIN": OFF, "WF_SWEEP2_MIN": OFF, "WF_MID": "0"})
 
 
-@pytest.mark.parametrize("env", [{"WF_SPLIT_MIN": "8", "WF_SWEEP2_MIN": OFF},
-                                 {"WF_SPLIT_MIN": OFF, "WF_SWEEP2_MIN": "8"}],
-                         ids=["split", "one_launch"])
-def test_relax_paths_match_oracle_and_in_place(env, in_place):
+@pytest.mark.parametrize("env,exact", [
+    ({"WF_SPLIT_MIN": "8", "WF_SWEEP2_MIN": OFF, "WF_MID": "0"}, True),
+    ({"WF_SPLIT_MIN": OFF, "WF_SWEEP2_MIN": "8", "WF_MID": "0"}, True),
+    ({"WF_SPLIT_MIN": OFF, "WF_SWEEP2_MIN": OFF, "WF_MID": "1"}, False)],
+    ids=["split", "one_launch", "mid_cluster"])
+def test_relax_paths_match_oracle_and_in_place(env, exact, in_place):
     res = _run(env)
     for key, val in res.items():
         if key.startswith("hash_"):
-            assert val == in_place[key], key
+            if exact:
+                assert val == in_place[key], key
             continue
         tol = 1e-5 if key.endswith("mixed") else 1e-11
         assert val <= tol, (key, val)
         assert in_place[key] <= tol, (key, in_place[key])
+        if not exact and not key.endswith("mixed"):
+            # both within 1e-11 of the oracle; the paths differ by rounding only
+            assert abs(val - in_place[key]) <= 1e-11, key

@@ -63,6 +63,45 @@ __device__ __forceinline__ void ring_mirror(const Lvl<T>& L, int i, int j, int k
   if (k == n - 1) L.phi[c + 1] = x;
 }
 
+// x / d, correctly rounded, from y = RN(1/d): one residual correction makes
+// the quotient faithful, a second rounds it correctly (P. Markstein,
+// "Computation of elementary functions on the IBM RISC System/6000
+// processor", IBM J. Res. Dev. 34(1), 1990).  Valid away from overflow and
+// underflow, which the multigrid's values stay far from; four FMAs and a
+// multiply in place of a full division.
+template <class T>
+__device__ __forceinline__ T div_by_recip(T x, T d, T y) {
+  T q = x * y;
+  T r = fma(-q, d, x);
+  q = fma(r, y, q);
+  r = fma(-q, d, x);
+  return fma(r, y, q);
+}
+
+// RN(1/ap) for every boundary pattern of a cell: index 9*cx + 3*cy + cz,
+// c = number of non-zero coefficients along the axis (0, 1 or 2).  ap is
+// summed in the kernels' order; zero terms do not change an IEEE sum, so
+// the pattern counts fix ap exactly.
+template <class T>
+struct ApRecip {
+  T y[27];
+};
+
+template <class T>
+static ApRecip<T> ap_recip(const Lvl<T>& L) {
+  ApRecip<T> t;
+  for (int cx = 0; cx < 3; ++cx)
+    for (int cy = 0; cy < 3; ++cy)
+      for (int cz = 0; cz < 3; ++cz) {
+        const T aw = cx > 0 ? L.ax : T(0), ae = cx > 1 ? L.ax : T(0);
+        const T as = cy > 0 ? L.ay : T(0), an = cy > 1 ? L.ay : T(0);
+        const T ab = cz > 0 ? L.az : T(0), at = cz > 1 ? L.az : T(0);
+        const T ap = -(aw + ae + as + an + ab + at);
+        t.y[9 * cx + 3 * cy + cz] = ap != T(0) ? T(1) / ap : T(0);
+      }
+  return t;
+}
+
 // one colour half-sweep (multigrid.py:70-90): update where (i+j+k+color)%2==1
 template <class T>
 __global__ void __launch_bounds__(MG_TPB) k_rbgs(const Lvl<T> L, int color) {
@@ -288,7 +327,9 @@ __device__ __forceinline__ void half_sweep_cols(const T* __restrict__ oth, T* __
 // [column parity][k][i][j/2], where the four in-plane neighbours of a
 // column (all of the other parity) are contiguous across the lanes of a
 // warp.  The diagonal is applied as a reciprocal (one rounding away from the
-// division).  Ring terms have zero coefficients and are not read.
+// division; correcting it to the exact quotient lengthens the dependent
+// chain of every update, which is what these latency-bound kernels cannot
+// afford).  Ring terms have zero coefficients and are not read.
 template <int NC>
 struct CoarseShape {
   static constexpr int THREADS = 2 * (((NC * (NC / 2)) + 31) / 32) * 32;
@@ -799,6 +840,33 @@ static int try_coarse_p2p(const Lvl<T>& L, int nsweeps, cudaStream_t s, int* rc)
   }
 }
 
+// mid-size levels (a few sweeps of 28^3..48^3): the whole level resident in
+// the distributed shared memory of one cluster, so a 6-sweep relax is one
+// launch instead of twelve.  Off by default (WF_MID=1 turns it on): inside
+// the step graph, programmatic dependent launch already brings a
+// one-colour half-sweep of these levels to about 1.3 us, and the 80^3 step
+// measured 2.47 ms with it against 2.41 ms without.
+static bool mid_p2p_enabled() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("WF_MID");
+    v = (e && e[0] == '1') ? 1 : 0;
+  }
+  return v == 1;
+}
+
+template <class T>
+static int try_relax_mid(const Lvl<T>& L, int nsweeps, cudaStream_t s, int* rc) {
+  if (!mid_p2p_enabled()) return 0;
+  switch (L.n) {
+    case 28: *rc = launch_coarse_p2p<T, 28, 4>(L, nsweeps, s); return 1;
+    case 32: *rc = launch_coarse_p2p<T, 32, 4>(L, nsweeps, s); return 1;
+    case 40: *rc = launch_coarse_p2p<T, 40, 4>(L, nsweeps, s); return 1;
+    case 48: *rc = launch_coarse_p2p<T, 48, 4>(L, nsweeps, s); return 1;
+    default: return 0;
+  }
+}
+
 // ---- temporal blocking: one exchange per full sweep ----------------------
 // As k_coarse_p2p, but each CTA also keeps two halo planes on each side, so
 // it can run a whole sweep locally: red on its slab plus one plane on each
@@ -1105,45 +1173,6 @@ __global__ void __launch_bounds__(32 * SPLIT_ROWS)
     sp[dst + q] = L.phi[src + a];
     if (with_rhs) sr[dst + q] = L.rhs[src + a];
   }
-}
-
-// x / d, correctly rounded, from y = RN(1/d): one residual correction makes
-// the quotient faithful, a second rounds it correctly (P. Markstein,
-// "Computation of elementary functions on the IBM RISC System/6000
-// processor", IBM J. Res. Dev. 34(1), 1990).  Valid away from overflow and
-// underflow, which the multigrid's values stay far from; four FMAs and a
-// multiply in place of a full division.
-template <class T>
-__device__ __forceinline__ T div_by_recip(T x, T d, T y) {
-  T q = x * y;
-  T r = fma(-q, d, x);
-  q = fma(r, y, q);
-  r = fma(-q, d, x);
-  return fma(r, y, q);
-}
-
-// RN(1/ap) for every boundary pattern of a cell: index 9*cx + 3*cy + cz,
-// c = number of non-zero coefficients along the axis (0, 1 or 2).  ap is
-// summed in the kernels' order; zero terms do not change an IEEE sum, so
-// the pattern counts fix ap exactly.
-template <class T>
-struct ApRecip {
-  T y[27];
-};
-
-template <class T>
-static ApRecip<T> ap_recip(const Lvl<T>& L) {
-  ApRecip<T> t;
-  for (int cx = 0; cx < 3; ++cx)
-    for (int cy = 0; cy < 3; ++cy)
-      for (int cz = 0; cz < 3; ++cz) {
-        const T aw = cx > 0 ? L.ax : T(0), ae = cx > 1 ? L.ax : T(0);
-        const T as = cy > 0 ? L.ay : T(0), an = cy > 1 ? L.ay : T(0);
-        const T ab = cz > 0 ? L.az : T(0), at = cz > 1 ? L.az : T(0);
-        const T ap = -(aw + ae + as + an + ab + at);
-        t.y[9 * cx + 3 * cy + cz] = ap != T(0) ? T(1) / ap : T(0);
-      }
-  return t;
 }
 
 // one colour half-sweep on the split copy: a warp updates CPT runs of 32
@@ -1628,6 +1657,10 @@ static int relax(const Lvl<T>& L, int nsweeps, cudaStream_t s, bool rhs_ready = 
   }
   if (L.tmp && (L.n & 1) == 0 && L.n >= split_min_n())
     return relax_split<T>(L, nsweeps, rhs_ready, s);
+  {
+    int rc = WF_OK;
+    if (try_relax_mid<T>(L, nsweeps, s, &rc)) return rc;
+  }
   if (L.tmp && nsweeps >= 2 && L.n >= sweep2_min_n()) {
     // pairs of one-launch sweeps: phi -> tmp -> phi
     const int pairs = nsweeps / 2;
