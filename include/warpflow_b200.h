@@ -106,6 +106,9 @@ typedef struct wf_case {
                                      levels relax on row-parity-split copies of phi and rhs
                                      held there; NULL = relax in place */
   wf_scalars* sc;                 /* device scalar block */
+  void* mg_cop;                   /* optional coarse-level operator (may be shared
+                                     by cases), see wf_mg_build_coarse_op; NULL = sweeps */
+  void* mg_cop_part;              /* this case's partial-sum scratch for it */
 } wf_case;
 
 /* ---- library ---------------------------------------------------------- */
@@ -122,6 +125,20 @@ WF_API int wf_scalars_init(wf_scalars* sc, double dt0, void* stream);
 WF_API int wf_set_coarse_strategy(int32_t n, int32_t fp32, int32_t strategy);
 /* bytes of MG workspace a case needs at each level (caller allocates) */
 WF_API int wf_mg_level_elems(int32_t n, int32_t nlev, int32_t level, int64_t* elems);
+/* No counterpart in the reference.  The coarsest-level relax of a V-cycle
+ * (multigrid.py:301-322: n_coarse RBGS sweeps starting from phi = 0) is a
+ * fixed linear map of the level's rhs.  wf_mg_build_coarse_op stores it, for
+ * the case's n, nlev, spacing, n_coarse and precision (c->mg_fp32 selects
+ * FP32), as a dense operator in c->mg_cop: row j = the relaxed field for
+ * rhs = unit vector j.  With c->mg_cop set, V-cycles apply it as one
+ * matrix-vector product (HBM-bound) instead of the latency-bound sweeps;
+ * the results agree to rounding.  Coarsest edges 4, 8, 12, 16, 20, 24 only
+ * (WF_EUNSUPPORTED otherwise).  The operator is read-only once built and can
+ * be shared by cases of the same size; each case needs its own partial-sum
+ * scratch (c->mg_cop_part).  wf_mg_coarse_op_elems gives both element counts. */
+WF_API int wf_mg_coarse_op_elems(int32_t n, int32_t nlev, int64_t* op_elems,
+                                 int64_t* scratch_elems);
+WF_API int wf_mg_build_coarse_op(const wf_case* c, void* stream);
 
 /* ---- initial state ---------------------------------------------------- */
 /* kernels.py:452-471 init_noise: u = v = amp*r, w = -amp*r (uint32 hash). */

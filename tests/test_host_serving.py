@@ -73,8 +73,14 @@ def test_case_bytes_formula():
     vol = 82 ** 3 + 42 ** 3 + 22 ** 3
     mg64 = 2 * 8 * vol + 2 * 8 * vol      # phi, rhs + two-array scratch
     mg32 = 2 * 4 * vol + 2 * 4 * vol
-    assert case_bytes(n, 3, "fp64") - f - mg64 < 4096
-    assert case_bytes(n, 3, "mixed") - f - 2 * 8 * vol - mg32 < 4096
+    cop64, cop32 = 32 * 20 ** 3 * 8, 32 * 20 ** 3 * 4   # coarse-operator scratch
+    assert 0 <= case_bytes(n, 3, "fp64") - f - mg64 - cop64 < 4096
+    assert 0 <= case_bytes(n, 3, "mixed") - f - 2 * 8 * vol - mg32 - cop32 < 4096
+    # a coarsest edge without an operator (18) adds no scratch
+    n2 = 72
+    f2 = 13 * 78 ** 3 * 8
+    vol2 = 74 ** 3 + 38 ** 3 + 20 ** 3
+    assert 0 <= case_bytes(n2, 3, "fp64") - f2 - 4 * 8 * vol2 < 4096
 
 
 def test_shard_round_robin():

@@ -335,9 +335,13 @@ struct CoarseShape {
   static constexpr int THREADS = 2 * (((NC * (NC / 2)) + 31) / 32) * 32;
 };
 
+// With unit_out set, CTA b relaxes rhs = unit vector b from phi = 0 and
+// writes the result as row b of unit_out (cells in (i, j, k) order): the
+// rows of the coarse-level operator.
 template <class T, int NC, bool RHS_SMEM>
 __global__ void __launch_bounds__(CoarseShape<NC>::THREADS) k_coarse_cols(Lvl<T> L,
-                                                                           int nsweeps) {
+                                                                           int nsweeps,
+                                                                           T* unit_out) {
   pdl_entry();
   constexpr int H = NC / 2;
   constexpr int HALF = NC * H;                  // columns per parity
@@ -372,8 +376,14 @@ __global__ void __launch_bounds__(CoarseShape<NC>::THREADS) k_coarse_cols(Lvl<T>
   const long c0 = lid(L, i + 1, j + 1, 1);
 #pragma unroll
   for (int k = 0; k < NC; ++k) {
-    ph[k] = active ? L.phi[c0 + k] : T(0);
-    const T r = active ? L.rhs[c0 + k] : T(0);
+    T r;
+    if (unit_out) {
+      ph[k] = T(0);
+      r = (active && (i * NC + j) * NC + k == (int)blockIdx.x) ? T(1) : T(0);
+    } else {
+      ph[k] = active ? L.phi[c0 + k] : T(0);
+      r = active ? L.rhs[c0 + k] : T(0);
+    }
     if (RHS_SMEM) {
       if (active) srh[(g * NC + k) * PLANE + me] = r;
     } else {
@@ -399,6 +409,12 @@ __global__ void __launch_bounds__(CoarseShape<NC>::THREADS) k_coarse_cols(Lvl<T>
     }
   }
   if (!active) return;
+  if (unit_out) {
+    T* row = unit_out + (long)blockIdx.x * (NC * NC * NC) + (i * NC + j) * NC;
+#pragma unroll
+    for (int k = 0; k < NC; ++k) row[k] = ph[k];
+    return;
+  }
 #pragma unroll
   for (int k = 0; k < NC; ++k) {
     const long c = c0 + k;
@@ -408,13 +424,14 @@ __global__ void __launch_bounds__(CoarseShape<NC>::THREADS) k_coarse_cols(Lvl<T>
 }
 
 template <class T, int NC, bool RHS_SMEM>
-static int launch_coarse(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
+static int launch_coarse(const Lvl<T>& L, int nsweeps, cudaStream_t s, T* unit_out = nullptr) {
   constexpr int HALF = NC * (NC / 2);
   constexpr int GROUP = ((HALF + 31) / 32) * 32;
   const size_t sb = (size_t)NC * NC * NC * sizeof(T) * (RHS_SMEM ? 2 : 1);
   WF_CK(cudaFuncSetAttribute(k_coarse_cols<T, NC, RHS_SMEM>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb));
-  WF_CK(launch_k(k_coarse_cols<T, NC, RHS_SMEM>, 1, 2 * GROUP, sb, s, L, nsweeps));
+  const int nb = unit_out ? NC * NC * NC : 1;
+  WF_CK(launch_k(k_coarse_cols<T, NC, RHS_SMEM>, nb, 2 * GROUP, sb, s, L, nsweeps, unit_out));
   WF_CKL("k_coarse_cols");
   return WF_OK;
 }
@@ -1088,6 +1105,92 @@ static int try_coarse_tb(const Lvl<T>& L, int nsweeps, cudaStream_t s, int* rc) 
   }
 }
 
+// ---- the coarse-level relax as a precomputed operator ----------------------
+// n_coarse sweeps from phi = 0 are linear in rhs: phi = sum_j rhs_j * row_j,
+// row_j = the relaxed field for rhs = e_j (built by k_coarse_cols in unit
+// mode).  Applying it reads the operator once (N^2 elements, N = n^3), an
+// HBM-bound product instead of 2*n_coarse dependent half-sweeps.  The sum is
+// split over COP_CH row chunks with partial sums in fixed order (chunk
+// partials, then chunks in ascending order), so results do not depend on
+// scheduling: a case computes the same bits alone or beside other cases.
+constexpr int COP_CH = 32;
+
+static bool cop_size_ok(int nc) {
+  return nc == 4 || nc == 8 || nc == 12 || nc == 16 || nc == 20 || nc == 24;
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_cop_partial(const T* __restrict__ op, const Lvl<T> L,
+                                                     T* __restrict__ part) {
+  pdl_entry();
+  __shared__ T rs[512];
+  const int n = L.n, N = n * n * n;
+  const int jc = (N + COP_CH - 1) / COP_CH;
+  const int j0 = blockIdx.y * jc, j1 = min(N, j0 + jc);
+  for (int t = threadIdx.x; t < j1 - j0; t += 256) {
+    const int jj = j0 + t;
+    const int a = jj / (n * n), rem = jj - a * n * n;
+    const int b = rem / n, cc = rem - b * n;
+    rs[t] = L.rhs[lid(L, a + 1, b + 1, cc + 1)];
+  }
+  __syncthreads();
+  const int i = blockIdx.x * 256 + threadIdx.x;
+  if (i >= N) return;
+  const T* col = op + (long)j0 * N + i;
+  T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+  const int cnt = j1 - j0;
+  int t = 0;
+  for (; t + 4 <= cnt; t += 4) {
+    a0 = fma(rs[t], col[(long)t * N], a0);
+    a1 = fma(rs[t + 1], col[(long)(t + 1) * N], a1);
+    a2 = fma(rs[t + 2], col[(long)(t + 2) * N], a2);
+    a3 = fma(rs[t + 3], col[(long)(t + 3) * N], a3);
+  }
+  for (; t < cnt; ++t) a0 = fma(rs[t], col[(long)t * N], a0);
+  part[(long)blockIdx.y * N + i] = (a0 + a1) + (a2 + a3);
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_cop_finish(const T* __restrict__ part, Lvl<T> L) {
+  pdl_entry();
+  const int n = L.n, N = n * n * n;
+  const int t = blockIdx.x * 256 + threadIdx.x;
+  if (t >= N) return;
+  T x = part[t];
+#pragma unroll 4
+  for (int ch = 1; ch < COP_CH; ++ch) x += part[(long)ch * N + t];
+  const int i = t / (n * n), rem = t - i * n * n;
+  const int j = rem / n, k = rem - j * n;
+  const long c = lid(L, i + 1, j + 1, k + 1);
+  L.phi[c] = x;
+  ring_mirror(L, i, j, k, c, x);
+}
+
+// phi of the coarsest level = operator x rhs (the level's phi is overwritten);
+// part: this case's COP_CH x N scratch
+template <class T>
+static int apply_coarse_op(const Lvl<T>& L, const T* op, T* part, cudaStream_t s) {
+  const int N = L.n * L.n * L.n;
+  WF_CK(launch_k(k_cop_partial<T>, dim3((N + 255) / 256, COP_CH), 256, 0, s, op, L, part));
+  WF_CKL("k_cop_partial");
+  WF_CK(launch_k(k_cop_finish<T>, (N + 255) / 256, 256, 0, s, (const T*)part, L));
+  WF_CKL("k_cop_finish");
+  return WF_OK;
+}
+
+template <class T>
+static int build_coarse_op(const Lvl<T>& L, int nsweeps, T* op, cudaStream_t s) {
+  switch (L.n) {
+    case 4: return launch_coarse<T, 4, false>(L, nsweeps, s, op);
+    case 8: return launch_coarse<T, 8, false>(L, nsweeps, s, op);
+    case 12: return launch_coarse<T, 12, false>(L, nsweeps, s, op);
+    case 16: return launch_coarse<T, 16, false>(L, nsweeps, s, op);
+    case 20: return launch_coarse<T, 20, false>(L, nsweeps, s, op);
+    case 24: return launch_coarse<T, 24, true>(L, nsweeps, s, op);
+    default: return fail(WF_EUNSUPPORTED, "coarse operator: coarsest edge must be 4..24, step 4");
+  }
+}
+
 // coarse strategy: 0 = one CTA (k_coarse_cols), 1 = cluster with a cluster
 // barrier per half-sweep (k_coarse_cluster), 2 = cluster with point-to-point
 // halo pushes (k_coarse_p2p).  Chosen per level size and precision from a
@@ -1722,7 +1825,10 @@ static int vcycle(std::vector<Lvl<T>>& lv, const wf_case& c, cudaStream_t s,
           lv[l - 1], const_cast<T*>(C.rhs), C));
       WF_CKL("k_restrict");
     }
-    WF_TRY(relax(lv[l], l < L - 1 ? c.n_pre : c.n_coarse, s, l == 0 && rhs0_ready));
+    if (l == L - 1 && L > 1 && c.mg_cop && c.mg_cop_part && cop_size_ok(lv[l].n))
+      WF_TRY(apply_coarse_op<T>(lv[l], (const T*)c.mg_cop, (T*)c.mg_cop_part, s));
+    else
+      WF_TRY(relax(lv[l], l < L - 1 ? c.n_pre : c.n_coarse, s, l == 0 && rhs0_ready));
   }
   for (int l = L - 2; l >= 0; --l) {
     WF_CK(launch_k(k_prolong<T>, cells3(lv[l].n, lv[l].n, lv[l].n), cell_block(), 0, s, lv[l + 1],
@@ -1881,6 +1987,40 @@ int mg_dc_cycle_pair(const wf_case& c, double* phi0, const double* rhs0, cudaStr
   std::vector<Lvl<float>> lvf;
   WF_TRY(build_levels_f32(c, lvf));
   return dc_cycle(level0_view(c, phi0, rhs0, m * m, m), lvf, c, s);
+}
+
+int coarse_op_elems(int n, int nlev, int64_t* op_elems, int64_t* scratch_elems) {
+  if (nlev < 2 || nlev > WF_MAX_LEVELS || n < 1) return fail(WF_EINVAL, "bad n or nlev");
+  const int nc = n >> (nlev - 1);
+  if ((nc << (nlev - 1)) != n) return fail(WF_EINVAL, "n must be divisible by 2^(nlev-1)");
+  if (!cop_size_ok(nc))
+    return fail(WF_EUNSUPPORTED, "coarse operator: coarsest edge must be 4..24, step 4");
+  const int64_t N = (int64_t)nc * nc * nc;
+  if (op_elems) *op_elems = N * N;
+  if (scratch_elems) *scratch_elems = (int64_t)COP_CH * N;
+  return WF_OK;
+}
+
+int build_coarse_op_case(const wf_case& c, cudaStream_t s) {
+  if (!c.mg_cop) return fail(WF_EINVAL, "mg_cop is null");
+  WF_TRY(coarse_op_elems(c.n, c.nlev, nullptr, nullptr));
+  const int l = c.nlev - 1;
+  const double s2 = (double)(1 << l);
+  const double dxl = c.dx * s2, dyl = c.dy * s2, dzl = c.dz * s2;
+  if (c.mg_fp32) {
+    Lvl<float> L = {};
+    L.n = c.n >> l;
+    L.ax = (float)(1.0 / (dxl * dxl));
+    L.ay = (float)(1.0 / (dyl * dyl));
+    L.az = (float)(1.0 / (dzl * dzl));
+    return build_coarse_op<float>(L, c.n_coarse, (float*)c.mg_cop, s);
+  }
+  Lvl<double> L = {};
+  L.n = c.n >> l;
+  L.ax = 1.0 / (dxl * dxl);
+  L.ay = 1.0 / (dyl * dyl);
+  L.az = 1.0 / (dzl * dzl);
+  return build_coarse_op<double>(L, c.n_coarse, (double*)c.mg_cop, s);
 }
 
 int mg_solve(const wf_case& c, cudaStream_t s) {

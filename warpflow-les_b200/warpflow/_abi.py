@@ -68,6 +68,8 @@ class WfCase(ctypes.Structure):
         ("mg_rhs", ctypes.c_void_p * MAX_LEVELS),
         ("mg_tmp", ctypes.c_void_p * MAX_LEVELS),
         ("sc", ctypes.c_void_p),
+        ("mg_cop", ctypes.c_void_p),
+        ("mg_cop_part", ctypes.c_void_p),
     ]
 
 
@@ -84,6 +86,9 @@ SIGNATURES = {
     "wf_scalars_init": (_I32, [_VP, _D, _VP]),
     "wf_set_coarse_strategy": (_I32, [_I32, _I32, _I32]),
     "wf_mg_level_elems": (_I32, [_I32, _I32, _I32, ctypes.POINTER(ctypes.c_int64)]),
+    "wf_mg_coarse_op_elems": (_I32, [_I32, _I32, ctypes.POINTER(ctypes.c_int64),
+                                     ctypes.POINTER(ctypes.c_int64)]),
+    "wf_mg_build_coarse_op": (_I32, [_CP, _VP]),
     "wf_init_noise": (_I32, [_VP, _VP, _VP, _I32, _D, _I32, _VP]),
     "wf_fill_initial": (_I32, [_CP, _VP]),
     "wf_fill_u": (_I32, [_VP, _I32, _D, _VP]),

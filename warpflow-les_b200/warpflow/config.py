@@ -5,9 +5,12 @@ Same schema, defaults and validation as the reference loader
 flattened into ``sgs_enabled/sgs_model/sgs_cw``, and every grid axis must
 divide by the domain count and by 2**(mg_levels-1).
 
-One addition: ``numerics.mg_precision`` selects the multigrid arithmetic,
+Two additions: ``numerics.mg_precision`` selects the multigrid arithmetic,
 ``"fp64"`` (default, the reference's) or ``"mixed"`` (FP32 V-cycles inside
-an FP64 defect correction).
+an FP64 defect correction); ``numerics.mg_coarse`` selects how the coarsest
+level's n_coarse sweeps run, ``"operator"`` (default: the same linear map
+applied as one precomputed matrix-vector product, where the coarsest edge is
+4..24 in steps of 4) or ``"sweeps"``.
 """
 from __future__ import annotations
 
@@ -67,6 +70,7 @@ class NumericsCfg:
     div_tolerance: float = 1.0e-6
     ghost_layers: int = 3
     mg_precision: str = "fp64"
+    mg_coarse: str = "operator"
 
 
 @dataclass
@@ -133,6 +137,9 @@ def case_from_dict(raw: dict) -> CaseConfig:
     if cfg.numerics.mg_precision not in ("fp64", "mixed"):
         raise ValueError("numerics.mg_precision must be 'fp64' or 'mixed', got %r"
                          % (cfg.numerics.mg_precision,))
+    if cfg.numerics.mg_coarse not in ("operator", "sweeps"):
+        raise ValueError("numerics.mg_coarse must be 'operator' or 'sweeps', got %r"
+                         % (cfg.numerics.mg_coarse,))
     ncell = (cfg.grid.nx, cfg.grid.ny, cfg.grid.nz)
     div = 2 ** (cfg.numerics.mg_levels - 1)
     for axis, (n, m) in enumerate(zip(ncell, cfg.mpi.domains)):

@@ -15,6 +15,14 @@ The level-0 ``phi``/``rhs`` arrays serve the standalone harness form
 ``precision="mixed"`` (config ``numerics.mg_precision``) runs every V-cycle
 in FP32 as a correction of an FP64 defect correction: the residual, the
 accumulation of the solution and everything outside the multigrid stay FP64.
+
+``coarse="operator"`` (config ``numerics.mg_coarse``, the default) applies
+the coarsest level's n_coarse sweeps from zero -- a fixed linear map of its
+rhs -- as one precomputed dense operator (``wf_mg_build_coarse_op``), built
+once per (size, spacing, n_coarse, precision) and shared by every
+Multigrid of the process; each instance keeps its own partial-sum scratch.
+Where the coarsest edge is not 4..24 in steps of 4, or the operator would
+exceed ``COARSE_OP_MAX_BYTES``, the sweeps run as before.
 """
 from __future__ import annotations
 
@@ -27,6 +35,9 @@ from . import _abi
 from .fields import DeviceField, cuda_device
 
 NPL_MG = 1  # one ring layer per level (reference multigrid.py:20)
+COARSE_OP_MAX_BYTES = 2 * 1024 ** 3
+
+_COARSE_OPS = {}  # (device, n, nlev, h, n_coarse, dtype) -> built operator tensor
 
 
 class _CoeffView:
@@ -76,11 +87,15 @@ class _Level:
 
 
 class Multigrid:
-    def __init__(self, cfg, topo, device, dx, dy, dz, precision=None):
+    def __init__(self, cfg, topo, device, dx, dy, dz, precision=None, coarse=None):
         self.cfg = cfg
         self.precision = precision or getattr(cfg.numerics, "mg_precision", "fp64")
         if self.precision not in ("fp64", "mixed"):
             raise ValueError("precision must be 'fp64' or 'mixed'")
+        self.coarse = coarse or getattr(cfg.numerics, "mg_coarse", "operator")
+        if self.coarse not in ("operator", "sweeps"):
+            raise ValueError("coarse must be 'operator' or 'sweeps'")
+        self._cop_part = None
         self.topo = topo
         self.device = cuda_device(device)
         nb = topo.local_ncells
@@ -115,6 +130,31 @@ class Multigrid:
     def _stream(self):
         return ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
 
+    def _coarse_op(self, c):
+        """(operator, scratch) tensors for case `c` of the full hierarchy, or
+        None when the coarse sweeps run as sweeps."""
+        if self.coarse != "operator" or c.nlev < 2:
+            return None
+        op_e, sc_e = ctypes.c_int64(), ctypes.c_int64()
+        if _abi.load().wf_mg_coarse_op_elems(c.n, c.nlev, ctypes.byref(op_e),
+                                            ctypes.byref(sc_e)) != 0:
+            return None
+        dt = torch.float32 if c.mg_fp32 else torch.float64
+        if op_e.value * (4 if c.mg_fp32 else 8) > COARSE_OP_MAX_BYTES:
+            return None
+        key = (self.device.index, c.n, c.nlev, c.dx, c.dy, c.dz, c.n_coarse, str(dt))
+        op = _COARSE_OPS.get(key)
+        if op is None:
+            op = torch.empty(op_e.value, dtype=dt, device=self.device)
+            c.mg_cop = op.data_ptr()
+            _abi.call("wf_mg_build_coarse_op", ctypes.byref(c), self._stream())
+            torch.cuda.current_stream(self.device).synchronize()
+            _COARSE_OPS[key] = op
+        if self._cop_part is None or self._cop_part.numel() != sc_e.value \
+                or self._cop_part.dtype != dt:
+            self._cop_part = torch.empty(sc_e.value, dtype=dt, device=self.device)
+        return op, self._cop_part
+
     def case(self, su=None, pp=None, levels=None) -> _abi.WfCase:
         """The wf_case the multigrid entry points read (levels >= 1 buffers,
         sweep counts, spacing); ``su``/``pp`` are set for ``solve``."""
@@ -140,6 +180,10 @@ class Multigrid:
                 for l, lev in enumerate(levels):
                     if lev in self.levels:
                         c.mg_tmp[l] = self._tmp64[self.levels.index(lev)].ptr
+        if levels is self.levels:
+            cop = self._coarse_op(c)
+            if cop is not None:
+                c.mg_cop, c.mg_cop_part = cop[0].data_ptr(), cop[1].data_ptr()
         if su is not None:
             c.fld[_abi.FIELD_NAMES.index("su")] = su.ptr
         if pp is not None:

@@ -26,6 +26,7 @@ import torch
 from . import _abi
 from .ensemble import cavity_case
 from .fields import cuda_device
+from .multigrid import COARSE_OP_MAX_BYTES
 from .solver import FlowSolver
 from .topology import build_topology
 
@@ -35,9 +36,11 @@ NFIELDS = 13
 def case_bytes(n, levels=3, precision="mixed"):
     """Device bytes a FlowSolver of an n^3 case allocates: 13 padded FP64
     fields, FP64 multigrid levels (phi, rhs with one ring, level 0
-    included), the FP32 copies of every level in mixed precision, one sweep
-    buffer per level in the multigrid's precision, and two scalar blocks
-    plus one residual slot."""
+    included), the FP32 copies of every level in mixed precision, a scratch
+    of two level arrays per level in the multigrid's precision, the
+    partial-sum scratch of the coarse-level operator (32 coarse-level
+    arrays; the operator itself is shared by every case of the size), and
+    two scalar blocks plus one residual slot."""
     fields = NFIELDS * (n + 6) ** 3 * 8
     mg = 0
     for l in range(levels):
@@ -47,6 +50,10 @@ def case_bytes(n, levels=3, precision="mixed"):
             mg += 2 * m ** 3 * 4 + 2 * m ** 3 * 4
         else:
             mg += 2 * m ** 3 * 8
+    nc = n >> (levels - 1)
+    word = 4 if precision == "mixed" else 8
+    if levels > 1 and nc in (4, 8, 12, 16, 20, 24) and nc ** 6 * word <= COARSE_OP_MAX_BYTES:
+        mg += 32 * nc ** 3 * word
     return fields + mg + 2 * ctypes.sizeof(_abi.WfScalars) + 8
 
 

@@ -218,8 +218,9 @@ class FlowSolver:
                 "iters": self.outer_iters, "cfl": self.cfl}
 
     def device_bytes(self):
-        """Device memory held by this solver's fields, multigrid hierarchy
-        and scalar block."""
+        """Device memory held by this solver's fields, multigrid hierarchy,
+        scratch and scalar block (a coarse-level operator is shared by all
+        solvers of its size and not counted here)."""
         ts = [f.t for f in self.f.values()] + [self._sc]
         for lev in self.mg.levels:
             ts += [lev.phi.t, lev.rhs.t]
@@ -227,6 +228,8 @@ class FlowSolver:
             ts += [a.t, b.t]
         ts += [t.t for t in self.mg._tmp]
         ts += [self.mg._sc, self.mg._out]
+        if self.mg._cop_part is not None:   # the coarse operator itself is shared
+            ts.append(self.mg._cop_part)
         return int(sum(t.numel() * t.element_size() for t in ts))
 
     def close(self):
