@@ -139,6 +139,10 @@ WF_API int wf_mg_level_elems(int32_t n, int32_t nlev, int32_t level, int64_t* el
 WF_API int wf_mg_coarse_op_elems(int32_t n, int32_t nlev, int64_t* op_elems,
                                  int64_t* scratch_elems);
 WF_API int wf_mg_build_coarse_op(const wf_case* c, void* stream);
+/* The coarsest-level solve of a V-cycle (multigrid.py:301-322, coarsest
+ * level: phi from zero, n_coarse sweeps) on an explicit FP64 pair of
+ * (n_c+2)^3 doubles: through c->mg_cop when it is set, else as sweeps. */
+WF_API int wf_mg_coarse_solve(const wf_case* c, double* phi, const double* rhs, void* stream);
 
 /* ---- initial state ---------------------------------------------------- */
 /* kernels.py:452-471 init_noise: u = v = amp*r, w = -amp*r (uint32 hash). */

@@ -1113,16 +1113,25 @@ static int try_coarse_tb(const Lvl<T>& L, int nsweeps, cudaStream_t s, int* rc) 
 // split over COP_CH row chunks with partial sums in fixed order (chunk
 // partials, then chunks in ascending order), so results do not depend on
 // scheduling: a case computes the same bits alone or beside other cases.
-constexpr int COP_CH = 32;
+constexpr int COP_CH = 64;
 
 static bool cop_size_ok(int nc) {
   return nc == 4 || nc == 8 || nc == 12 || nc == 16 || nc == 20 || nc == 24;
 }
 
+template <class T> struct Vec2;
+template <> struct Vec2<double> { using type = double2; };
+template <> struct Vec2<float> { using type = float2; };
+
+// grid (ceil(N/512), COP_CH): a thread owns outputs i, i+1 (one 2-vector
+// load per operator row) and runs 8 rows at a time, each row with its own
+// pair of accumulators, so 8 vector loads are in flight per thread
 template <class T>
 __global__ void __launch_bounds__(256) k_cop_partial(const T* __restrict__ op, const Lvl<T> L,
                                                      T* __restrict__ part) {
   pdl_entry();
+  using V = typename Vec2<T>::type;
+  constexpr int U = 8;
   __shared__ T rs[512];
   const int n = L.n, N = n * n * n;
   const int jc = (N + COP_CH - 1) / COP_CH;
@@ -1134,20 +1143,38 @@ __global__ void __launch_bounds__(256) k_cop_partial(const T* __restrict__ op, c
     rs[t] = L.rhs[lid(L, a + 1, b + 1, cc + 1)];
   }
   __syncthreads();
-  const int i = blockIdx.x * 256 + threadIdx.x;
-  if (i >= N) return;
-  const T* col = op + (long)j0 * N + i;
-  T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+  const int i = 2 * (blockIdx.x * 256 + threadIdx.x);
+  if (i >= N) return;   // N is even: i+1 < N as well
+  const V* col = reinterpret_cast<const V*>(op + (long)j0 * N + i);
+  const long rowv = N / 2;   // one operator row in 2-vectors
+  T ax[U], ay[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) ax[u] = ay[u] = T(0);
   const int cnt = j1 - j0;
   int t = 0;
-  for (; t + 4 <= cnt; t += 4) {
-    a0 = fma(rs[t], col[(long)t * N], a0);
-    a1 = fma(rs[t + 1], col[(long)(t + 1) * N], a1);
-    a2 = fma(rs[t + 2], col[(long)(t + 2) * N], a2);
-    a3 = fma(rs[t + 3], col[(long)(t + 3) * N], a3);
+  for (; t + U <= cnt; t += U) {
+    V v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) v[u] = __ldg(col + (long)(t + u) * rowv);
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      ax[u] = fma(rs[t + u], v[u].x, ax[u]);
+      ay[u] = fma(rs[t + u], v[u].y, ay[u]);
+    }
   }
-  for (; t < cnt; ++t) a0 = fma(rs[t], col[(long)t * N], a0);
-  part[(long)blockIdx.y * N + i] = (a0 + a1) + (a2 + a3);
+  for (; t < cnt; ++t) {
+    const V v = __ldg(col + (long)t * rowv);
+    ax[0] = fma(rs[t], v.x, ax[0]);
+    ay[0] = fma(rs[t], v.y, ay[0]);
+  }
+  T sx = T(0), sy = T(0);
+#pragma unroll
+  for (int u = 0; u < U; ++u) {   // fixed order
+    sx += ax[u];
+    sy += ay[u];
+  }
+  part[(long)blockIdx.y * N + i] = sx;
+  part[(long)blockIdx.y * N + i + 1] = sy;
 }
 
 template <class T>
@@ -1171,7 +1198,7 @@ __global__ void __launch_bounds__(256) k_cop_finish(const T* __restrict__ part, 
 template <class T>
 static int apply_coarse_op(const Lvl<T>& L, const T* op, T* part, cudaStream_t s) {
   const int N = L.n * L.n * L.n;
-  WF_CK(launch_k(k_cop_partial<T>, dim3((N + 255) / 256, COP_CH), 256, 0, s, op, L, part));
+  WF_CK(launch_k(k_cop_partial<T>, dim3((N + 511) / 512, COP_CH), 256, 0, s, op, L, part));
   WF_CKL("k_cop_partial");
   WF_CK(launch_k(k_cop_finish<T>, (N + 255) / 256, 256, 0, s, (const T*)part, L));
   WF_CKL("k_cop_finish");
@@ -2063,6 +2090,34 @@ int mg_relax_pair(const wf_case& c, double* phi0, const double* rhs0, int nsweep
   std::vector<Lvl<double>> lv;
   WF_TRY(build_levels<double>(c, phi0, rhs0, m * m, m, lv));
   return relax<double>(lv[0], nsweeps, s);
+}
+
+// the coarsest-level solve of a V-cycle on an explicit (n_c+2)^3 pair: phi
+// from zero by the case's coarse operator when it has one, else n_coarse
+// sweeps
+int mg_coarse_solve_pair(const wf_case& c, double* phi, const double* rhs, cudaStream_t s) {
+  if (c.nlev < 2) return fail(WF_EINVAL, "coarse solve needs nlev >= 2");
+  const int l = c.nlev - 1;
+  Lvl<double> L = {};
+  L.n = c.n >> l;
+  if ((L.n << l) != c.n || L.n < 1) return fail(WF_EINVAL, "n must be divisible by 2^(nlev-1)");
+  const double s2 = (double)(1 << l);
+  const double dxl = c.dx * s2, dyl = c.dy * s2, dzl = c.dz * s2;
+  L.ax = 1.0 / (dxl * dxl);
+  L.ay = 1.0 / (dyl * dyl);
+  L.az = 1.0 / (dzl * dzl);
+  L.phi = phi;
+  L.rhs = rhs;
+  L.sJ = L.n + 2;
+  L.sI = (long)(L.n + 2) * (L.n + 2);
+  L.err = c.sc ? &c.sc->status : nullptr;
+  L.gbar = c.sc ? c.sc->gbar : nullptr;
+  const long m = (long)L.n + 2;
+  WF_CK(launch_k(k_zero<double>, mg_blocks(m * m * m), MG_TPB, 0, s, phi, m * m * m));
+  WF_CKL("k_zero");
+  if (c.mg_cop && c.mg_cop_part && !c.mg_fp32 && cop_size_ok(L.n))
+    return apply_coarse_op<double>(L, (const double*)c.mg_cop, (double*)c.mg_cop_part, s);
+  return relax<double>(L, c.n_coarse, s);
 }
 
 __global__ void k_refill(Lvl<double> L) {

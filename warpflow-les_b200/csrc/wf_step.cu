@@ -341,6 +341,11 @@ int wf_mg_coarse_op_elems(int32_t n, int32_t nlev, int64_t* op_elems, int64_t* s
   return coarse_op_elems(n, nlev, op_elems, scratch_elems);
 }
 
+int wf_mg_coarse_solve(const wf_case* c, double* phi, const double* rhs, void* s) {
+  if (!c || !phi || !rhs) return fail(WF_EINVAL, "null argument");
+  return mg_coarse_solve_pair(*c, phi, rhs, (cudaStream_t)s);
+}
+
 int wf_mg_build_coarse_op(const wf_case* c, void* s) {
   if (!c) return fail(WF_EINVAL, "null argument");
   return build_coarse_op_case(*c, (cudaStream_t)s);

@@ -89,6 +89,7 @@ SIGNATURES = {
     "wf_mg_coarse_op_elems": (_I32, [_I32, _I32, ctypes.POINTER(ctypes.c_int64),
                                      ctypes.POINTER(ctypes.c_int64)]),
     "wf_mg_build_coarse_op": (_I32, [_CP, _VP]),
+    "wf_mg_coarse_solve": (_I32, [_CP, _VP, _VP, _VP]),
     "wf_init_noise": (_I32, [_VP, _VP, _VP, _I32, _D, _I32, _VP]),
     "wf_fill_initial": (_I32, [_CP, _VP]),
     "wf_fill_u": (_I32, [_VP, _I32, _D, _VP]),

@@ -201,6 +201,17 @@ class Multigrid:
         _abi.call("wf_mg_relax", ctypes.byref(c), lev.phi.ptr, lev.rhs.ptr,
                   int(nsweeps), self._stream())
 
+    def _coarse_solve(self):
+        """The V-cycle's coarsest-level solve on the harness arrays of the
+        coarsest level: phi from zero, by the coarse operator when this
+        Multigrid uses one, else n_coarse sweeps."""
+        lev = self.levels[-1]
+        c = self.case()
+        if c.mg_fp32:   # the FP32 operator serves FP32 levels only
+            c.mg_cop = c.mg_cop_part = None
+        _abi.call("wf_mg_coarse_solve", ctypes.byref(c), lev.phi.ptr, lev.rhs.ptr,
+                  self._stream())
+
     def _vcycle(self):
         """One V-cycle on level 0 (multigrid.py:301-322); in mixed precision
         one FP64 defect-correction cycle around an FP32 V-cycle."""

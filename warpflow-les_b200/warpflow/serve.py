@@ -38,7 +38,7 @@ def case_bytes(n, levels=3, precision="mixed"):
     fields, FP64 multigrid levels (phi, rhs with one ring, level 0
     included), the FP32 copies of every level in mixed precision, a scratch
     of two level arrays per level in the multigrid's precision, the
-    partial-sum scratch of the coarse-level operator (32 coarse-level
+    partial-sum scratch of the coarse-level operator (64 coarse-level
     arrays; the operator itself is shared by every case of the size), and
     two scalar blocks plus one residual slot."""
     fields = NFIELDS * (n + 6) ** 3 * 8
@@ -53,7 +53,7 @@ def case_bytes(n, levels=3, precision="mixed"):
     nc = n >> (levels - 1)
     word = 4 if precision == "mixed" else 8
     if levels > 1 and nc in (4, 8, 12, 16, 20, 24) and nc ** 6 * word <= COARSE_OP_MAX_BYTES:
-        mg += 32 * nc ** 3 * word
+        mg += 64 * nc ** 3 * word
     return fields + mg + 2 * ctypes.sizeof(_abi.WfScalars) + 8
 
 
