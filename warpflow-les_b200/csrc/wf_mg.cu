@@ -1388,7 +1388,7 @@ static int split_min_n() {
   static int v = -1;
   if (v < 0) {
     const char* e = getenv("WF_SPLIT_MIN");
-    v = e ? atoi(e) : 128;
+    v = e ? atoi(e) : 80;
   }
   return v;
 }
