@@ -1383,14 +1383,16 @@ __global__ void __launch_bounds__(32 * SPLIT_ROWS)
   }
 }
 
-// smallest even level edge that relaxes on the split copy (WF_SPLIT_MIN overrides)
-static int split_min_n() {
+// smallest even level edge that relaxes on the split copy (WF_SPLIT_MIN
+// overrides both): 80 for FP64, 128 for FP32, whose 80^3 level stays in L2
+// (step time at 80^3, FP64 1.332 ms split vs 1.348 in place; mixed 1.255 vs 1.184)
+static int split_min_n(bool fp32) {
   static int v = -1;
   if (v < 0) {
     const char* e = getenv("WF_SPLIT_MIN");
-    v = e ? atoi(e) : 80;
+    v = e ? atoi(e) : 0;
   }
-  return v;
+  return v > 0 ? v : (fp32 ? 128 : 80);
 }
 
 // rhs_ready: the scratch already holds the split rhs of this level (the
@@ -1785,7 +1787,7 @@ static int relax(const Lvl<T>& L, int nsweeps, cudaStream_t s, bool rhs_ready = 
     if (nsweeps > 12 && strat == 1 && try_coarse_cluster<T>(L, nsweeps, s, &rc)) return rc;
     if (try_coarse<T>(L, nsweeps, s, &rc)) return rc;
   }
-  if (L.tmp && (L.n & 1) == 0 && L.n >= split_min_n())
+  if (L.tmp && (L.n & 1) == 0 && L.n >= split_min_n(sizeof(T) == 4))
     return relax_split<T>(L, nsweeps, rhs_ready, s);
   {
     int rc = WF_OK;
