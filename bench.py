@@ -383,7 +383,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--mode", default="step", choices=["step", "ensemble", "serve", "poisson"])
     ap.add_argument("--cases", type=int, default=64)
-    ap.add_argument("--streams", type=int, default=16)
+    ap.add_argument("--streams", type=int, default=32)
     ap.add_argument("--requests", type=int, default=48)
     ap.add_argument("--step-scale", type=float, default=0.05)
     args = ap.parse_args()

@@ -65,7 +65,7 @@ class Ensemble:
     info dict per case (or the exception a case raised, which retires it).
     """
 
-    def __init__(self, cfgs, device="cuda:0", nstreams=16):
+    def __init__(self, cfgs, device="cuda:0", nstreams=32):
         self.device = cuda_device(device)
         # Concurrent cases: kernels that wait for their predecessor while
         # resident would hold SMs other streams could use.
