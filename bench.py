@@ -259,7 +259,7 @@ def bench_ensemble(args):
 
     def run(precision, concurrent, steps, warm):
         cfgs = [cavity_case(sp.n, sp.re, sp.ulid, precision=precision) for sp in specs]
-        ens = Ensemble(cfgs, nstreams=args.streams if concurrent else 1)
+        ens = Ensemble(cfgs, nstreams=(args.streams or 32) if concurrent else 1)
         for _ in range(warm):
             ens.step()
         torch.cuda.synchronize()
@@ -285,7 +285,7 @@ def bench_ensemble(args):
         "ms_per_batch_step": round(1e3 * dt / K, 3), "iters_mean": round(iters, 2),
         "plain_fp64_per_case_loop": round(plain, 2),
         "speedup_vs_plain": round(val / plain, 2),
-        "config": {"cases": args.cases, "streams": args.streams,
+        "config": {"cases": args.cases, "streams": args.streams or 32,
                    "sizes": sorted({sp.n for sp in specs}),
                    "seed": 0, "timing": "wall clock around whole batch steps, synced"}}),
         flush=True)
@@ -298,7 +298,7 @@ def bench_serve(args):
     from warpflow.serve import CavityServer, poisson_stream
     reqs = poisson_stream(count=args.requests, rate=20.0, seed=0,
                           step_scale=args.step_scale)
-    srv = CavityServer(budget_bytes=150 * 10 ** 9, nstreams=args.streams)
+    srv = CavityServer(budget_bytes=150 * 10 ** 9, nstreams=args.streams or 16)
     srv.run(reqs)
     s = srv.summary()
     print(json.dumps({
@@ -308,7 +308,7 @@ def bench_serve(args):
         "wall_s": round(s["wall_s"], 2), "step_batches": s["step_batches"],
         "peak_resident_GB": round(s["peak_resident_bytes"] / 1e9, 3),
         "config": {"requests": args.requests, "rate_per_s": 20.0, "seed": 0,
-                   "step_scale": args.step_scale, "budget_GB": 150, "streams": args.streams,
+                   "step_scale": args.step_scale, "budget_GB": 150, "streams": args.streams or 16,
                    "latency": "arrival to end of last step, wall clock"}}), flush=True)
 
 
@@ -383,7 +383,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--mode", default="step", choices=["step", "ensemble", "serve", "poisson"])
     ap.add_argument("--cases", type=int, default=64)
-    ap.add_argument("--streams", type=int, default=32)
+    ap.add_argument("--streams", type=int, default=None,
+                    help="stream pool (default: 32 for --mode ensemble, 16 for --mode serve)")
     ap.add_argument("--requests", type=int, default=48)
     ap.add_argument("--step-scale", type=float, default=0.05)
     args = ap.parse_args()
