@@ -43,11 +43,15 @@ struct Lvl {
   T* tmp;        // scratch of two level arrays: split copies / one-launch sweeps (may be null)
   long tI, tJ;   // its strides
   unsigned* gbar;  // two words of grid-barrier state (may be null)
+  int split = 0;   // phi/rhs stored row-parity split (see k_rbgs_split)
 };
+
+// position of array index a within a row of the row-parity-split layout
+__host__ __device__ __forceinline__ int spos(int a, int H) { return (a & 1) * H + (a >> 1); }
 
 template <class T>
 __device__ __forceinline__ long lid(const Lvl<T>& L, int i, int j, int k) {
-  return (long)i * L.sI + (long)j * L.sJ + k;
+  return (long)i * L.sI + (long)j * L.sJ + (L.split ? spos(k, (L.n + 2) >> 1) : k);
 }
 
 // write the face-ring mirrors of real cell (i,j,k) (0-based) with value x
@@ -155,8 +159,9 @@ __global__ void __launch_bounds__(MG_TPB) k_restrict(const Lvl<T> F, T* rhs_c, L
           const T ab = k > 0 ? F.az : T(0), at = k < n - 1 ? F.az : T(0);
           const T ap = -(aw + ae + as + an + ab + at);
           const T* p = F.phi;
+          const long cb = lid(F, i + 1, j + 1, k), ct = lid(F, i + 1, j + 1, k + 2);
           const T res = F.rhs[c] - (aw * p[c - F.sI] + ae * p[c + F.sI] + as * p[c - F.sJ] +
-                                    an * p[c + F.sJ] + ab * p[c - 1] + at * p[c + 1] +
+                                    an * p[c + F.sJ] + ab * p[cb] + at * p[ct] +
                                     ap * p[c]);
           acc = acc + res;
         }
@@ -221,7 +226,7 @@ __global__ void __launch_bounds__(MG_TPB) k_prolong(const Lvl<T> C, Lvl<T> F) {
     const long c = lid(F, i + 1, j + 1, k + 1);
     const T x = F.phi[c] + acc;
     F.phi[c] = x;
-    ring_mirror(F, i, j, k, c, x);
+    if (!F.split) ring_mirror(F, i, j, k, c, x);
   }
 }
 
@@ -1283,8 +1288,6 @@ static int try_coarse_cluster(const Lvl<T>& L, int nsweeps, cudaStream_t s, int*
 // has the ring of the original (face-ring values only ever meet a zero
 // coefficient); copying back writes the real cells and their face-ring
 // mirrors, which is what k_rbgs leaves in the ring after the last sweep.
-__device__ __forceinline__ int spos(int a, int H) { return (a & 1) * H + (a >> 1); }
-
 constexpr int SPLIT_ROWS = 8;  // rows (one warp each) per CTA
 
 // level phi (all (n+2)^3 cells) and rhs -> split copies sp, sr (dense strides)
@@ -1395,31 +1398,95 @@ static int split_min_n(bool fp32) {
   return v > 0 ? v : (fp32 ? 128 : 80);
 }
 
-// rhs_ready: the scratch already holds the split rhs of this level (the
-// level's rhs has not changed since the last split relax of it)
+// level -> split copies (phi, and rhs unless the scratch already holds it)
 template <class T>
-static int relax_split(const Lvl<T>& L, int nsweeps, bool rhs_ready, cudaStream_t s) {
+static int split_in(const Lvl<T>& L, bool with_rhs, cudaStream_t s) {
   const int m = L.n + 2;
   T* sp = L.tmp;
   T* sr = L.tmp + (long)m * m * m;
-  const int nb_all = (m * m + SPLIT_ROWS - 1) / SPLIT_ROWS;
-  const int nb = (L.n * L.n + SPLIT_ROWS - 1) / SPLIT_ROWS;
+  WF_CK(launch_k(k_split_in<T>, (m * m + SPLIT_ROWS - 1) / SPLIT_ROWS, 32 * SPLIT_ROWS, 0, s, L,
+                 sp, sr, with_rhs ? 1 : 0));
+  WF_CKL("k_split_in");
+  return WF_OK;
+}
+
+// the half-sweeps of a relax on the split copies
+template <class T>
+static int split_sweeps(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
+  const int m = L.n + 2;
+  T* sp = L.tmp;
+  const T* sr = L.tmp + (long)m * m * m;
   const int cpt = split_cpt();
   const dim3 grid((L.n / 2 + 32 * cpt - 1) / (32 * cpt), (L.n + SPLIT_ROWS - 1) / SPLIT_ROWS,
                   L.n);
   const ApRecip<T> rt = ap_recip(L);
   auto kern = cpt == 4 ? k_rbgs_split<T, 4> : cpt == 2 ? k_rbgs_split<T, 2> : k_rbgs_split<T, 1>;
-  WF_CK(launch_k(k_split_in<T>, nb_all, 32 * SPLIT_ROWS, 0, s, L, sp, sr, rhs_ready ? 0 : 1));
-  WF_CKL("k_split_in");
   for (int it = 0; it < nsweeps; ++it) {
     for (int color = 0; color < 2; ++color) {
-      WF_CK(launch_k(kern, grid, dim3(32, SPLIT_ROWS), 0, s, L, sp, (const T*)sr, color, rt));
+      WF_CK(launch_k(kern, grid, dim3(32, SPLIT_ROWS), 0, s, L, sp, sr, color, rt));
       WF_CKL("k_rbgs_split");
     }
   }
-  WF_CK(launch_k(k_split_out<T>, nb, 32 * SPLIT_ROWS, 0, s, L, (const T*)sp));
+  return WF_OK;
+}
+
+// split copy of phi -> the level's real cells and face-ring mirrors
+template <class T>
+static int split_out(const Lvl<T>& L, cudaStream_t s) {
+  WF_CK(launch_k(k_split_out<T>, (L.n * L.n + SPLIT_ROWS - 1) / SPLIT_ROWS, 32 * SPLIT_ROWS, 0,
+                 s, L, (const T*)L.tmp));
   WF_CKL("k_split_out");
   return WF_OK;
+}
+
+// rhs_ready: the scratch already holds the split rhs of this level (the
+// level's rhs has not changed since the last split relax of it)
+template <class T>
+static int relax_split(const Lvl<T>& L, int nsweeps, bool rhs_ready, cudaStream_t s) {
+  WF_TRY(split_in(L, !rhs_ready, s));
+  WF_TRY(split_sweeps(L, nsweeps, s));
+  return split_out(L, s);
+}
+
+// The V-cycle keeps large levels in the split layout from their
+// pre-smoothing to their post-smoothing: restriction reads and writes split
+// views, prolongation adds into them, and only level 0 is copied in and out
+// once per V-cycle.  A split view addresses the scratch copies through lid().
+template <class T>
+static Lvl<T> split_view(const Lvl<T>& L) {
+  Lvl<T> V = L;
+  const long m = (long)L.n + 2;
+  V.phi = L.tmp;
+  V.rhs = L.tmp + m * m * m;
+  V.sI = L.tI;
+  V.sJ = L.tJ;
+  V.split = 1;
+  return V;
+}
+
+// face-ring mirrors of a split view (what k_rbgs leaves in the ring; the
+// prolongation out of this level reads them)
+template <class T>
+__global__ void __launch_bounds__(256) k_split_ring(const Lvl<T> V) {
+  pdl_entry();
+  const int n = V.n;
+  const int t = blockIdx.x * 256 + threadIdx.x;
+  if (t >= 6 * n * n) return;
+  const int face = t / (n * n), r = t - face * n * n;
+  const int a = r / n + 1, b = r % n + 1;   // the two in-face coordinates, 1..n
+  const int lo = (face & 1) ? n + 1 : 0, in = (face & 1) ? n : 1;
+  long dst, src;
+  if (face < 2) {
+    dst = lid(V, lo, a, b);
+    src = lid(V, in, a, b);
+  } else if (face < 4) {
+    dst = lid(V, a, lo, b);
+    src = lid(V, a, in, b);
+  } else {
+    dst = lid(V, a, b, lo);
+    src = lid(V, a, b, in);
+  }
+  V.phi[dst] = V.phi[src];
 }
 
 // ---- one whole red-black sweep per launch (fine levels) -------------------
@@ -1838,33 +1905,62 @@ static int relax(const Lvl<T>& L, int nsweeps, cudaStream_t s, bool rhs_ready = 
   return WF_OK;
 }
 
+// a level the V-cycle keeps in the split layout: one that relax() would send
+// to relax_split for both smoothings
+template <class T>
+static bool split_resident(const Lvl<T>& L, const wf_case& c) {
+  return L.tmp && (L.n & 1) == 0 && L.n > 24 && L.n >= split_min_n(sizeof(T) == 4) &&
+         c.n_pre >= 1 && c.n_pre <= 12 && c.n_post >= 1 && c.n_post <= 12;
+}
+
 // rhs0_ready: level 0's rhs is unchanged since the previous V-cycle relaxed
 // it (a solve's V-cycles share rhs = su)
 template <class T>
 static int vcycle(std::vector<Lvl<T>>& lv, const wf_case& c, cudaStream_t s,
                   bool rhs0_ready = false) {
   const int L = (int)lv.size();
+  std::vector<Lvl<T>> vw(lv);    // the views restriction and prolongation work on
+  std::vector<char> res(L, 0);   // level kept split from pre- to post-smoothing
+  for (int l = 0; l + 1 < L; ++l)
+    if (split_resident(lv[l], c)) {
+      res[l] = 1;
+      vw[l] = split_view(lv[l]);
+    }
   for (int l = 0; l < L; ++l) {
     if (l > 0) {
-      Lvl<T>& C = lv[l];
+      Lvl<T>& C = vw[l];
       const long m = (long)C.n + 2;
       WF_CK(launch_k(k_zero<T>, mg_blocks(m * m * m), MG_TPB, 0, s, C.phi, m * m * m));
       WF_CKL("k_zero");
       WF_CK(launch_k(k_restrict<T>, cells3(C.n, C.n, C.n), cell_block(), 0, s,
-          lv[l - 1], const_cast<T*>(C.rhs), C));
+          vw[l - 1], const_cast<T*>(C.rhs), C));
       WF_CKL("k_restrict");
+    } else if (res[0]) {
+      WF_TRY(split_in(lv[0], !rhs0_ready, s));
     }
     if (l == L - 1 && L > 1 && c.mg_cop && c.mg_cop_part && cop_size_ok(lv[l].n))
       WF_TRY(apply_coarse_op<T>(lv[l], (const T*)c.mg_cop, (T*)c.mg_cop_part, s));
+    else if (res[l])
+      WF_TRY(split_sweeps(lv[l], c.n_pre, s));
     else
       WF_TRY(relax(lv[l], l < L - 1 ? c.n_pre : c.n_coarse, s, l == 0 && rhs0_ready));
   }
   for (int l = L - 2; l >= 0; --l) {
-    WF_CK(launch_k(k_prolong<T>, cells3(lv[l].n, lv[l].n, lv[l].n), cell_block(), 0, s, lv[l + 1],
-                                                                                 lv[l]));
+    WF_CK(launch_k(k_prolong<T>, cells3(lv[l].n, lv[l].n, lv[l].n), cell_block(), 0, s,
+                   vw[l + 1], vw[l]));
     WF_CKL("k_prolong");
-    // the rhs of level l is the one its pre-smoothing saw
-    WF_TRY(relax(lv[l], c.n_post, s, c.n_pre > 0 || (l == 0 && rhs0_ready)));
+    if (res[l]) {
+      WF_TRY(split_sweeps(lv[l], c.n_post, s));
+      if (l > 0) {
+        WF_CK(launch_k(k_split_ring<T>, (6 * lv[l].n * lv[l].n + 255) / 256, 256, 0, s, vw[l]));
+        WF_CKL("k_split_ring");
+      } else {
+        WF_TRY(split_out(lv[0], s));
+      }
+    } else {
+      // the rhs of level l is the one its pre-smoothing saw
+      WF_TRY(relax(lv[l], c.n_post, s, c.n_pre > 0 || (l == 0 && rhs0_ready)));
+    }
   }
   return WF_OK;
 }
