@@ -147,7 +147,8 @@ def load_peaks():
 
 # DRAM bytes per launch of the dominant kernels, from the ncu captures
 # summarised under profiles/ (dram__bytes_read.sum + dram__bytes_write.sum)
-NCU_TRAFFIC = {("k_rbgs_split", 256): (189055488, "profiles/rbgs_split_256_full.md"),
+NCU_TRAFFIC = {("k_rbgs_split", 256): (189163264, "profiles/rbgs_split_256_full.md"),
+               ("cop", 20): (518313472, "profiles/cop_20_full.md"),
                ("coarse", 20): (172032, "profiles/coarse_p2p_20_full.md")}
 
 
