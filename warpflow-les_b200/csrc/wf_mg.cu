@@ -1914,10 +1914,13 @@ static bool split_resident(const Lvl<T>& L, const wf_case& c) {
 }
 
 // rhs0_ready: level 0's rhs is unchanged since the previous V-cycle relaxed
-// it (a solve's V-cycles share rhs = su)
+// it (a solve's V-cycles share rhs = su).  split0_in: level 0's split copy
+// already holds its current phi (left there by the previous V-cycle);
+// split0_keep: leave the result in the split copy (the next V-cycle of the
+// same solve continues from it) instead of copying it back.
 template <class T>
 static int vcycle(std::vector<Lvl<T>>& lv, const wf_case& c, cudaStream_t s,
-                  bool rhs0_ready = false) {
+                  bool rhs0_ready = false, bool split0_in = false, bool split0_keep = false) {
   const int L = (int)lv.size();
   std::vector<Lvl<T>> vw(lv);    // the views restriction and prolongation work on
   std::vector<char> res(L, 0);   // level kept split from pre- to post-smoothing
@@ -1935,7 +1938,7 @@ static int vcycle(std::vector<Lvl<T>>& lv, const wf_case& c, cudaStream_t s,
       WF_CK(launch_k(k_restrict<T>, cells3(C.n, C.n, C.n), cell_block(), 0, s,
           vw[l - 1], const_cast<T*>(C.rhs), C));
       WF_CKL("k_restrict");
-    } else if (res[0]) {
+    } else if (res[0] && !split0_in) {
       WF_TRY(split_in(lv[0], !rhs0_ready, s));
     }
     if (l == L - 1 && L > 1 && c.mg_cop && c.mg_cop_part && cop_size_ok(lv[l].n))
@@ -1954,7 +1957,7 @@ static int vcycle(std::vector<Lvl<T>>& lv, const wf_case& c, cudaStream_t s,
       if (l > 0) {
         WF_CK(launch_k(k_split_ring<T>, (6 * lv[l].n * lv[l].n + 255) / 256, 256, 0, s, vw[l]));
         WF_CKL("k_split_ring");
-      } else {
+      } else if (!split0_keep) {
         WF_TRY(split_out(lv[0], s));
       }
     } else {
@@ -2170,8 +2173,12 @@ int mg_solve(const wf_case& c, cudaStream_t s) {
   // multigrid.py:332-333: pp and level-0 phi start from zero
   WF_CK(launch_k(k_zero<double>, mg_blocks(P * P * P), MG_TPB, 0, s, pp, P * P * P));
   WF_CKL("k_zero pp");
+  // a level 0 kept in the split layout stays there from the first V-cycle's
+  // copy-in to the last one's copy-out
+  const bool keep = split_resident(lv[0], c) && lv.size() > 1;
   for (int cyc = 0; cyc < c.n_vcycles; ++cyc)
-    WF_TRY(vcycle<double>(lv, c, s, cyc > 0 && (c.n_pre > 0 || c.n_post > 0)));
+    WF_TRY(vcycle<double>(lv, c, s, cyc > 0 && (c.n_pre > 0 || c.n_post > 0),
+                          keep && cyc > 0, keep && cyc + 1 < c.n_vcycles));
   return WF_OK;
 }
 
