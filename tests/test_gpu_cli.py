@@ -64,3 +64,31 @@ def test_resume_is_exact(tmp_path):
     assert c.itime == 6 and info["ctime"] == a.ctime
     for k in ("u", "v", "w", "p", "vis"):
         np.testing.assert_array_equal(c.f[k].numpy(), a.f[k].numpy())
+
+
+def test_async_snapshot_matches_sync(tmp_path):
+    """A snapshot taken by SnapshotWriter while the solver keeps stepping is
+    the same file content as write_snapshot at that step."""
+    from warpflow import FlowSolver, build_topology, load_case
+    from warpflow.io import SnapshotWriter, read_snapshot, write_snapshot
+    cfg = load_case(_case(tmp_path))
+    cfg.output.outdir = str(tmp_path / "async")
+    a = FlowSolver(cfg, build_topology(cfg), "cuda:0")
+    w = SnapshotWriter(a)
+    for _ in range(3):
+        a.step()
+    w.write(3)
+    for _ in range(2):        # later steps overwrite the fields meanwhile
+        a.step()
+    path = w.wait()
+    w.close()
+    cfg2 = load_case(_case(tmp_path))
+    cfg2.output.outdir = str(tmp_path / "sync")
+    b = FlowSolver(cfg2, build_topology(cfg2), "cuda:0")
+    for _ in range(3):
+        b.step()
+    ref = read_snapshot(write_snapshot(b, 3))
+    got = read_snapshot(path)
+    assert sorted(got) == sorted(ref)
+    for k in ref:
+        np.testing.assert_array_equal(got[k], ref[k], err_msg=k)

@@ -16,7 +16,7 @@ import time
 sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 
 from warpflow import FlowSolver, __version__, build_topology, load_case  # noqa: E402
-from warpflow.io import read_snapshot, restore, write_snapshot  # noqa: E402
+from warpflow.io import SnapshotWriter, read_snapshot, restore  # noqa: E402
 
 
 def main(argv=None):
@@ -44,6 +44,7 @@ def main(argv=None):
     if args.resume:
         restore(sol, read_snapshot(args.resume))
         start = sol.itime
+    snaps = SnapshotWriter(sol)
     t0 = time.time()
     for itime in range(start + 1, start + nsteps + 1):
         info = sol.step()
@@ -52,10 +53,11 @@ def main(argv=None):
                   % (itime, info["ctime"], info["dt"], info["rmax"], info["iters"],
                      info["cfl"]), flush=True)
         if itime % cfg.output.n_out == 0:
-            write_snapshot(sol, itime)
+            snaps.write(itime)
     last = start + nsteps
     if last % cfg.output.n_out != 0:
-        write_snapshot(sol, last)
+        snaps.write(last)
+    snaps.close()
     if topo.rank == 0:
         print("done: itime=%d ctime=%.6f wall=%.1fs" % (last, sol.ctime, time.time() - t0),
               flush=True)
