@@ -260,7 +260,10 @@ def bench_ensemble(args):
 
     def run(precision, concurrent, steps, warm):
         cfgs = [cavity_case(sp.n, sp.re, sp.ulid, precision=precision) for sp in specs]
-        ens = Ensemble(cfgs, nstreams=(args.streams or 32) if concurrent else 1)
+        if concurrent:
+            ens = Ensemble(cfgs, nstreams=args.streams or 32, single_graph=args.single_graph)
+        else:
+            ens = Ensemble(cfgs, nstreams=1, single_graph=False)
         for _ in range(warm):
             ens.step()
         torch.cuda.synchronize()
@@ -287,6 +290,7 @@ def bench_ensemble(args):
         "plain_fp64_per_case_loop": round(plain, 2),
         "speedup_vs_plain": round(val / plain, 2),
         "config": {"cases": args.cases, "streams": args.streams or 32,
+                   "single_graph": bool(args.single_graph),
                    "sizes": sorted({sp.n for sp in specs}),
                    "seed": 0, "timing": "wall clock around whole batch steps, synced"}}),
         flush=True)
@@ -386,6 +390,8 @@ def main():
     ap.add_argument("--cases", type=int, default=64)
     ap.add_argument("--streams", type=int, default=None,
                     help="stream pool (default: 32 for --mode ensemble, 16 for --mode serve)")
+    ap.add_argument("--single-graph", type=int, default=1,
+                    help="ensemble: all cases in one CUDA graph (1) or a stream pool (0)")
     ap.add_argument("--requests", type=int, default=48)
     ap.add_argument("--step-scale", type=float, default=0.05)
     args = ap.parse_args()

@@ -236,6 +236,19 @@ WF_API int wf_stepper_step(wf_stepper* s, void* stream);
 WF_API int wf_stepper_launch_counts(const wf_stepper* s, int32_t counts[4]);
 WF_API int wf_stepper_destroy(wf_stepper* s);
 
+/* No counterpart in the reference (its cases run one at a time).  Many
+ * independent cases stepped by ONE graph launch: wf_ensemble_create appends
+ * every case's step (as wf_stepper_create builds it) to a single CUDA graph
+ * as independent branches, so the device schedules all cases' kernels
+ * concurrently without a stream per case.  `cases` are copied; mode 0 or
+ * WF_STEP_SERIAL.  wf_ensemble_step enqueues one step of every case; read
+ * each case's scalar block after the stream finishes. */
+typedef struct wf_ensemble wf_ensemble;
+WF_API int wf_ensemble_create(const wf_case* cases, int32_t ncases, int32_t mode,
+                              wf_ensemble** out);
+WF_API int wf_ensemble_step(wf_ensemble* e, void* stream);
+WF_API int wf_ensemble_destroy(wf_ensemble* e);
+
 #ifdef __cplusplus
 }
 #endif

@@ -19,11 +19,13 @@ def _alone(n, re, ulid, steps, precision):
     return infos, {k: sol.f[k].numpy() for k in ("u", "v", "w", "p", "vis")}
 
 
+@pytest.mark.parametrize("single_graph", [True, False], ids=["one_graph", "streams"])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_ensemble_matches_alone(precision):
+def test_ensemble_matches_alone(precision, single_graph):
     from warpflow.ensemble import Ensemble, cavity_case
     cfgs = [cavity_case(n, re, u, precision=precision) for n, re, u in SPECS]
-    ens = Ensemble(cfgs, nstreams=3)
+    ens = Ensemble(cfgs, nstreams=3, single_graph=single_graph)
+    assert (ens._graph is not None) == single_graph
     steps = 4
     for _ in range(steps):
         infos = ens.step()

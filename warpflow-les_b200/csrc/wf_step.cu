@@ -124,14 +124,15 @@ struct wf_stepper {
   int32_t* hflag;  // pinned, host-loop mode
 };
 
-static int build_graph(wf_stepper* st) {
-  const wf_case& c = st->c;
+// Append one case's step to graph g as an independent branch (its first
+// nodes have no dependencies): the prologue, a WHILE node over calmas and
+// an IF node holding the multigrid part, then the epilogue.  counts gets the
+// launches of each part.
+static int append_step(cudaGraph_t g, const wf_case& c, int32_t counts[4]) {
   cudaStream_t cap;
   WF_CK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
   int rc = WF_OK;
-  cudaGraph_t g = nullptr;
   do {
-    if (cudaGraphCreate(&g, 0) != cudaSuccess) { rc = cuda_fail(cudaGetLastError(), "cudaGraphCreate"); break; }
     cudaGraphConditionalHandle h_loop;
     cudaError_t e = cudaGraphConditionalHandleCreate(&h_loop, g, 1, cudaGraphCondAssignDefault);
     if (e != cudaSuccess) { rc = cuda_fail(e, "cudaGraphConditionalHandleCreate(loop)"); break; }
@@ -139,7 +140,7 @@ static int build_graph(wf_stepper* st) {
     if (e != cudaSuccess) { rc = cuda_fail(e, "cudaStreamBeginCaptureToGraph"); break; }
     long l0 = g_launches;
     rc = step_prologue(c, cap);
-    st->counts[0] = (int32_t)(g_launches - l0);
+    counts[0] = (int32_t)(g_launches - l0);
     cudaGraphNode_t wnode = nullptr;
     cudaGraph_t wbody = nullptr;
     if (rc == WF_OK) {
@@ -163,7 +164,7 @@ static int build_graph(wf_stepper* st) {
       }
       l0 = g_launches;
       if (rc == WF_OK) rc = step_epilogue(c, cap);
-      st->counts[3] = (int32_t)(g_launches - l0);
+      counts[3] = (int32_t)(g_launches - l0);
     }
     cudaGraph_t gout = nullptr;
     e = cudaStreamEndCapture(cap, &gout);
@@ -178,7 +179,7 @@ static int build_graph(wf_stepper* st) {
     if (e != cudaSuccess) { rc = cuda_fail(e, "cudaStreamBeginCaptureToGraph(while)"); break; }
     l0 = g_launches;
     rc = launch_calmas(c, (unsigned long long)h_if, (unsigned long long)h_loop, cap);
-    st->counts[1] = (int32_t)(g_launches - l0);
+    counts[1] = (int32_t)(g_launches - l0);
     cudaGraph_t ibody = nullptr;
     if (rc == WF_OK) {
       cudaStreamCaptureStatus cst;
@@ -209,20 +210,34 @@ static int build_graph(wf_stepper* st) {
     if (e != cudaSuccess) { rc = cuda_fail(e, "cudaStreamBeginCaptureToGraph(if)"); break; }
     l0 = g_launches;
     rc = step_mg_part(c, cap);
-    st->counts[2] = (int32_t)(g_launches - l0);
+    counts[2] = (int32_t)(g_launches - l0);
     e = cudaStreamEndCapture(cap, &gout);
     if (rc == WF_OK && e != cudaSuccess) rc = cuda_fail(e, "cudaStreamEndCapture(if)");
     if (rc != WF_OK) break;
 
-    e = cudaGraphInstantiate(&st->exec, g, 0);
-    if (e != cudaSuccess) { rc = cuda_fail(e, "cudaGraphInstantiate(step)"); break; }
-    st->graph = g;
-    g = nullptr;
   } while (0);
-  if (g) cudaGraphDestroy(g);
   cudaStreamDestroy(cap);
   return rc;
 }
+
+static int build_graph(wf_stepper* st) {
+  cudaGraph_t g = nullptr;
+  WF_CK(cudaGraphCreate(&g, 0));
+  int rc = append_step(g, st->c, st->counts);
+  if (rc == WF_OK) {
+    const cudaError_t e = cudaGraphInstantiate(&st->exec, g, 0);
+    if (e != cudaSuccess) rc = cuda_fail(e, "cudaGraphInstantiate(step)");
+  }
+  if (rc == WF_OK) st->graph = g;
+  else cudaGraphDestroy(g);
+  return rc;
+}
+
+struct wf_ensemble {
+  int ncases;
+  cudaGraph_t graph;
+  cudaGraphExec_t exec;
+};
 
 extern "C" {
 
@@ -415,6 +430,52 @@ int wf_stepper_step(wf_stepper* st, void* stream) {
   l0 = g_launches;
   WF_TRY(step_epilogue(c, s));
   st->counts[3] = (int32_t)(g_launches - l0);
+  return WF_OK;
+}
+
+int wf_ensemble_create(const wf_case* cases, int32_t ncases, int32_t mode, wf_ensemble** out) {
+  if (!cases || !out || ncases < 1) return fail(WF_EINVAL, "null argument or no cases");
+  *out = nullptr;
+  if (mode & ~WF_STEP_SERIAL) return fail(WF_EINVAL, "ensemble mode: 0 or WF_STEP_SERIAL");
+  for (int i = 0; i < ncases; ++i) WF_TRY(validate_case(cases[i]));
+  PdlOff guard((mode & WF_STEP_SERIAL) != 0);
+  cudaGraph_t g = nullptr;
+  WF_CK(cudaGraphCreate(&g, 0));
+  int rc = WF_OK;
+  int32_t counts[4];
+  for (int i = 0; i < ncases && rc == WF_OK; ++i) rc = append_step(g, cases[i], counts);
+  wf_ensemble* en = nullptr;
+  if (rc == WF_OK) {
+    en = new wf_ensemble();
+    en->ncases = ncases;
+    en->graph = g;
+    en->exec = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&en->exec, g, 0);
+    if (e != cudaSuccess) rc = cuda_fail(e, "cudaGraphInstantiate(ensemble)");
+  }
+  if (rc != WF_OK) {
+    if (en) {
+      wf_ensemble_destroy(en);
+    } else {
+      cudaGraphDestroy(g);
+    }
+    return rc;
+  }
+  *out = en;
+  return WF_OK;
+}
+
+int wf_ensemble_step(wf_ensemble* en, void* stream) {
+  if (!en) return fail(WF_EINVAL, "null ensemble");
+  WF_CK(cudaGraphLaunch(en->exec, (cudaStream_t)stream));
+  return WF_OK;
+}
+
+int wf_ensemble_destroy(wf_ensemble* en) {
+  if (!en) return WF_OK;
+  if (en->exec) cudaGraphExecDestroy(en->exec);
+  if (en->graph) cudaGraphDestroy(en->graph);
+  delete en;
   return WF_OK;
 }
 

@@ -115,6 +115,9 @@ SIGNATURES = {
     "wf_stepper_create": (_I32, [_CP, _I32, ctypes.POINTER(_VP)]),
     "wf_stepper_step": (_I32, [_VP, _VP]),
     "wf_stepper_destroy": (_I32, [_VP]),
+    "wf_ensemble_create": (_I32, [_CP, _I32, _I32, ctypes.POINTER(_VP)]),
+    "wf_ensemble_step": (_I32, [_VP, _VP]),
+    "wf_ensemble_destroy": (_I32, [_VP]),
     "wf_stepper_launch_counts": (_I32, [_VP, ctypes.POINTER(_I32)]),
 }
 

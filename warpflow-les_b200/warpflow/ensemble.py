@@ -24,7 +24,7 @@ import torch
 from . import _abi
 from .config import case_from_dict
 from .fields import cuda_device
-from .solver import FlowSolver
+from .solver import STEP_SERIAL, FlowSolver
 from .topology import build_topology
 
 
@@ -63,15 +63,28 @@ class Ensemble:
 
     ``step()`` advances every active case by one time step and returns one
     info dict per case (or the exception a case raised, which retires it).
+
+    With ``single_graph`` (default) all cases' steps also form ONE CUDA graph
+    (``wf_ensemble_create``: every case an independent branch), and a step
+    of the whole ensemble is one graph launch; once a case has retired, or
+    for a subset, the cases' own graphs are launched on a pool of
+    ``nstreams`` streams instead.
     """
 
-    def __init__(self, cfgs, device="cuda:0", nstreams=32):
+    def __init__(self, cfgs, device="cuda:0", nstreams=32, single_graph=True):
         self.device = cuda_device(device)
         # Concurrent cases: kernels that wait for their predecessor while
         # resident would hold SMs other streams could use.
+        concurrent = nstreams > 1 or single_graph
         self.solvers = [FlowSolver(cfg, build_topology(cfg), self.device,
-                                   serial=nstreams > 1) for cfg in cfgs]
+                                   serial=concurrent) for cfg in cfgs]
         self.active = [True] * len(self.solvers)
+        self._graph = None
+        if single_graph and len(self.solvers) > 1:
+            arr = (_abi.WfCase * len(self.solvers))(*[sv.case for sv in self.solvers])
+            self._graph = ctypes.c_void_p()
+            _abi.call("wf_ensemble_create", arr, len(self.solvers), STEP_SERIAL,
+                      ctypes.byref(self._graph))
         ns = max(1, min(nstreams, len(self.solvers)))
         self.streams = [torch.cuda.Stream(self.device) for _ in range(ns)]
         nsc = ctypes.sizeof(_abi.WfScalars)
@@ -95,6 +108,9 @@ class Ensemble:
         """Enqueue one step of the selected cases (default: all active)."""
         idx = self._which(which)
         main = torch.cuda.current_stream(self.device)
+        if self._graph is not None and idx == list(range(len(self.solvers))):
+            _abi.call("wf_ensemble_step", self._graph, ctypes.c_void_p(main.cuda_stream))
+            return idx
         start = torch.cuda.Event()
         start.record(main)
         used = set()
@@ -133,5 +149,8 @@ class Ensemble:
         return self.finish(self.launch(which))
 
     def close(self):
+        if self._graph is not None:
+            _abi.load().wf_ensemble_destroy(self._graph)
+            self._graph = None
         for s in self.solvers:
             s.close()
