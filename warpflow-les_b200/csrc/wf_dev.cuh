@@ -87,4 +87,19 @@ __device__ __forceinline__ bool last_block(unsigned int* ticket) {
   return is_last;
 }
 
+// x / d, correctly rounded, from y = RN(1/d): one residual correction makes
+// the quotient faithful, a second rounds it correctly (P. Markstein,
+// "Computation of elementary functions on the IBM RISC System/6000
+// processor", IBM J. Res. Dev. 34(1), 1990).  Valid away from overflow and
+// underflow, which the solver's values stay far from; four FMAs and a
+// multiply in place of a full division.
+template <class T>
+__device__ __forceinline__ T div_by_recip(T x, T d, T y) {
+  T q = x * y;
+  T r = fma(-q, d, x);
+  q = fma(r, y, q);
+  r = fma(-q, d, x);
+  return fma(r, y, q);
+}
+
 }  // namespace wf

@@ -67,20 +67,6 @@ __device__ __forceinline__ void ring_mirror(const Lvl<T>& L, int i, int j, int k
   if (k == n - 1) L.phi[c + 1] = x;
 }
 
-// x / d, correctly rounded, from y = RN(1/d): one residual correction makes
-// the quotient faithful, a second rounds it correctly (P. Markstein,
-// "Computation of elementary functions on the IBM RISC System/6000
-// processor", IBM J. Res. Dev. 34(1), 1990).  Valid away from overflow and
-// underflow, which the multigrid's values stay far from; four FMAs and a
-// multiply in place of a full division.
-template <class T>
-__device__ __forceinline__ T div_by_recip(T x, T d, T y) {
-  T q = x * y;
-  T r = fma(-q, d, x);
-  q = fma(r, y, q);
-  r = fma(-q, d, x);
-  return fma(r, y, q);
-}
 
 // RN(1/ap) for every boundary pattern of a cell: index 9*cx + 3*cy + cz,
 // c = number of non-zero coefficients along the axis (0, 1 or 2).  ap is

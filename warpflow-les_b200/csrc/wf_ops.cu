@@ -22,6 +22,30 @@ struct Geo {
   }
 };
 
+// The constant divisors of the stage kernels with their reciprocals
+// RN(1/d), computed on the host with the same expressions the kernels use
+// (24h, 12h*h, h, 3): x/d is then div_by_recip(x, d, RN(1/d)), the same
+// correctly rounded quotient as the division.
+struct Divs {
+  double d24[3], y24[3], d12[3], y12[3], dh[3], yh[3], d3, y3;
+};
+
+static inline Divs divs_of(const wf_case& c) {
+  Divs v;
+  const double h[3] = {c.dx, c.dy, c.dz};
+  for (int a = 0; a < 3; ++a) {
+    v.d24[a] = 24.0 * h[a];
+    v.y24[a] = 1.0 / v.d24[a];
+    v.d12[a] = 12.0 * h[a] * h[a];
+    v.y12[a] = 1.0 / v.d12[a];
+    v.dh[a] = h[a];
+    v.yh[a] = 1.0 / h[a];
+  }
+  v.d3 = 3.0;
+  v.y3 = 1.0 / 3.0;
+  return v;
+}
+
 static inline Geo geo_of(int n) {
   Geo g;
   g.n = n;
@@ -123,7 +147,7 @@ int launch_init_noise(double* u, double* v, double* w, int n, double amp, int se
 // and the viscous/advective min in one pass; the last block finishes the
 // dt update on the device.
 // --------------------------------------------------------------------------
-__global__ void __launch_bounds__(TPB) k_checkdt(const wf_case c, Geo g) {
+__global__ void __launch_bounds__(TPB) k_checkdt(const wf_case c, Geo g, const Divs dv) {
   pdl_entry();
   __shared__ double sm[32];
   const double* u = c.fld[WF_U];
@@ -145,7 +169,9 @@ __global__ void __launch_bounds__(TPB) k_checkdt(const wf_case c, Geo g) {
     const double uc = 0.5 * (uu + LD(u, id - g.sI));
     const double vc = 0.5 * (vv + LD(v, id - g.sJ));
     const double wc = 0.5 * (ww + LD(w, id - 1));
-    const double val = 1.0 / (fabs(uc) / dx + fabs(vc) / dy + fabs(wc) / dz +
+    const double val = 1.0 / (div_by_recip(fabs(uc), dv.dh[0], dv.yh[0]) +
+                              div_by_recip(fabs(vc), dv.dh[1], dv.yh[1]) +
+                              div_by_recip(fabs(wc), dv.dh[2], dv.yh[2]) +
                               2.0 * LD(vis, id) * inv2 + 1.0e-30);
     mdt = fmin(mdt, val);
   }
@@ -193,7 +219,7 @@ __global__ void __launch_bounds__(TPB) k_checkdt(const wf_case c, Geo g) {
 
 int launch_checkdt(const wf_case& c, cudaStream_t s) {
   Geo g = geo_of(c.n);
-  WF_CK(launch_k(k_checkdt, reduce_grid(c.n), TPB, 0, s, c, g));
+  WF_CK(launch_k(k_checkdt, reduce_grid(c.n), TPB, 0, s, c, g, divs_of(c)));
   WF_CKL("k_checkdt");
   return WF_OK;
 }
@@ -239,7 +265,7 @@ int launch_copy_oo(const wf_case& c, cudaStream_t s) {
 // --------------------------------------------------------------------------
 // WALE eddy viscosity (kernels.py:297-367)
 // --------------------------------------------------------------------------
-__global__ void __launch_bounds__(TPB) k_wale(const wf_case c, Geo g) {
+__global__ void __launch_bounds__(TPB) k_wale(const wf_case c, Geo g, const Divs dv) {
   pdl_entry();
   const double* u = c.fld[WF_U];
   const double* v = c.fld[WF_V];
@@ -259,15 +285,15 @@ __global__ void __launch_bounds__(TPB) k_wale(const wf_case c, Geo g) {
 #define U_(a) LD(u, id + (a))
 #define V_(a) LD(v, id + (a))
 #define W_(a) LD(w, id + (a))
-    const double dudx = (U_(0) - U_(-sI)) / dx;
-    const double dudy = (0.25 * (U_(sJ) + U_(-sI + sJ) - U_(-sJ) - U_(-sI - sJ))) / dy;
-    const double dudz = (0.25 * (U_(1) + U_(-sI + 1) - U_(-1) - U_(-sI - 1))) / dz;
-    const double dvdx = (0.25 * (V_(sI) + V_(sI - sJ) - V_(-sI) - V_(-sI - sJ))) / dx;
-    const double dvdy = (V_(0) - V_(-sJ)) / dy;
-    const double dvdz = (0.25 * (V_(1) + V_(-sJ + 1) - V_(-1) - V_(-sJ - 1))) / dz;
-    const double dwdx = (0.25 * (W_(sI) + W_(sI - 1) - W_(-sI) - W_(-sI - 1))) / dx;
-    const double dwdy = (0.25 * (W_(sJ) + W_(sJ - 1) - W_(-sJ) - W_(-sJ - 1))) / dy;
-    const double dwdz = (W_(0) - W_(-1)) / dz;
+    const double dudx = div_by_recip(U_(0) - U_(-sI), dv.dh[0], dv.yh[0]);
+    const double dudy = div_by_recip(0.25 * (U_(sJ) + U_(-sI + sJ) - U_(-sJ) - U_(-sI - sJ)), dv.dh[1], dv.yh[1]);
+    const double dudz = div_by_recip(0.25 * (U_(1) + U_(-sI + 1) - U_(-1) - U_(-sI - 1)), dv.dh[2], dv.yh[2]);
+    const double dvdx = div_by_recip(0.25 * (V_(sI) + V_(sI - sJ) - V_(-sI) - V_(-sI - sJ)), dv.dh[0], dv.yh[0]);
+    const double dvdy = div_by_recip(V_(0) - V_(-sJ), dv.dh[1], dv.yh[1]);
+    const double dvdz = div_by_recip(0.25 * (V_(1) + V_(-sJ + 1) - V_(-1) - V_(-sJ - 1)), dv.dh[2], dv.yh[2]);
+    const double dwdx = div_by_recip(0.25 * (W_(sI) + W_(sI - 1) - W_(-sI) - W_(-sI - 1)), dv.dh[0], dv.yh[0]);
+    const double dwdy = div_by_recip(0.25 * (W_(sJ) + W_(sJ - 1) - W_(-sJ) - W_(-sJ - 1)), dv.dh[1], dv.yh[1]);
+    const double dwdz = div_by_recip(W_(0) - W_(-1), dv.dh[2], dv.yh[2]);
 #undef U_
 #undef V_
 #undef W_
@@ -280,7 +306,7 @@ __global__ void __launch_bounds__(TPB) k_wale(const wf_case c, Geo g) {
     const double g2zx = dwdx * dudx + dwdy * dvdx + dwdz * dudz;
     const double g2yz = dvdx * dudz + dvdy * dvdz + dvdz * dwdz;
     const double g2zy = dwdx * dudy + dwdy * dvdy + dwdz * dudy;
-    const double tr = (g2xx + g2yy + g2zz) / 3.0;
+    const double tr = div_by_recip(g2xx + g2yy + g2zz, dv.d3, dv.y3);
     const double sdxx = g2xx - tr, sdyy = g2yy - tr, sdzz = g2zz - tr;
     const double sdxy = 0.5 * (g2xy + g2yx);
     const double sdxz = 0.5 * (g2xz + g2zx);
@@ -323,7 +349,7 @@ int launch_wale(const wf_case& c, cudaStream_t s) {
   Geo g = geo_of(c.n);
   const long tot = (long)c.n * c.n * c.n;
   if (c.sgs) {
-    WF_CK(launch_k(k_wale, cells3(c.n, c.n, c.n), cell_block(), 0, s, c, g));
+    WF_CK(launch_k(k_wale, cells3(c.n, c.n, c.n), cell_block(), 0, s, c, g, divs_of(c)));
     WF_CKL("k_wale");
     FillReq r{c.fld[WF_VIS], FILL_VIS, c.rrey};
     return launch_fills(&r, 1, c.n, s);
@@ -351,7 +377,7 @@ __host__ __device__ __forceinline__ void op_dims(int comp, int n, int& ni, int& 
 
 template <int COMP>
 __global__ void __launch_bounds__(TPB) k_conv(const wf_case c, Geo g, double alpha,
-                                             const double* __restrict__ dtp) {
+                                             const double* __restrict__ dtp, const Divs dv) {
   pdl_entry();
   const double* u = c.fld[WF_U];
   const double* v = c.fld[WF_V];
@@ -378,17 +404,17 @@ __global__ void __launch_bounds__(TPB) k_conv(const wf_case c, Geo g, double alp
       a = I4(u, id + X, X); const double sp1 = a * a;
       a = I4(u, id, X); const double sn = a * a;
       a = I4(u, id - X, X); const double sm1 = a * a;
-      const double du2dx = (-sp2 + 27.0 * sp1 - 27.0 * sn + sm1) / (24.0 * dx);
+      const double du2dx = div_by_recip(-sp2 + 27.0 * sp1 - 27.0 * sn + sm1, dv.d24[0], dv.y24[0]);
       double p1 = I4(u, id + 2 * Y, Y) * I4(v, id + X + Y, X);
       double p0 = I4(u, id + Y, Y) * I4(v, id + X, X);
       double m1 = I4(u, id, Y) * I4(v, id + X - Y, X);
       double m2 = I4(u, id - Y, Y) * I4(v, id + X - 2 * Y, X);
-      const double duvdy = (-p1 + 27.0 * p0 - 27.0 * m1 + m2) / (24.0 * dy);
+      const double duvdy = div_by_recip(-p1 + 27.0 * p0 - 27.0 * m1 + m2, dv.d24[1], dv.y24[1]);
       p1 = I4(u, id + 2 * Z, Z) * I4(w, id + X + Z, X);
       p0 = I4(u, id + Z, Z) * I4(w, id + X, X);
       m1 = I4(u, id, Z) * I4(w, id + X - Z, X);
       m2 = I4(u, id - Z, Z) * I4(w, id + X - 2 * Z, X);
-      const double duwdz = (-p1 + 27.0 * p0 - 27.0 * m1 + m2) / (24.0 * dz);
+      const double duwdz = div_by_recip(-p1 + 27.0 * p0 - 27.0 * m1 + m2, dv.d24[2], dv.y24[2]);
       tot3 = du2dx + duvdy + duwdz;
     } else if (COMP == 1) {
       double a;
@@ -396,17 +422,17 @@ __global__ void __launch_bounds__(TPB) k_conv(const wf_case c, Geo g, double alp
       a = I4(v, id + Y, Y); const double sp1 = a * a;
       a = I4(v, id, Y); const double sn = a * a;
       a = I4(v, id - Y, Y); const double sm1 = a * a;
-      const double dv2dy = (-sp2 + 27.0 * sp1 - 27.0 * sn + sm1) / (24.0 * dy);
+      const double dv2dy = div_by_recip(-sp2 + 27.0 * sp1 - 27.0 * sn + sm1, dv.d24[1], dv.y24[1]);
       double p1 = I4(v, id + 2 * X, X) * I4(u, id + X + Y, Y);
       double p0 = I4(v, id + X, X) * I4(u, id + Y, Y);
       double m1 = I4(v, id, X) * I4(u, id - X + Y, Y);
       double m2 = I4(v, id - X, X) * I4(u, id - 2 * X + Y, Y);
-      const double duvdx = (-p1 + 27.0 * p0 - 27.0 * m1 + m2) / (24.0 * dx);
+      const double duvdx = div_by_recip(-p1 + 27.0 * p0 - 27.0 * m1 + m2, dv.d24[0], dv.y24[0]);
       p1 = I4(v, id + 2 * Z, Z) * I4(w, id + Y + Z, Y);
       p0 = I4(v, id + Z, Z) * I4(w, id + Y, Y);
       m1 = I4(v, id, Z) * I4(w, id + Y - Z, Y);
       m2 = I4(v, id - Z, Z) * I4(w, id + Y - 2 * Z, Y);
-      const double dvwdz = (-p1 + 27.0 * p0 - 27.0 * m1 + m2) / (24.0 * dz);
+      const double dvwdz = div_by_recip(-p1 + 27.0 * p0 - 27.0 * m1 + m2, dv.d24[2], dv.y24[2]);
       tot3 = duvdx + dv2dy + dvwdz;
     } else {
       double a;
@@ -414,32 +440,33 @@ __global__ void __launch_bounds__(TPB) k_conv(const wf_case c, Geo g, double alp
       a = I4(w, id + Z, Z); const double sp1 = a * a;
       a = I4(w, id, Z); const double sn = a * a;
       a = I4(w, id - Z, Z); const double sm1 = a * a;
-      const double dw2dz = (-sp2 + 27.0 * sp1 - 27.0 * sn + sm1) / (24.0 * dz);
+      const double dw2dz = div_by_recip(-sp2 + 27.0 * sp1 - 27.0 * sn + sm1, dv.d24[2], dv.y24[2]);
       double p1 = I4(w, id + 2 * X, X) * I4(u, id + X + Z, Z);
       double p0 = I4(w, id + X, X) * I4(u, id + Z, Z);
       double m1 = I4(w, id, X) * I4(u, id - X + Z, Z);
       double m2 = I4(w, id - X, X) * I4(u, id - 2 * X + Z, Z);
-      const double duwdx = (-p1 + 27.0 * p0 - 27.0 * m1 + m2) / (24.0 * dx);
+      const double duwdx = div_by_recip(-p1 + 27.0 * p0 - 27.0 * m1 + m2, dv.d24[0], dv.y24[0]);
       p1 = I4(w, id + 2 * Y, Y) * I4(v, id + Y + Z, Z);
       p0 = I4(w, id + Y, Y) * I4(v, id + Z, Z);
       m1 = I4(w, id, Y) * I4(v, id - Y + Z, Z);
       m2 = I4(w, id - Y, Y) * I4(v, id - 2 * Y + Z, Z);
-      const double dvwdy = (-p1 + 27.0 * p0 - 27.0 * m1 + m2) / (24.0 * dy);
+      const double dvwdy = div_by_recip(-p1 + 27.0 * p0 - 27.0 * m1 + m2, dv.d24[1], dv.y24[1]);
       tot3 = duwdx + dvwdy + dw2dz;
     }
     star[id] = LD(oo, id) - dt * alpha * tot3;
   }
 }
 
-__device__ __forceinline__ double lap1(const double* f, long id, long s, double d) {
-  return (-LD(f, id + 2 * s) + 16.0 * LD(f, id + s) - 30.0 * LD(f, id) +
-          16.0 * LD(f, id - s) - LD(f, id - 2 * s)) /
-         (12.0 * d * d);
+__device__ __forceinline__ double lap1(const double* f, long id, long s, double d,
+                                       double y) {
+  return div_by_recip(-LD(f, id + 2 * s) + 16.0 * LD(f, id + s) - 30.0 * LD(f, id) +
+                          16.0 * LD(f, id - s) - LD(f, id - 2 * s),
+                      d, y);
 }
 
 template <int COMP>
 __global__ void __launch_bounds__(TPB) k_diff(const wf_case c, Geo g, double alpha,
-                                             const double* __restrict__ dtp) {
+                                             const double* __restrict__ dtp, const Divs dv) {
   pdl_entry();
   const double* f = c.fld[WF_U + COMP];
   const double* vis = c.fld[WF_VIS];
@@ -456,7 +483,8 @@ __global__ void __launch_bounds__(TPB) k_diff(const wf_case c, Geo g, double alp
     const int j = NPL + jy_;
     const int i = NPL + (int)blockIdx.z;
     const long id = g.at(i, j, k);
-    const double l4 = lap1(f, id, g.sI, c.dx) + lap1(f, id, g.sJ, c.dy) + lap1(f, id, 1, c.dz);
+    const double l4 = lap1(f, id, g.sI, dv.d12[0], dv.y12[0]) +
+                      lap1(f, id, g.sJ, dv.d12[1], dv.y12[1]) + lap1(f, id, 1, dv.d12[2], dv.y12[2]);
     const double diff = LD(vis, id + vofs) * l4;
     star[id] = star[id] + dt * alpha * diff;
   }
@@ -470,9 +498,9 @@ int launch_conv(const wf_case& c, int comp, double alpha, const double* dt,
   int ni, nj, nk;
   op_dims(comp, c.n, ni, nj, nk);
   const dim3 gr = cells3(ni, nj, nk), bl = cell_block();
-  if (comp == 0) WF_CK(launch_k(k_conv<0>, gr, bl, 0, s, c, g, alpha, dt));
-  else if (comp == 1) WF_CK(launch_k(k_conv<1>, gr, bl, 0, s, c, g, alpha, dt));
-  else if (comp == 2) WF_CK(launch_k(k_conv<2>, gr, bl, 0, s, c, g, alpha, dt));
+  if (comp == 0) WF_CK(launch_k(k_conv<0>, gr, bl, 0, s, c, g, alpha, dt, divs_of(c)));
+  else if (comp == 1) WF_CK(launch_k(k_conv<1>, gr, bl, 0, s, c, g, alpha, dt, divs_of(c)));
+  else if (comp == 2) WF_CK(launch_k(k_conv<2>, gr, bl, 0, s, c, g, alpha, dt, divs_of(c)));
   else return fail(WF_EINVAL, "conv: comp must be 0, 1 or 2");
   WF_CKL("k_conv");
   return WF_OK;
@@ -486,9 +514,9 @@ int launch_diff(const wf_case& c, int comp, double alpha, const double* dt,
   int ni, nj, nk;
   op_dims(comp, c.n, ni, nj, nk);
   const dim3 gr = cells3(ni, nj, nk), bl = cell_block();
-  if (comp == 0) WF_CK(launch_k(k_diff<0>, gr, bl, 0, s, c, g, alpha, dt));
-  else if (comp == 1) WF_CK(launch_k(k_diff<1>, gr, bl, 0, s, c, g, alpha, dt));
-  else if (comp == 2) WF_CK(launch_k(k_diff<2>, gr, bl, 0, s, c, g, alpha, dt));
+  if (comp == 0) WF_CK(launch_k(k_diff<0>, gr, bl, 0, s, c, g, alpha, dt, divs_of(c)));
+  else if (comp == 1) WF_CK(launch_k(k_diff<1>, gr, bl, 0, s, c, g, alpha, dt, divs_of(c)));
+  else if (comp == 2) WF_CK(launch_k(k_diff<2>, gr, bl, 0, s, c, g, alpha, dt, divs_of(c)));
   else return fail(WF_EINVAL, "diff: comp must be 0, 1 or 2");
   WF_CKL("k_diff");
   return WF_OK;
@@ -498,7 +526,7 @@ int launch_diff(const wf_case& c, int comp, double alpha, const double* dt,
 // calvel (kernels.py:232-264): the three components in one launch
 // --------------------------------------------------------------------------
 __global__ void __launch_bounds__(TPB) k_calvel(const wf_case c, Geo g, double alpha,
-                                               const double* __restrict__ dtp) {
+                                               const double* __restrict__ dtp, const Divs dv) {
   pdl_entry();
   const double* p = c.fld[WF_P];
   const double dt = *dtp;
@@ -512,17 +540,20 @@ __global__ void __launch_bounds__(TPB) k_calvel(const wf_case c, Geo g, double a
     const long id = g.at(i, j, k);
     const double p0 = LD(p, id);
     if (i < hi)
-      c.fld[WF_U][id] = LD(c.fld[WF_USTAR], id) - dt * alpha * (LD(p, id + g.sI) - p0) / c.dx;
+      c.fld[WF_U][id] = LD(c.fld[WF_USTAR], id) -
+                        div_by_recip(dt * alpha * (LD(p, id + g.sI) - p0), dv.dh[0], dv.yh[0]);
     if (j < hi)
-      c.fld[WF_V][id] = LD(c.fld[WF_VSTAR], id) - dt * alpha * (LD(p, id + g.sJ) - p0) / c.dy;
+      c.fld[WF_V][id] = LD(c.fld[WF_VSTAR], id) -
+                        div_by_recip(dt * alpha * (LD(p, id + g.sJ) - p0), dv.dh[1], dv.yh[1]);
     if (k < hi)
-      c.fld[WF_W][id] = LD(c.fld[WF_WSTAR], id) - dt * alpha * (LD(p, id + 1) - p0) / c.dz;
+      c.fld[WF_W][id] = LD(c.fld[WF_WSTAR], id) -
+                        div_by_recip(dt * alpha * (LD(p, id + 1) - p0), dv.dh[2], dv.yh[2]);
   }
 }
 
 int launch_calvel(const wf_case& c, double alpha, const double* dt, cudaStream_t s) {
   Geo g = geo_of(c.n);
-  WF_CK(launch_k(k_calvel, cells3(c.n, c.n, c.n), cell_block(), 0, s, c, g, alpha, dt));
+  WF_CK(launch_k(k_calvel, cells3(c.n, c.n, c.n), cell_block(), 0, s, c, g, alpha, dt, divs_of(c)));
   WF_CKL("k_calvel");
   return WF_OK;
 }
@@ -533,7 +564,7 @@ int launch_calvel(const wf_case& c, double alpha, const double* dt, cudaStream_t
 // --------------------------------------------------------------------------
 __global__ void __launch_bounds__(TPB) k_calmas(const wf_case c, Geo g,
                                                unsigned long long h_if,
-                                               unsigned long long h_loop) {
+                                               unsigned long long h_loop, const Divs dv) {
   pdl_entry();
   __shared__ double sm[32];
   const double* u = c.fld[WF_U];
@@ -542,6 +573,7 @@ __global__ void __launch_bounds__(TPB) k_calmas(const wf_case c, Geo g,
   double* su = c.fld[WF_SU];
   wf_scalars* sc = c.sc;
   const double dt = sc->dt;
+  const double rdt = 1.0 / dt;   // fact / dt below as div_by_recip(fact, dt, rdt)
   const double dx = c.dx, dy = c.dy, dz = c.dz;
   double mloc = 0.0;
   const int k = NPL + blockIdx.x * 32 + (threadIdx.x & 31);
@@ -550,14 +582,14 @@ __global__ void __launch_bounds__(TPB) k_calmas(const wf_case c, Geo g,
   for (int i = NPL + blockIdx.z; in && i < NPL + g.n; i += gridDim.z) {
     const long id = g.at(i, j, k);
     const long X = g.sI, Y = g.sJ;
-    const double dudx = (-LD(u, id + X) + 27.0 * LD(u, id) - 27.0 * LD(u, id - X) +
-                         LD(u, id - 2 * X)) / (24.0 * dx);
-    const double dvdy = (-LD(v, id + Y) + 27.0 * LD(v, id) - 27.0 * LD(v, id - Y) +
-                         LD(v, id - 2 * Y)) / (24.0 * dy);
-    const double dwdz = (-LD(w, id + 1) + 27.0 * LD(w, id) - 27.0 * LD(w, id - 1) +
-                         LD(w, id - 2)) / (24.0 * dz);
+    const double dudx = div_by_recip(-LD(u, id + X) + 27.0 * LD(u, id) - 27.0 * LD(u, id - X) +
+                                         LD(u, id - 2 * X), dv.d24[0], dv.y24[0]);
+    const double dvdy = div_by_recip(-LD(v, id + Y) + 27.0 * LD(v, id) - 27.0 * LD(v, id - Y) +
+                                         LD(v, id - 2 * Y), dv.d24[1], dv.y24[1]);
+    const double dwdz = div_by_recip(-LD(w, id + 1) + 27.0 * LD(w, id) - 27.0 * LD(w, id - 1) +
+                                         LD(w, id - 2), dv.d24[2], dv.y24[2]);
     const double fact = dudx + dvdy + dwdz;
-    su[id] = fact / dt;
+    su[id] = div_by_recip(fact, dt, rdt);
     mloc = fmax(mloc, fabs(fact * dx * dy * dz));
   }
   mloc = block_max(mloc, sm);
@@ -584,7 +616,7 @@ __global__ void __launch_bounds__(TPB) k_calmas(const wf_case c, Geo g,
 int launch_calmas(const wf_case& c, unsigned long long h_if, unsigned long long h_loop,
                   cudaStream_t s) {
   Geo g = geo_of(c.n);
-  WF_CK(launch_k(k_calmas, reduce_grid(c.n), TPB, 0, s, c, g, h_if, h_loop));
+  WF_CK(launch_k(k_calmas, reduce_grid(c.n), TPB, 0, s, c, g, h_if, h_loop, divs_of(c)));
   WF_CKL("k_calmas");
   return WF_OK;
 }
