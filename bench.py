@@ -148,81 +148,94 @@ def load_peaks():
 # DRAM bytes per launch of the dominant kernels, from the ncu captures
 # summarised under profiles/ (dram__bytes_read.sum + dram__bytes_write.sum)
 NCU_TRAFFIC = {("k_rbgs_split", 256): (189163264, "profiles/rbgs_split_256_full.md"),
-               ("cop", 20): (518313472, "profiles/cop_20_full.md"),
+               ("k_rbgs_split", 80): (5156864, "profiles/rbgs_split_80_full.md"),
+               ("cop", 20): (133432832, "profiles/cop_20_full.md"),
                ("coarse", 20): (172032, "profiles/coarse_p2p_20_full.md")}
 
 
 def kernel_roofline(sol, args, peak, peak_kind):
-    """The dominant kernel of the step, timed live with CUDA events on the
-    launching stream after the timed region.  Levels >= 128 (FP64): the
-    split half-sweep of level 0 -- relax(6) and relax(12) differ by exactly
-    12 half-sweep launches, so their difference isolates the kernel; its
-    algorithmic bytes are 1.5 words per cell (read the other colour, read the
-    own colour's rhs, write the own colour).  Smaller cases: the coarse-level
-    relax (300 sweeps in one launch, the largest share of the step), whose
-    global traffic is reading phi and rhs and writing phi once."""
-    import numpy as np
+    """The dominant kernel of the step (largest share of the step's launch
+    list), timed live with CUDA events on the launching stream after the
+    timed region.  Level 0 of 80^3 and larger (FP64): the split half-sweep
+    -- relax(6) and relax(12) differ by exactly 12 half-sweep launches, so
+    their difference isolates the kernel; its algorithmic bytes are 1.5 words
+    per cell (read the other colour, read the own colour's rhs, write the own
+    colour).  Smaller cases: the coarse-level relax.  Where the coarse level
+    runs through its operator and is not the dominant kernel, it is reported
+    beside it as ``roofline_coarse``."""
     import torch
     if args.precision != "fp64":
         return {"bound": "hbm", "kernel": None, "achieved": None, "peak": peak,
                 "unit": "GB/s", "frac": None, "traffic": None,
                 "note": "mixed precision relaxes FP32 levels outside the FP64 harness; "
-                        "see roofline_step"}
+                        "see roofline_step"}, None
     mg = sol.mg
-
-    def timed(l, sweeps, reps):
-        mg._relax(l, sweeps)
-        torch.cuda.synchronize()
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record()
-        for _ in range(reps):
-            mg._relax(l, sweeps)
-        b.record()
-        torch.cuda.synchronize()
-        return a.elapsed_time(b) / reps / 1e3   # s per relax
-
     n = args.n
-    lev0 = mg.levels[0]
-    lev0.rhs.assign(np.random.default_rng(7).standard_normal(lev0.shape))
-    if n >= 128:
-        t = (timed(0, 12, 5) - timed(0, 6, 5)) / 12
-        alg = 1.5 * n ** 3 * 8
-        name = "k_rbgs_split (level-0 half-sweep, FP64)"
-        key = ("k_rbgs_split", n)
-    else:
-        lc = args.levels - 1
-        nc = n >> lc
-        lv = mg.levels[lc]
-        lv.rhs.assign(np.random.default_rng(8).standard_normal(lv.shape))
-        if mg._cop_part is not None:
-            # the coarse solve as the precomputed operator: read N^2 operator
-            # words (the partial sums, 2 x 64 x N words, are 1.6 % of it)
-            mg._coarse_solve()
-            torch.cuda.synchronize()
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record()
-            for _ in range(10):
-                mg._coarse_solve()
-            b.record()
-            torch.cuda.synchronize()
-            t = a.elapsed_time(b) / 10 / 1e3
-            N = nc ** 3
-            alg = N * N * 8 + 2 * 64 * N * 8
-            name = "coarse %d^3 operator product (k_cop_partial + k_cop_finish)" % nc
-            key = ("cop", nc)
-        else:
-            t = timed(lc, 300, 5)
-            alg = 3 * (nc + 2) ** 3 * 8
-            name = "coarse relax %d^3, 300 sweeps in one launch (latency-bound)" % nc
-            key = ("coarse", nc)
+    if n >= 80:
+        main = _split_roofline(mg, n, peak, peak_kind)
+        extra = _coarse_roofline(mg, args, peak, peak_kind) if mg._cop_part is not None \
+            else None
+        return main, extra
+    return _coarse_roofline(mg, args, peak, peak_kind), None
+
+
+def _timed_relax(mg, l, sweeps, reps):
+    import torch
+    mg._relax(l, sweeps)
+    torch.cuda.synchronize()
+    a, b = _events()
+    a.record()
+    for _ in range(reps):
+        mg._relax(l, sweeps)
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps / 1e3   # s per relax
+
+
+def _roof(name, key, alg, t, peak, peak_kind):
     traffic, src = NCU_TRAFFIC.get(key, (None, None))
     ach = alg / t / 1e9
     return {"bound": "hbm", "kernel": name, "achieved": round(ach, 2), "peak": peak,
             "peak_kind": peak_kind, "unit": "GB/s", "frac": round(ach / peak, 5),
             "traffic": traffic, "traffic_source": src, "alg_bytes_per_launch": round(alg),
             "us_per_launch": round(t * 1e6, 2)}
+
+
+def _split_roofline(mg, n, peak, peak_kind):
+    import numpy as np
+    lev0 = mg.levels[0]
+    lev0.rhs.assign(np.random.default_rng(7).standard_normal(lev0.shape))
+    t = (_timed_relax(mg, 0, 12, 5) - _timed_relax(mg, 0, 6, 5)) / 12
+    return _roof("k_rbgs_split (level-0 half-sweep, FP64)", ("k_rbgs_split", n),
+                 1.5 * n ** 3 * 8, t, peak, peak_kind)
+
+
+def _coarse_roofline(mg, args, peak, peak_kind):
+    import numpy as np
+    import torch
+    lc = args.levels - 1
+    nc = args.n >> lc
+    lv = mg.levels[lc]
+    lv.rhs.assign(np.random.default_rng(8).standard_normal(lv.shape))
+    if mg._cop_part is None:
+        t = _timed_relax(mg, lc, 300, 5)
+        return _roof("coarse relax %d^3, 300 sweeps in one launch (latency-bound)" % nc,
+                     ("coarse", nc), 3 * (nc + 2) ** 3 * 8, t, peak, peak_kind)
+    # the coarse solve through the precomputed operator: read (N/2)^2
+    # operator words (the partial sums, 2 x nch x N/2 words with nch <= 64,
+    # are at most 3 % of it; the two closing half-sweeps 3 x N words)
+    mg._coarse_solve()
+    torch.cuda.synchronize()
+    a, b = _events()
+    a.record()
+    for _ in range(10):
+        mg._coarse_solve()
+    b.record()
+    torch.cuda.synchronize()
+    t = a.elapsed_time(b) / 10 / 1e3
+    N = nc ** 3
+    return _roof("coarse %d^3 relax via the operator (k_cop_partial + k_cop_finish "
+                 "+ 2 k_rbgs)" % nc, ("cop", nc), (N // 2) ** 2 * 8, t, peak, peak_kind)
 
 
 # ---------------------------------------------------------------------------
@@ -304,6 +317,7 @@ def bench_serve(args):
     reqs = poisson_stream(count=args.requests, rate=20.0, seed=0,
                           step_scale=args.step_scale)
     srv = CavityServer(budget_bytes=150 * 10 ** 9, nstreams=args.streams or 16)
+    srv.warmup(reqs)
     srv.run(reqs)
     s = srv.summary()
     print(json.dumps({
@@ -314,7 +328,9 @@ def bench_serve(args):
         "peak_resident_GB": round(s["peak_resident_bytes"] / 1e9, 3),
         "config": {"requests": args.requests, "rate_per_s": 20.0, "seed": 0,
                    "step_scale": args.step_scale, "budget_GB": 150, "streams": args.streams or 16,
-                   "latency": "arrival to end of last step, wall clock"}}), flush=True)
+                   "latency": "arrival to end of last step, wall clock",
+                   "startup": "one case per size built and stepped before the stream starts"}}),
+          flush=True)
 
 
 def bench_poisson(args):
@@ -506,7 +522,7 @@ def main():
                      "alg_bytes_per_step": round(bytes_tot / K),
                      "note": "algorithmic bytes of the reference passes (measured iters per "
                              "step) / device step time; frac of the measured copy peak"}
-    roofline = kernel_roofline(sol, args, peak, peak_kind)
+    roofline, roofline_coarse = kernel_roofline(sol, args, peak, peak_kind)
 
     # ---- end to end through the public API with host buffers ---------------
     e2e = None
@@ -567,6 +583,7 @@ def main():
                 "wall_s": round(wall, 3), "gpu_launches": int(launches),
                 "launches_per_step": round(launches / K, 1),
                 "clocks": clocks, "roofline": roofline, "roofline_step": roofline_step,
+                "roofline_coarse": roofline_coarse,
                 "cpu_baseline": cpu, "e2e": e2e}
         print(json.dumps(line), flush=True)
     sol.close()

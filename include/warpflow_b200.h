@@ -129,11 +129,16 @@ WF_API int wf_mg_level_elems(int32_t n, int32_t nlev, int32_t level, int64_t* el
  * (multigrid.py:301-322: n_coarse RBGS sweeps starting from phi = 0) is a
  * fixed linear map of the level's rhs.  wf_mg_build_coarse_op stores it, for
  * the case's n, nlev, spacing, n_coarse and precision (c->mg_fp32 selects
- * FP32), as a dense operator in c->mg_cop: row j = the relaxed field for
- * rhs = unit vector j.  With c->mg_cop set, V-cycles apply it as one
- * matrix-vector product (HBM-bound) instead of the latency-bound sweeps;
- * the results agree to rounding.  Coarsest edges 4, 8, 12, 16, 20, 24 only
- * (WF_EUNSUPPORTED otherwise).  The operator is read-only once built and can
+ * FP32), in c->mg_cop: every cell neighbours only cells of the other
+ * parity of i+j+k, so after the first sweep from zero the even-parity half
+ * of phi evolves on its own, and the dense map from that half after sweep 1
+ * to it after n_coarse - 1 sweeps ((n_c^3/2)^2 elements) is stored; row u =
+ * the even-parity half of phi after n_coarse - 1 sweeps from zero with
+ * rhs = unit vector at the u-th even-parity cell.  With c->mg_cop set,
+ * V-cycles run the relax as the first sweep's even-parity numerators, one
+ * matrix-vector product (HBM-bound) and the last sweep, instead of the
+ * latency-bound sweeps; the results agree to rounding.  Coarsest edges 4, 8,
+ * 12, 16, 20, 24 and n_coarse >= 2 only (WF_EUNSUPPORTED / WF_EINVAL).  The operator is read-only once built and can
  * be shared by cases of the same size; each case needs its own partial-sum
  * scratch (c->mg_cop_part).  wf_mg_coarse_op_elems gives both element counts. */
 WF_API int wf_mg_coarse_op_elems(int32_t n, int32_t nlev, int64_t* op_elems,

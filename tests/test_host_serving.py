@@ -73,7 +73,7 @@ def test_case_bytes_formula():
     vol = 82 ** 3 + 42 ** 3 + 22 ** 3
     mg64 = 2 * 8 * vol + 2 * 8 * vol      # phi, rhs + two-array scratch
     mg32 = 2 * 4 * vol + 2 * 4 * vol
-    cop64, cop32 = 64 * 20 ** 3 * 8, 64 * 20 ** 3 * 4   # coarse-operator scratch
+    cop64, cop32 = 32 * 20 ** 3 * 8, 32 * 20 ** 3 * 4   # coarse-operator scratch
     assert 0 <= case_bytes(n, 3, "fp64") - f - mg64 - cop64 < 4096
     assert 0 <= case_bytes(n, 3, "mixed") - f - 2 * 8 * vol - mg32 - cop32 < 4096
     # a coarsest edge without an operator (18) adds no scratch

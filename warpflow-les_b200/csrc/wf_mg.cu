@@ -326,9 +326,10 @@ struct CoarseShape {
   static constexpr int THREADS = 2 * (((NC * (NC / 2)) + 31) / 32) * 32;
 };
 
-// With unit_out set, CTA b relaxes rhs = unit vector b from phi = 0 and
-// writes the result as row b of unit_out (cells in (i, j, k) order): the
-// rows of the coarse-level operator.
+// With unit_out set, CTA b relaxes rhs = e_u from phi = 0, u the b-th cell
+// of even i+j+k in (i, j, k) order (cell index 2b or 2b+1), and writes the
+// even-parity cells of the result as row b of unit_out (position = cell
+// index / 2): the rows of the coarse-level operator.
 template <class T, int NC, bool RHS_SMEM>
 __global__ void __launch_bounds__(CoarseShape<NC>::THREADS) k_coarse_cols(Lvl<T> L,
                                                                            int nsweeps,
@@ -365,12 +366,15 @@ __global__ void __launch_bounds__(CoarseShape<NC>::THREADS) k_coarse_cols(Lvl<T>
   T ph[NC];
   T rh[RHS_SMEM ? 1 : NC];
   const long c0 = lid(L, i + 1, j + 1, 1);
+  // the unit cell of this CTA: the one of cells 2b, 2b+1 with even i+j+k
+  const int unit = 2 * (int)blockIdx.x + (((2 * (int)blockIdx.x / NC) / NC +
+                                           (2 * (int)blockIdx.x / NC) % NC) & 1);
 #pragma unroll
   for (int k = 0; k < NC; ++k) {
     T r;
     if (unit_out) {
       ph[k] = T(0);
-      r = (active && (i * NC + j) * NC + k == (int)blockIdx.x) ? T(1) : T(0);
+      r = (active && (i * NC + j) * NC + k == unit) ? T(1) : T(0);
     } else {
       ph[k] = active ? L.phi[c0 + k] : T(0);
       r = active ? L.rhs[c0 + k] : T(0);
@@ -401,9 +405,10 @@ __global__ void __launch_bounds__(CoarseShape<NC>::THREADS) k_coarse_cols(Lvl<T>
   }
   if (!active) return;
   if (unit_out) {
-    T* row = unit_out + (long)blockIdx.x * (NC * NC * NC) + (i * NC + j) * NC;
+    T* row = unit_out + (long)blockIdx.x * (NC * NC * NC / 2) + ((i * NC + j) * NC >> 1);
 #pragma unroll
-    for (int k = 0; k < NC; ++k) row[k] = ph[k];
+    for (int k = 0; k < NC; ++k)
+      if (((i + j + k) & 1) == 0) row[k >> 1] = ph[k];
     return;
   }
 #pragma unroll
@@ -421,7 +426,7 @@ static int launch_coarse(const Lvl<T>& L, int nsweeps, cudaStream_t s, T* unit_o
   const size_t sb = (size_t)NC * NC * NC * sizeof(T) * (RHS_SMEM ? 2 : 1);
   WF_CK(cudaFuncSetAttribute(k_coarse_cols<T, NC, RHS_SMEM>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb));
-  const int nb = unit_out ? NC * NC * NC : 1;
+  const int nb = unit_out ? NC * NC * NC / 2 : 1;
   WF_CK(launch_k(k_coarse_cols<T, NC, RHS_SMEM>, nb, 2 * GROUP, sb, s, L, nsweeps, unit_out));
   WF_CKL("k_coarse_cols");
   return WF_OK;
@@ -1097,14 +1102,24 @@ static int try_coarse_tb(const Lvl<T>& L, int nsweeps, cudaStream_t s, int* rc) 
 }
 
 // ---- the coarse-level relax as a precomputed operator ----------------------
-// n_coarse sweeps from phi = 0 are linear in rhs: phi = sum_j rhs_j * row_j,
-// row_j = the relaxed field for rhs = e_j (built by k_coarse_cols in unit
-// mode).  Applying it reads the operator once (N^2 elements, N = n^3), an
-// HBM-bound product instead of 2*n_coarse dependent half-sweeps.  The sum is
-// split over COP_CH row chunks with partial sums in fixed order (chunk
-// partials, then chunks in ascending order), so results do not depend on
-// scheduling: a case computes the same bits alone or beside other cases.
+// Colour A = cells of odd i+j+k (each sweep updates them first), colour B =
+// even i+j+k; every neighbour of a cell has the other colour.  From phi = 0
+// the first sweep gives x_A = b_A / ap and then x_B = v_B / ap with
+// v_B = b_B - sum_nb a_nb x_A(nb); every later sweep maps x_B linearly
+// (x_B <- x_B1 + G x_B).  So after m = n_coarse - 1 sweeps x_B = S v_B with
+// S fixed by the level (row u of S = the B part of m sweeps from zero with
+// rhs = e_u, built by k_coarse_cols in unit mode), and the n_coarse-th sweep
+// is run as such from that x_B.  Applying the relax therefore reads S once
+// ((N/2)^2 elements, N = n^3, a quarter of the full map's) in an HBM-bound
+// product instead of 2*n_coarse dependent half-sweeps.  The sum is split over
+// row chunks with partial sums in fixed order (chunk partials, then the
+// chunks in a fixed tree), so results do not depend on scheduling: a case
+// computes the same bits alone or beside other cases.  The chunk count is a
+// function of the size only (cop_chunks), at most COP_CH.
 constexpr int COP_CH = 64;
+// CTAs of k_cop_partial resident at once on a B200 (148 SMs x 3 CTAs of 256
+// threads at its register count): the chunk count fills one wave
+constexpr int COP_SLOTS = 148 * 3;
 
 static bool cop_size_ok(int nc) {
   return nc == 4 || nc == 8 || nc == 12 || nc == 16 || nc == 20 || nc == 24;
@@ -1114,30 +1129,68 @@ template <class T> struct Vec2;
 template <> struct Vec2<double> { using type = double2; };
 template <> struct Vec2<float> { using type = float2; };
 
-// grid (ceil(N/512), COP_CH): a thread owns outputs i, i+1 (one 2-vector
-// load per operator row) and runs 8 rows at a time, each row with its own
-// pair of accumulators, so 8 vector loads are in flight per thread
+// (i, j, k) of the B cell at position b of the B-only order (n even: cells
+// 2b and 2b+1 share i and j, and exactly one of them has even i+j+k)
+__device__ __forceinline__ void b_cell(int b, int n, int& i, int& j, int& k) {
+  const int rw = 2 * b / n;
+  i = rw / n;
+  j = rw - i * n;
+  k = 2 * b - rw * n + ((i + j) & 1);
+}
+
+// v_B of B cell (i,j,k): its rhs minus its neighbours' first-sweep values
+// b/ap (every neighbour is an A cell, updated from phi = 0); the terms in
+// the order of k_rbgs, absent faces with zero coefficients
+template <class T>
+__device__ __forceinline__ T first_sweep_v(const Lvl<T>& L, int i, int j, int k) {
+  const int n = L.n;
+  auto x1 = [&](int a, int bq, int cq) -> T {
+    const T aw = a > 0 ? L.ax : T(0), ae = a < n - 1 ? L.ax : T(0);
+    const T as = bq > 0 ? L.ay : T(0), an = bq < n - 1 ? L.ay : T(0);
+    const T ab = cq > 0 ? L.az : T(0), at = cq < n - 1 ? L.az : T(0);
+    return L.rhs[lid(L, a + 1, bq + 1, cq + 1)] / (-(aw + ae + as + an + ab + at));
+  };
+  const T W = i > 0 ? L.ax * x1(i - 1, j, k) : T(0);
+  const T E = i < n - 1 ? L.ax * x1(i + 1, j, k) : T(0);
+  const T S = j > 0 ? L.ay * x1(i, j - 1, k) : T(0);
+  const T N = j < n - 1 ? L.ay * x1(i, j + 1, k) : T(0);
+  const T B = k > 0 ? L.az * x1(i, j, k - 1) : T(0);
+  const T U = k < n - 1 ? L.az * x1(i, j, k + 1) : T(0);
+  return L.rhs[lid(L, i + 1, j + 1, k + 1)] - (W + E + S + N + B + U);
+}
+
+// chunks of the operator rows for M = N/2 outputs: as many as fill one wave
+// of k_cop_partial, at least enough that a chunk fits its 256-entry v_B
+// buffer, at most COP_CH
+static int cop_chunks(int M) {
+  const int gx = (M + 511) / 512;
+  return std::min(COP_CH, std::max((M + 255) / 256, COP_SLOTS / gx));
+}
+
+// grid (ceil(M/512), nch), M = N/2: a CTA forms v_B of its row chunk in
+// shared memory, then a thread owns outputs o, o+1 (one 2-vector load per
+// operator row) and runs 8 rows at a time, each row with its own pair of
+// accumulators, so 8 vector loads are in flight per thread
 template <class T>
 __global__ void __launch_bounds__(256) k_cop_partial(const T* __restrict__ op, const Lvl<T> L,
                                                      T* __restrict__ part) {
   pdl_entry();
   using V = typename Vec2<T>::type;
   constexpr int U = 8;
-  __shared__ T rs[512];
-  const int n = L.n, N = n * n * n;
-  const int jc = (N + COP_CH - 1) / COP_CH;
-  const int j0 = blockIdx.y * jc, j1 = min(N, j0 + jc);
+  __shared__ T rs[256];
+  const int n = L.n, M = n * n * n / 2;
+  const int jc = (M + gridDim.y - 1) / gridDim.y;
+  const int j0 = blockIdx.y * jc, j1 = min(M, j0 + jc);
   for (int t = threadIdx.x; t < j1 - j0; t += 256) {
-    const int jj = j0 + t;
-    const int a = jj / (n * n), rem = jj - a * n * n;
-    const int b = rem / n, cc = rem - b * n;
-    rs[t] = L.rhs[lid(L, a + 1, b + 1, cc + 1)];
+    int a, bq, cq;
+    b_cell(j0 + t, n, a, bq, cq);
+    rs[t] = first_sweep_v(L, a, bq, cq);
   }
   __syncthreads();
-  const int i = 2 * (blockIdx.x * 256 + threadIdx.x);
-  if (i >= N) return;   // N is even: i+1 < N as well
-  const V* col = reinterpret_cast<const V*>(op + (long)j0 * N + i);
-  const long rowv = N / 2;   // one operator row in 2-vectors
+  const int o = 2 * (blockIdx.x * 256 + threadIdx.x);
+  if (o >= M) return;   // M is even: o+1 < M as well
+  const V* col = reinterpret_cast<const V*>(op + (long)j0 * M + o);
+  const long rowv = M / 2;   // one operator row in 2-vectors
   T ax[U], ay[U];
 #pragma unroll
   for (int u = 0; u < U; ++u) ax[u] = ay[u] = T(0);
@@ -1164,40 +1217,61 @@ __global__ void __launch_bounds__(256) k_cop_partial(const T* __restrict__ op, c
     sx += ax[u];
     sy += ay[u];
   }
-  part[(long)blockIdx.y * N + i] = sx;
-  part[(long)blockIdx.y * N + i + 1] = sy;
+  part[(long)blockIdx.y * M + o] = sx;
+  part[(long)blockIdx.y * M + o + 1] = sy;
 }
 
+// x_B = the sum of the nch chunk partials: warp w of the CTA sums chunks
+// w, w+8, ... in ascending order for 32 outputs, then the 8 warp sums are
+// added in ascending order.  The A cell beside each B cell is zeroed (the
+// closing sweep overwrites it before reading it).
 template <class T>
-__global__ void __launch_bounds__(256) k_cop_finish(const T* __restrict__ part, Lvl<T> L) {
+__global__ void __launch_bounds__(256) k_cop_finish(const T* __restrict__ part, Lvl<T> L,
+                                                    int nch) {
   pdl_entry();
-  const int n = L.n, N = n * n * n;
-  const int t = blockIdx.x * 256 + threadIdx.x;
-  if (t >= N) return;
-  T x = part[t];
-#pragma unroll 4
-  for (int ch = 1; ch < COP_CH; ++ch) x += part[(long)ch * N + t];
-  const int i = t / (n * n), rem = t - i * n * n;
-  const int j = rem / n, k = rem - j * n;
-  const long c = lid(L, i + 1, j + 1, k + 1);
-  L.phi[c] = x;
-  ring_mirror(L, i, j, k, c, x);
+  __shared__ T ws[8][32];
+  const int n = L.n, M = n * n * n / 2;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int t = blockIdx.x * 32 + lane;
+  T x = T(0);
+  if (t < M)
+    for (int ch = w; ch < nch; ch += 8) x += part[(long)ch * M + t];
+  ws[w][lane] = x;
+  __syncthreads();
+  if (w != 0 || t >= M) return;
+  x = ws[0][lane];
+#pragma unroll
+  for (int q = 1; q < 8; ++q) x += ws[q][lane];
+  int i, j, k;
+  b_cell(t, n, i, j, k);
+  L.phi[lid(L, i + 1, j + 1, k + 1)] = x;
+  L.phi[lid(L, i + 1, j + 1, (k ^ 1) + 1)] = T(0);
 }
 
-// phi of the coarsest level = operator x rhs (the level's phi is overwritten);
-// part: this case's COP_CH x N scratch
+// phi of the coarsest level = the n_coarse-sweep relax of rhs from zero (the
+// level's phi is overwritten): the operator product for the B cells after
+// n_coarse - 1 sweeps, then the last sweep (k_rbgs, colour A then B, which
+// also writes the face-ring mirrors); part: this case's COP_CH x N/2 scratch
 template <class T>
 static int apply_coarse_op(const Lvl<T>& L, const T* op, T* part, cudaStream_t s) {
-  const int N = L.n * L.n * L.n;
-  WF_CK(launch_k(k_cop_partial<T>, dim3((N + 511) / 512, COP_CH), 256, 0, s, op, L, part));
+  const int M = L.n * L.n * L.n / 2;
+  const int nch = cop_chunks(M);
+  WF_CK(launch_k(k_cop_partial<T>, dim3((M + 511) / 512, nch), 256, 0, s, op, L, part));
   WF_CKL("k_cop_partial");
-  WF_CK(launch_k(k_cop_finish<T>, (N + 255) / 256, 256, 0, s, (const T*)part, L));
+  WF_CK(launch_k(k_cop_finish<T>, (M + 31) / 32, 256, 0, s, (const T*)part, L, nch));
   WF_CKL("k_cop_finish");
+  for (int color = 0; color < 2; ++color) {
+    WF_CK(launch_k(k_rbgs<T>, cells3(L.n, L.n, (L.n + 1) / 2), cell_block(), 0, s, L, color));
+    WF_CKL("k_rbgs");
+  }
   return WF_OK;
 }
 
+// the operator rows: n_coarse - 1 sweeps from zero per unit B cell
 template <class T>
-static int build_coarse_op(const Lvl<T>& L, int nsweeps, T* op, cudaStream_t s) {
+static int build_coarse_op(const Lvl<T>& L, int n_coarse, T* op, cudaStream_t s) {
+  if (n_coarse < 2) return fail(WF_EINVAL, "coarse operator needs n_coarse >= 2");
+  const int nsweeps = n_coarse - 1;
   switch (L.n) {
     case 4: return launch_coarse<T, 4, false>(L, nsweeps, s, op);
     case 8: return launch_coarse<T, 8, false>(L, nsweeps, s, op);
@@ -1927,7 +2001,8 @@ static int vcycle(std::vector<Lvl<T>>& lv, const wf_case& c, cudaStream_t s,
     } else if (res[0] && !split0_in) {
       WF_TRY(split_in(lv[0], !rhs0_ready, s));
     }
-    if (l == L - 1 && L > 1 && c.mg_cop && c.mg_cop_part && cop_size_ok(lv[l].n))
+    if (l == L - 1 && L > 1 && c.mg_cop && c.mg_cop_part && c.n_coarse >= 2 &&
+        cop_size_ok(lv[l].n))
       WF_TRY(apply_coarse_op<T>(lv[l], (const T*)c.mg_cop, (T*)c.mg_cop_part, s));
     else if (res[l])
       WF_TRY(split_sweeps(lv[l], c.n_pre, s));
@@ -2110,8 +2185,8 @@ int coarse_op_elems(int n, int nlev, int64_t* op_elems, int64_t* scratch_elems) 
   if (!cop_size_ok(nc))
     return fail(WF_EUNSUPPORTED, "coarse operator: coarsest edge must be 4..24, step 4");
   const int64_t N = (int64_t)nc * nc * nc;
-  if (op_elems) *op_elems = N * N;
-  if (scratch_elems) *scratch_elems = (int64_t)COP_CH * N;
+  if (op_elems) *op_elems = (N / 2) * (N / 2);
+  if (scratch_elems) *scratch_elems = (int64_t)COP_CH * (N / 2);
   return WF_OK;
 }
 
@@ -2206,7 +2281,7 @@ int mg_coarse_solve_pair(const wf_case& c, double* phi, const double* rhs, cudaS
   const long m = (long)L.n + 2;
   WF_CK(launch_k(k_zero<double>, mg_blocks(m * m * m), MG_TPB, 0, s, phi, m * m * m));
   WF_CKL("k_zero");
-  if (c.mg_cop && c.mg_cop_part && !c.mg_fp32 && cop_size_ok(L.n))
+  if (c.mg_cop && c.mg_cop_part && !c.mg_fp32 && c.n_coarse >= 2 && cop_size_ok(L.n))
     return apply_coarse_op<double>(L, (const double*)c.mg_cop, (double*)c.mg_cop_part, s);
   return relax<double>(L, c.n_coarse, s);
 }

@@ -16,13 +16,14 @@ The level-0 ``phi``/``rhs`` arrays serve the standalone harness form
 in FP32 as a correction of an FP64 defect correction: the residual, the
 accumulation of the solution and everything outside the multigrid stay FP64.
 
-``coarse="operator"`` (config ``numerics.mg_coarse``, the default) applies
+``coarse="operator"`` (config ``numerics.mg_coarse``, the default) runs
 the coarsest level's n_coarse sweeps from zero -- a fixed linear map of its
-rhs -- as one precomputed dense operator (``wf_mg_build_coarse_op``), built
-once per (size, spacing, n_coarse, precision) and shared by every
-Multigrid of the process; each instance keeps its own partial-sum scratch.
-Where the coarsest edge is not 4..24 in steps of 4, or the operator would
-exceed ``COARSE_OP_MAX_BYTES``, the sweeps run as before.
+rhs -- through one precomputed dense operator on the even-parity half of
+the cells (``wf_mg_build_coarse_op``) and a closing sweep, built once per
+(size, spacing, n_coarse, precision) and shared by every Multigrid of the
+process; each instance keeps its own partial-sum scratch.  Where the
+coarsest edge is not 4..24 in steps of 4, n_coarse < 2, or the operator
+would exceed ``COARSE_OP_MAX_BYTES``, the sweeps run as before.
 """
 from __future__ import annotations
 
@@ -134,7 +135,7 @@ class Multigrid:
     def _coarse_op(self, c):
         """(operator, scratch) tensors for case `c` of the full hierarchy, or
         None when the coarse sweeps run as sweeps."""
-        if self.coarse != "operator" or c.nlev < 2:
+        if self.coarse != "operator" or c.nlev < 2 or c.n_coarse < 2:
             return None
         op_e, sc_e = ctypes.c_int64(), ctypes.c_int64()
         if _abi.load().wf_mg_coarse_op_elems(c.n, c.nlev, ctypes.byref(op_e),

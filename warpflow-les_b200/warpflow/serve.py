@@ -38,7 +38,7 @@ def case_bytes(n, levels=3, precision="mixed"):
     fields, FP64 multigrid levels (phi, rhs with one ring, level 0
     included), the FP32 copies of every level in mixed precision, a scratch
     of two level arrays per level in the multigrid's precision, the
-    partial-sum scratch of the coarse-level operator (64 coarse-level
+    partial-sum scratch of the coarse-level operator (32 coarse-level
     arrays; the operator itself is shared by every case of the size), and
     two scalar blocks plus one residual slot."""
     fields = NFIELDS * (n + 6) ** 3 * 8
@@ -52,8 +52,9 @@ def case_bytes(n, levels=3, precision="mixed"):
             mg += 2 * m ** 3 * 8
     nc = n >> (levels - 1)
     word = 4 if precision == "mixed" else 8
-    if levels > 1 and nc in (4, 8, 12, 16, 20, 24) and nc ** 6 * word <= COARSE_OP_MAX_BYTES:
-        mg += 64 * nc ** 3 * word
+    if levels > 1 and nc in (4, 8, 12, 16, 20, 24) and \
+            (nc ** 3 // 2) ** 2 * word <= COARSE_OP_MAX_BYTES:
+        mg += 32 * nc ** 3 * word
     return fields + mg + 2 * ctypes.sizeof(_abi.WfScalars) + 8
 
 
@@ -179,6 +180,23 @@ class CavityServer:
                           precision=req.precision, name="req%d" % req.rid)
         return FlowSolver(cfg, build_topology(cfg), self.device,
                           serial=len(self.streams) > 1)
+
+    def warmup(self, requests):
+        """Server start-up, before the stream's clock runs: build and step
+        once a case of every (N, levels, precision) that `requests` use, so
+        that the CUDA context, the library's kernels and the shared
+        coarse-level operators are loaded when the first request arrives."""
+        seen = set()
+        for r in requests:
+            key = (r.n, r.levels, r.precision)
+            if key in seen:
+                continue
+            seen.add(key)
+            sol = self._build(Request(rid=-1, n=r.n, re=r.re, ulid=r.ulid, n_steps=1,
+                                      arrival=0.0, levels=r.levels, precision=r.precision))
+            sol.step()
+            sol.close()
+        torch.cuda.synchronize(self.device)
 
     def run(self, requests, time_scale=1.0):
         """Serve `requests` (arrival times in seconds, compressed by
