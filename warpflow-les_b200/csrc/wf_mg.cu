@@ -120,7 +120,8 @@ __global__ void __launch_bounds__(MG_TPB) k_rbgs(const Lvl<T> L, int color) {
   }
 }
 
-// restriction (multigrid.py:93-119): rhs_c = 1/8 sum of the 8 fine residuals
+// restriction (multigrid.py:93-119): rhs_c = 1/8 sum of the 8 fine residuals;
+// also zeroes the coarse level's phi, ring included
 template <class T>
 __global__ void __launch_bounds__(MG_TPB) k_restrict(const Lvl<T> F, T* rhs_c, Lvl<T> C) {
   pdl_entry();
@@ -152,6 +153,16 @@ __global__ void __launch_bounds__(MG_TPB) k_restrict(const Lvl<T> F, T* rhs_c, L
           acc = acc + res;
         }
     rhs_c[lid(C, ci + 1, cj + 1, ck + 1)] = acc * T(0.125);
+    // the coarse phi starts from zero (multigrid.py:314): this cell and the
+    // ring cells nearest to it (faces, edges, corners), so that every cell
+    // of the (nc+2)^3 array is zeroed exactly once
+    const int i0 = ci == 0 ? -1 : 0, i1 = ci == nc - 1 ? 1 : 0;
+    const int j0 = cj == 0 ? -1 : 0, j1 = cj == nc - 1 ? 1 : 0;
+    const int k0 = ck == 0 ? -1 : 0, k1 = ck == nc - 1 ? 1 : 0;
+    for (int oi = i0; oi <= i1; ++oi)
+      for (int oj = j0; oj <= j1; ++oj)
+        for (int ok = k0; ok <= k1; ++ok)
+          C.phi[lid(C, ci + 1 + oi, cj + 1 + oj, ck + 1 + ok)] = T(0);
   }
 }
 
@@ -1992,9 +2003,6 @@ static int vcycle(std::vector<Lvl<T>>& lv, const wf_case& c, cudaStream_t s,
   for (int l = 0; l < L; ++l) {
     if (l > 0) {
       Lvl<T>& C = vw[l];
-      const long m = (long)C.n + 2;
-      WF_CK(launch_k(k_zero<T>, mg_blocks(m * m * m), MG_TPB, 0, s, C.phi, m * m * m));
-      WF_CKL("k_zero");
       WF_CK(launch_k(k_restrict<T>, cells3(C.n, C.n, C.n), cell_block(), 0, s,
           vw[l - 1], const_cast<T*>(C.rhs), C));
       WF_CKL("k_restrict");

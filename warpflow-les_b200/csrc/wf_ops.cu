@@ -464,30 +464,48 @@ __device__ __forceinline__ double lap1(const double* f, long id, long s, double 
                       d, y);
 }
 
+// one cell (i0, j0, k0 from 0 within the op range) of component COMP
+template <int COMP>
+__device__ __forceinline__ void diff_cell(const wf_case& c, const Geo& g, double alpha,
+                                          double dt, const Divs& dv, int i0, int j0, int k0) {
+  const double* f = c.fld[WF_U + COMP];
+  const double* vis = c.fld[WF_VIS];
+  double* star = c.fld[WF_USTAR + COMP];
+  const long vofs = COMP == 0 ? 0 : (COMP == 1 ? g.sJ : 1);
+  const long id = g.at(NPL + i0, NPL + j0, NPL + k0);
+  const double l4 = lap1(f, id, g.sI, dv.d12[0], dv.y12[0]) +
+                    lap1(f, id, g.sJ, dv.d12[1], dv.y12[1]) + lap1(f, id, 1, dv.d12[2], dv.y12[2]);
+  const double diff = LD(vis, id + vofs) * l4;
+  star[id] = star[id] + dt * alpha * diff;
+}
+
 template <int COMP>
 __global__ void __launch_bounds__(TPB) k_diff(const wf_case c, Geo g, double alpha,
                                              const double* __restrict__ dtp, const Divs dv) {
   pdl_entry();
-  const double* f = c.fld[WF_U + COMP];
-  const double* vis = c.fld[WF_VIS];
-  double* star = c.fld[WF_USTAR + COMP];
-  const double dt = *dtp;
-  const long vofs = COMP == 0 ? 0 : (COMP == 1 ? g.sJ : 1);
   int ni, nj, nk;
   op_dims(COMP, g.n, ni, nj, nk);
-  const long tot = (long)ni * nj * nk;
-  {  // one thread per cell: x = k (runs of 32), y = j (groups of 8), z = i
-    const int kx_ = blockIdx.x * 32 + threadIdx.x, jy_ = blockIdx.y * 8 + threadIdx.y;
-    if (kx_ >= nk || jy_ >= nj) return;
-    const int k = NPL + kx_;
-    const int j = NPL + jy_;
-    const int i = NPL + (int)blockIdx.z;
-    const long id = g.at(i, j, k);
-    const double l4 = lap1(f, id, g.sI, dv.d12[0], dv.y12[0]) +
-                      lap1(f, id, g.sJ, dv.d12[1], dv.y12[1]) + lap1(f, id, 1, dv.d12[2], dv.y12[2]);
-    const double diff = LD(vis, id + vofs) * l4;
-    star[id] = star[id] + dt * alpha * diff;
-  }
+  // one thread per cell: x = k (runs of 32), y = j (groups of 8), z = i
+  const int kx_ = blockIdx.x * 32 + threadIdx.x, jy_ = blockIdx.y * 8 + threadIdx.y;
+  if (kx_ >= nk || jy_ >= nj) return;
+  diff_cell<COMP>(c, g, alpha, *dtp, dv, (int)blockIdx.z, jy_, kx_);
+}
+
+// the three components in one launch: z = comp * n + i.  Each reads only its
+// own velocity component and vis and writes its own star, so this equals the
+// three launches in any order.
+__global__ void __launch_bounds__(TPB) k_diff3(const wf_case c, Geo g, double alpha,
+                                              const double* __restrict__ dtp, const Divs dv) {
+  pdl_entry();
+  const int comp = (int)blockIdx.z / g.n, i0 = (int)blockIdx.z - comp * g.n;
+  int ni, nj, nk;
+  op_dims(comp, g.n, ni, nj, nk);
+  const int kx_ = blockIdx.x * 32 + threadIdx.x, jy_ = blockIdx.y * 8 + threadIdx.y;
+  if (i0 >= ni || kx_ >= nk || jy_ >= nj) return;
+  const double dt = *dtp;
+  if (comp == 0) diff_cell<0>(c, g, alpha, dt, dv, i0, jy_, kx_);
+  else if (comp == 1) diff_cell<1>(c, g, alpha, dt, dv, i0, jy_, kx_);
+  else diff_cell<2>(c, g, alpha, dt, dv, i0, jy_, kx_);
 }
 
 int launch_conv(const wf_case& c, int comp, double alpha, const double* dt,
@@ -519,6 +537,14 @@ int launch_diff(const wf_case& c, int comp, double alpha, const double* dt,
   else if (comp == 2) WF_CK(launch_k(k_diff<2>, gr, bl, 0, s, c, g, alpha, dt, divs_of(c)));
   else return fail(WF_EINVAL, "diff: comp must be 0, 1 or 2");
   WF_CKL("k_diff");
+  return WF_OK;
+}
+
+int launch_diff3(const wf_case& c, double alpha, const double* dt, cudaStream_t s) {
+  Geo g = geo_of(c.n);
+  const dim3 gr = cells3(3 * c.n, c.n, c.n), bl = cell_block();
+  WF_CK(launch_k(k_diff3, gr, bl, 0, s, c, g, alpha, dt, divs_of(c)));
+  WF_CKL("k_diff3");
   return WF_OK;
 }
 
