@@ -26,8 +26,10 @@ def test_poisson_stream_seeded():
 def test_levels_for_keeps_coarse_small():
     from warpflow.serve import levels_for
     assert levels_for(80) == 3
-    assert levels_for(128) == 3      # coarse 32
-    assert levels_for(256) == 4      # coarse 32
+    assert levels_for(96) == 3       # coarse 24, with an operator
+    assert levels_for(112) == 3      # coarse 28 (14 would be slower)
+    assert levels_for(128) == 4      # coarse 16 with an operator, not 32 by sweeps
+    assert levels_for(256) == 5      # coarse 16
     assert (256 >> (levels_for(256) - 1)) <= 32
 
 
