@@ -86,9 +86,9 @@ int launch_init_noise(double* u, double* v, double* w, int n, double amp,
 int launch_checkdt(const wf_case& c, cudaStream_t s);
 int launch_copy_oo(const wf_case& c, cudaStream_t s);
 int launch_wale(const wf_case& c, cudaStream_t s);
-int launch_conv(const wf_case& c, int comp, double alpha, const double* dt, cudaStream_t s);
+int launch_conv(const wf_case& c, int comp, double alpha, const double* dt, cudaStream_t s,
+                bool with_diff = false);
 int launch_diff(const wf_case& c, int comp, double alpha, const double* dt, cudaStream_t s);
-int launch_diff3(const wf_case& c, double alpha, const double* dt, cudaStream_t s);
 int launch_calvel(const wf_case& c, double alpha, const double* dt, cudaStream_t s);
 // calmas + projection-loop control (sets graph conditionals when h != 0)
 int launch_calmas(const wf_case& c, unsigned long long h_if,

@@ -375,7 +375,47 @@ __host__ __device__ __forceinline__ void op_dims(int comp, int n, int& ni, int& 
   if (comp == 2) nk = n - 1;
 }
 
+__device__ __forceinline__ double lap1(const double* f, long id, long s, double d,
+                                       double y) {
+  return div_by_recip(-LD(f, id + 2 * s) + 16.0 * LD(f, id + s) - 30.0 * LD(f, id) +
+                          16.0 * LD(f, id - s) - LD(f, id - 2 * s),
+                      d, y);
+}
+
+// star + dt*alpha*diff (kernels.py:221-225), the one form both the separate
+// diffusion and the diffusion fused into the convection use
+__device__ __forceinline__ double diff_add(double star, double dt, double alpha, double diff) {
+  return star + dt * alpha * diff;
+}
+
+// vis * lap4(f) at cell id of component COMP (kernels.py:189-225)
 template <int COMP>
+__device__ __forceinline__ double diff_term(const wf_case& c, const Geo& g, const Divs& dv,
+                                            long id) {
+  const double* f = c.fld[WF_U + COMP];
+  const long vofs = COMP == 0 ? 0 : (COMP == 1 ? g.sJ : 1);
+  const double l4 = lap1(f, id, g.sI, dv.d12[0], dv.y12[0]) +
+                    lap1(f, id, g.sJ, dv.d12[1], dv.y12[1]) + lap1(f, id, 1, dv.d12[2], dv.y12[2]);
+  return LD(c.fld[WF_VIS], id + vofs) * l4;
+}
+
+// one cell (i0, j0, k0 from 0 within the op range) of component COMP
+template <int COMP>
+__device__ __forceinline__ void diff_cell(const wf_case& c, const Geo& g, double alpha,
+                                          double dt, const Divs& dv, int i0, int j0, int k0) {
+  double* star = c.fld[WF_USTAR + COMP];
+  const long id = g.at(NPL + i0, NPL + j0, NPL + k0);
+  star[id] = diff_add(star[id], dt, alpha, diff_term<COMP>(c, g, dv, id));
+}
+
+// DIFF: also add the component's diffusion to star in the same pass.  The
+// step's fill of the component between its convection and its diffusion
+// (solver.py:253-263) changes only ghost cells that lie outside the grid in
+// two or more directions -- its other ghost cells are functions of real
+// cells, which do not change in between -- and the diffusion stencil never
+// reaches such cells, so the fused update reads the same values and gives
+// the same star.
+template <int COMP, bool DIFF>
 __global__ void __launch_bounds__(TPB) k_conv(const wf_case c, Geo g, double alpha,
                                              const double* __restrict__ dtp, const Divs dv) {
   pdl_entry();
@@ -453,30 +493,9 @@ __global__ void __launch_bounds__(TPB) k_conv(const wf_case c, Geo g, double alp
       const double dvwdy = div_by_recip(-p1 + 27.0 * p0 - 27.0 * m1 + m2, dv.d24[1], dv.y24[1]);
       tot3 = duwdx + dvwdy + dw2dz;
     }
-    star[id] = LD(oo, id) - dt * alpha * tot3;
+    const double s1 = LD(oo, id) - dt * alpha * tot3;
+    star[id] = DIFF ? diff_add(s1, dt, alpha, diff_term<COMP>(c, g, dv, id)) : s1;
   }
-}
-
-__device__ __forceinline__ double lap1(const double* f, long id, long s, double d,
-                                       double y) {
-  return div_by_recip(-LD(f, id + 2 * s) + 16.0 * LD(f, id + s) - 30.0 * LD(f, id) +
-                          16.0 * LD(f, id - s) - LD(f, id - 2 * s),
-                      d, y);
-}
-
-// one cell (i0, j0, k0 from 0 within the op range) of component COMP
-template <int COMP>
-__device__ __forceinline__ void diff_cell(const wf_case& c, const Geo& g, double alpha,
-                                          double dt, const Divs& dv, int i0, int j0, int k0) {
-  const double* f = c.fld[WF_U + COMP];
-  const double* vis = c.fld[WF_VIS];
-  double* star = c.fld[WF_USTAR + COMP];
-  const long vofs = COMP == 0 ? 0 : (COMP == 1 ? g.sJ : 1);
-  const long id = g.at(NPL + i0, NPL + j0, NPL + k0);
-  const double l4 = lap1(f, id, g.sI, dv.d12[0], dv.y12[0]) +
-                    lap1(f, id, g.sJ, dv.d12[1], dv.y12[1]) + lap1(f, id, 1, dv.d12[2], dv.y12[2]);
-  const double diff = LD(vis, id + vofs) * l4;
-  star[id] = star[id] + dt * alpha * diff;
 }
 
 template <int COMP>
@@ -491,35 +510,20 @@ __global__ void __launch_bounds__(TPB) k_diff(const wf_case c, Geo g, double alp
   diff_cell<COMP>(c, g, alpha, *dtp, dv, (int)blockIdx.z, jy_, kx_);
 }
 
-// the three components in one launch: z = comp * n + i.  Each reads only its
-// own velocity component and vis and writes its own star, so this equals the
-// three launches in any order.
-__global__ void __launch_bounds__(TPB) k_diff3(const wf_case c, Geo g, double alpha,
-                                              const double* __restrict__ dtp, const Divs dv) {
-  pdl_entry();
-  const int comp = (int)blockIdx.z / g.n, i0 = (int)blockIdx.z - comp * g.n;
-  int ni, nj, nk;
-  op_dims(comp, g.n, ni, nj, nk);
-  const int kx_ = blockIdx.x * 32 + threadIdx.x, jy_ = blockIdx.y * 8 + threadIdx.y;
-  if (i0 >= ni || kx_ >= nk || jy_ >= nj) return;
-  const double dt = *dtp;
-  if (comp == 0) diff_cell<0>(c, g, alpha, dt, dv, i0, jy_, kx_);
-  else if (comp == 1) diff_cell<1>(c, g, alpha, dt, dv, i0, jy_, kx_);
-  else diff_cell<2>(c, g, alpha, dt, dv, i0, jy_, kx_);
-}
 
 int launch_conv(const wf_case& c, int comp, double alpha, const double* dt,
-                cudaStream_t s) {
+                cudaStream_t s, bool with_diff) {
   Geo g = geo_of(c.n);
   const long tot = (long)c.n * c.n * (c.n - 1);
   const int nb = nblocks(tot);
   int ni, nj, nk;
   op_dims(comp, c.n, ni, nj, nk);
   const dim3 gr = cells3(ni, nj, nk), bl = cell_block();
-  if (comp == 0) WF_CK(launch_k(k_conv<0>, gr, bl, 0, s, c, g, alpha, dt, divs_of(c)));
-  else if (comp == 1) WF_CK(launch_k(k_conv<1>, gr, bl, 0, s, c, g, alpha, dt, divs_of(c)));
-  else if (comp == 2) WF_CK(launch_k(k_conv<2>, gr, bl, 0, s, c, g, alpha, dt, divs_of(c)));
-  else return fail(WF_EINVAL, "conv: comp must be 0, 1 or 2");
+  if (comp < 0 || comp > 2) return fail(WF_EINVAL, "conv: comp must be 0, 1 or 2");
+  void (*const kern[2][3])(const wf_case, Geo, double, const double*, const Divs) = {
+      {k_conv<0, false>, k_conv<1, false>, k_conv<2, false>},
+      {k_conv<0, true>, k_conv<1, true>, k_conv<2, true>}};
+  WF_CK(launch_k(kern[with_diff ? 1 : 0][comp], gr, bl, 0, s, c, g, alpha, dt, divs_of(c)));
   WF_CKL("k_conv");
   return WF_OK;
 }
@@ -540,13 +544,6 @@ int launch_diff(const wf_case& c, int comp, double alpha, const double* dt,
   return WF_OK;
 }
 
-int launch_diff3(const wf_case& c, double alpha, const double* dt, cudaStream_t s) {
-  Geo g = geo_of(c.n);
-  const dim3 gr = cells3(3 * c.n, c.n, c.n), bl = cell_block();
-  WF_CK(launch_k(k_diff3, gr, bl, 0, s, c, g, alpha, dt, divs_of(c)));
-  WF_CKL("k_diff3");
-  return WF_OK;
-}
 
 // --------------------------------------------------------------------------
 // calvel (kernels.py:232-264): the three components in one launch

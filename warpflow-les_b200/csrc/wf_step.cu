@@ -3,8 +3,8 @@
 //
 // Step layout (launch order follows solver.py exactly):
 //   prologue : checkdt -> uoo/voo/woo copy -> WALE + vis fill ->
-//              2 x RK stage (fill+conv per component, fill u,v,w + the
-//              three diffusions, calvel(0.5) after stage 1) -> calvel(1.0)
+//              2 x RK stage (fill + convection-diffusion per component,
+//              fill u,v,w, calvel(0.5) after stage 1) -> calvel(1.0)
 //   loop     : calmas + control  [if run] MG solve, p += pp, pbound,
 //              calvel(1.0)  -- repeated while the control says so
 //   epilogue : fill u, v, w
@@ -83,17 +83,17 @@ static int step_prologue(const wf_case& c, cudaStream_t s) {
   const double* dt = &c.sc->dt;
   const double alfark[2] = {0.5, 1.0};  // solver.py:26
   for (int st = 0; st < 2; ++st) {
+    // each component's diffusion runs inside its convection pass (k_conv
+    // with DIFF: the fill between them changes no cell the diffusion reads)
     for (int comp = 0; comp < 3; ++comp) {
       WF_TRY(fill_comp(c, comp, s));
-      WF_TRY(launch_conv(c, comp, alfark[st], dt, s));
+      WF_TRY(launch_conv(c, comp, alfark[st], dt, s, true));
     }
-    // solver.py:258-263 fills u, diffuses u, fills v, ...: each diffusion
-    // reads only its own component (and vis), so the three fills run first
-    // (one 3-field fill) and the three diffusions in one launch
+    // the fills solver.py:258-263 runs before each diffusion still set the
+    // ghost edges and corners that later fills read
     FillReq r[3] = {{c.fld[WF_U], FILL_U, c.ulid}, {c.fld[WF_V], FILL_V, 0.0},
                     {c.fld[WF_W], FILL_W, 0.0}};
     WF_TRY(launch_fills(r, 3, c.n, s));
-    WF_TRY(launch_diff3(c, alfark[st], dt, s));
     if (st == 0) WF_TRY(launch_calvel(c, alfark[st], dt, s));
   }
   return launch_calvel(c, 1.0, dt, s);
