@@ -132,6 +132,24 @@ __global__ void __launch_bounds__(MG_TPB) k_restrict(const Lvl<T> F, T* rhs_c, L
     const int ck = kx_;
     const int cj = jy_;
     const int ci = (int)blockIdx.z;
+    // the fine phi values the 8 residuals read -- the 2x2x2 block and its
+    // face neighbours, P[a][b][c] at fine cell (2ci-1+a, 2cj-1+b, 2ck-1+c)
+    // -- each loaded once (32 loads instead of 56)
+    const int i0 = 2 * ci, j0 = 2 * cj, k0 = 2 * ck;
+    const int H = (n + 2) >> 1;
+    long kp[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) kp[q] = F.split ? spos(k0 + q, H) : (k0 + q);
+    const T* p = F.phi;
+    T P[4][4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if ((a == 0 || a == 3) + (b == 0 || b == 3) + (q == 0 || q == 3) <= 1)
+            P[a][b][q] = p[(long)(i0 + a) * F.sI + (long)(j0 + b) * F.sJ + kp[q]];
     T acc = T(0);
 #pragma unroll
     for (int di = 0; di < 2; ++di)
@@ -139,29 +157,28 @@ __global__ void __launch_bounds__(MG_TPB) k_restrict(const Lvl<T> F, T* rhs_c, L
       for (int dj = 0; dj < 2; ++dj)
 #pragma unroll
         for (int dk = 0; dk < 2; ++dk) {
-          const int i = 2 * ci + di, j = 2 * cj + dj, k = 2 * ck + dk;
-          const long c = lid(F, i + 1, j + 1, k + 1);
+          const int i = i0 + di, j = j0 + dj, k = k0 + dk;
           const T aw = i > 0 ? F.ax : T(0), ae = i < n - 1 ? F.ax : T(0);
           const T as = j > 0 ? F.ay : T(0), an = j < n - 1 ? F.ay : T(0);
           const T ab = k > 0 ? F.az : T(0), at = k < n - 1 ? F.az : T(0);
           const T ap = -(aw + ae + as + an + ab + at);
-          const T* p = F.phi;
-          const long cb = lid(F, i + 1, j + 1, k), ct = lid(F, i + 1, j + 1, k + 2);
-          const T res = F.rhs[c] - (aw * p[c - F.sI] + ae * p[c + F.sI] + as * p[c - F.sJ] +
-                                    an * p[c + F.sJ] + ab * p[cb] + at * p[ct] +
-                                    ap * p[c]);
+          const int a = 1 + di, b = 1 + dj, q = 1 + dk;
+          const T r = F.rhs[(long)(i + 1) * F.sI + (long)(j + 1) * F.sJ + kp[q]];
+          const T res = r - (aw * P[a - 1][b][q] + ae * P[a + 1][b][q] + as * P[a][b - 1][q] +
+                             an * P[a][b + 1][q] + ab * P[a][b][q - 1] + at * P[a][b][q + 1] +
+                             ap * P[a][b][q]);
           acc = acc + res;
         }
     rhs_c[lid(C, ci + 1, cj + 1, ck + 1)] = acc * T(0.125);
     // the coarse phi starts from zero (multigrid.py:314): this cell and the
     // ring cells nearest to it (faces, edges, corners), so that every cell
     // of the (nc+2)^3 array is zeroed exactly once
-    const int i0 = ci == 0 ? -1 : 0, i1 = ci == nc - 1 ? 1 : 0;
-    const int j0 = cj == 0 ? -1 : 0, j1 = cj == nc - 1 ? 1 : 0;
-    const int k0 = ck == 0 ? -1 : 0, k1 = ck == nc - 1 ? 1 : 0;
-    for (int oi = i0; oi <= i1; ++oi)
-      for (int oj = j0; oj <= j1; ++oj)
-        for (int ok = k0; ok <= k1; ++ok)
+    const int zi0 = ci == 0 ? -1 : 0, zi1 = ci == nc - 1 ? 1 : 0;
+    const int zj0 = cj == 0 ? -1 : 0, zj1 = cj == nc - 1 ? 1 : 0;
+    const int zk0 = ck == 0 ? -1 : 0, zk1 = ck == nc - 1 ? 1 : 0;
+    for (int oi = zi0; oi <= zi1; ++oi)
+      for (int oj = zj0; oj <= zj1; ++oj)
+        for (int ok = zk0; ok <= zk1; ++ok)
           C.phi[lid(C, ci + 1 + oi, cj + 1 + oj, ck + 1 + ok)] = T(0);
   }
 }
@@ -225,6 +242,60 @@ __global__ void __launch_bounds__(MG_TPB) k_prolong(const Lvl<T> C, Lvl<T> F) {
     F.phi[c] = x;
     if (!F.split) ring_mirror(F, i, j, k, c, x);
   }
+}
+
+// the same prolongation with one thread per COARSE cell writing its 2x2x2
+// fine cells from the 27 coarse values around it, each loaded once (27 loads
+// for 8 outputs instead of 64); every output sums the same terms in the
+// same order as k_prolong, so the results are the same bits
+template <class T>
+__global__ void __launch_bounds__(MG_TPB) k_prolong8(const Lvl<T> C, Lvl<T> F) {
+  pdl_entry();
+  const int nc = C.n;
+  const int ck = blockIdx.x * 32 + threadIdx.x, cj = blockIdx.y * 8 + threadIdx.y;
+  if (ck >= nc || cj >= nc) return;
+  const int ci = (int)blockIdx.z;
+  const int Hc = (nc + 2) >> 1;
+  long kq[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) kq[q] = C.split ? spos(ck + q, Hc) : (ck + q);
+  T Q[3][3][3];   // coarse (ci-1+a, cj-1+b, ck-1+q), ring included
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int q = 0; q < 3; ++q)
+        Q[a][b][q] = C.phi[(long)(ci + a) * C.sI + (long)(cj + b) * C.sJ + kq[q]];
+#pragma unroll
+  for (int pi = 0; pi < 2; ++pi)
+#pragma unroll
+    for (int pj = 0; pj < 2; ++pj)
+#pragma unroll
+      for (int pk = 0; pk < 2; ++pk) {
+        const T wx0 = pi == 0 ? T(0.25) : T(0.75);
+        const T wy0 = pj == 0 ? T(0.25) : T(0.75);
+        const T wz0 = pk == 0 ? T(0.25) : T(0.75);
+        T acc = T(0);
+#pragma unroll
+        for (int di = 0; di < 2; ++di) {
+          const T wxi = di == 0 ? wx0 : T(1) - wx0;
+#pragma unroll
+          for (int dj = 0; dj < 2; ++dj) {
+            const T wyj = dj == 0 ? wy0 : T(1) - wy0;
+#pragma unroll
+            for (int dk = 0; dk < 2; ++dk) {
+              const T wzk = dk == 0 ? wz0 : T(1) - wz0;
+              acc = acc + wxi * wyj * wzk * Q[pi + di][pj + dj][pk + dk];
+            }
+          }
+        }
+        const int i = 2 * ci + pi, j = 2 * cj + pj, k = 2 * ck + pk;
+        const long c = lid(F, i + 1, j + 1, k + 1);
+        const T x = F.phi[c] + acc;
+        F.phi[c] = x;
+        if (!F.split) ring_mirror(F, i, j, k, c, x);
+      }
 }
 
 // ---- a whole relax() of a small level inside one CTA's shared memory ------
@@ -2018,9 +2089,17 @@ static int vcycle(std::vector<Lvl<T>>& lv, const wf_case& c, cudaStream_t s,
       WF_TRY(relax(lv[l], l < L - 1 ? c.n_pre : c.n_coarse, s, l == 0 && rhs0_ready));
   }
   for (int l = L - 2; l >= 0; --l) {
-    WF_CK(launch_k(k_prolong<T>, cells3(lv[l].n, lv[l].n, lv[l].n), cell_block(), 0, s,
-                   vw[l + 1], vw[l]));
-    WF_CKL("k_prolong");
+    // fine levels from 64: one thread per coarse cell (fewer loads); smaller
+    // ones keep one thread per fine cell (more threads in flight)
+    if (lv[l].n >= 64 && (lv[l].n & 1) == 0) {
+      WF_CK(launch_k(k_prolong8<T>, cells3(lv[l + 1].n, lv[l + 1].n, lv[l + 1].n), cell_block(),
+                     0, s, vw[l + 1], vw[l]));
+      WF_CKL("k_prolong8");
+    } else {
+      WF_CK(launch_k(k_prolong<T>, cells3(lv[l].n, lv[l].n, lv[l].n), cell_block(), 0, s,
+                     vw[l + 1], vw[l]));
+      WF_CKL("k_prolong");
+    }
     if (res[l]) {
       WF_TRY(split_sweeps(lv[l], c.n_post, s));
       if (l > 0) {
