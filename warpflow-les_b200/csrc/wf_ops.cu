@@ -6,6 +6,7 @@
 // NPL..NPL+n-1.  One thread per output cell; consecutive threads walk k so
 // every access of a warp is a contiguous run.
 #include <algorithm>
+#include <cmath>
 
 #include "wf_dev.cuh"
 #include "wf_internal.h"
@@ -265,15 +266,16 @@ int launch_copy_oo(const wf_case& c, cudaStream_t s) {
 // --------------------------------------------------------------------------
 // WALE eddy viscosity (kernels.py:297-367)
 // --------------------------------------------------------------------------
-__global__ void __launch_bounds__(TPB) k_wale(const wf_case c, Geo g, const Divs dv) {
+// ls = cw * (dx dy dz)^(1/3) comes from the host (kernels.py:360-361 compute
+// it in every thread; one host pow gives the same value without a device
+// pow per cell)
+__global__ void __launch_bounds__(TPB) k_wale(const wf_case c, Geo g, const Divs dv,
+                                             const double ls) {
   pdl_entry();
   const double* u = c.fld[WF_U];
   const double* v = c.fld[WF_V];
   const double* w = c.fld[WF_W];
   double* vis = c.fld[WF_VIS];
-  const double dx = c.dx, dy = c.dy, dz = c.dz;
-  const double delta = pow(dx * dy * dz, 1.0 / 3.0);
-  const double ls = c.cw * delta;
   const long sI = g.sI, sJ = g.sJ;
   {  // one thread per cell: x = k (runs of 32), y = j (groups of 8), z = i
     const int kx_ = blockIdx.x * 32 + threadIdx.x, jy_ = blockIdx.y * 8 + threadIdx.y;
@@ -349,7 +351,8 @@ int launch_wale(const wf_case& c, cudaStream_t s) {
   Geo g = geo_of(c.n);
   const long tot = (long)c.n * c.n * c.n;
   if (c.sgs) {
-    WF_CK(launch_k(k_wale, cells3(c.n, c.n, c.n), cell_block(), 0, s, c, g, divs_of(c)));
+    const double ls = c.cw * std::pow(c.dx * c.dy * c.dz, 1.0 / 3.0);
+    WF_CK(launch_k(k_wale, cells3(c.n, c.n, c.n), cell_block(), 0, s, c, g, divs_of(c), ls));
     WF_CKL("k_wale");
     FillReq r{c.fld[WF_VIS], FILL_VIS, c.rrey};
     return launch_fills(&r, 1, c.n, s);
