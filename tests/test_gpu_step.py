@@ -61,6 +61,17 @@ def test_serial_stepper_bit_identical():
         np.testing.assert_array_equal(a.f[name].numpy(), b.f[name].numpy())
 
 
+def test_old_velocities_are_the_whole_pre_step_fields():
+    """uoo/voo/woo hold u/v/w as they were when the step began, ghost layers
+    included (solver.py:223-225; the step copies them in its dt pass)."""
+    sol = _solver(make_cfg(20, levels=2))
+    sol.step()
+    before = {k: sol.f[k].numpy() for k in ("u", "v", "w")}
+    sol.step()
+    for k in ("u", "v", "w"):
+        np.testing.assert_array_equal(sol.f[k + "oo"].numpy(), before[k])
+
+
 def _compare_run(cfg, nsteps, check_every=1):
     sol = _solver(cfg)
     ora = O.OracleSolver(cfg)
