@@ -16,6 +16,7 @@ dependency, so it is tested on the CPU.
 from __future__ import annotations
 
 import collections
+import concurrent.futures
 import ctypes
 import time
 from dataclasses import dataclass, field
@@ -214,58 +215,82 @@ class CavityServer:
         for r in sorted(requests, key=lambda r: r.arrival):
             self.adm.submit(r)
         live = {}          # rid -> (req, solver, admitted_at, steps_done)
+        building = {}      # rid -> (req, future of its solver, admitted_at)
         t0 = time.perf_counter()
         main = torch.cuda.current_stream(self.device)
         total = len(requests)
-        while len(self.results) < total:
-            now = (time.perf_counter() - t0) / time_scale
-            for req in self.adm.admit(now):
-                live[req.rid] = [req, self._build(req), now, 0]
-            if not live:
-                nxt = self.adm.queue[0].arrival if self.adm.queue else now
-                time.sleep(max(0.0, (nxt - now) * time_scale))
-                continue
-            rids = list(live)
-            start = torch.cuda.Event()
-            start.record(main)
-            used = set()
-            for slot, rid in enumerate(rids):
-                s = self.streams[slot % len(self.streams)]
-                used.add(s)
-                s.wait_event(start)
-                with torch.cuda.stream(s):
-                    live[rid][1].launch_step()
-            for s in used:
-                main.wait_stream(s)
-            blob = torch.cat([live[rid][1]._sc for rid in rids])
-            if blob.numel() > self._host.numel():
-                self._host = torch.empty(blob.numel(), dtype=torch.uint8, pin_memory=True)
-            host = self._host[:blob.numel()]
-            host.copy_(blob, non_blocking=True)
-            main.synchronize()
-            self.step_batches += 1
-            done_t = (time.perf_counter() - t0) / time_scale
-            for k, rid in enumerate(rids):
-                req, sol, adm_t, nst = live[rid]
-                view = _abi.WfScalars.from_address(host.data_ptr() + k * self._nsc)
-                err = ""
-                try:
-                    info = sol.apply_scalars(view)
-                except RuntimeError as e:
-                    info, err = {}, str(e)
-                nst += 1
-                live[rid][3] = nst
-                self.cell_steps += req.n ** 3
-                if nst >= req.n_steps or err:
-                    self.results[rid] = Completion(rid, req.arrival, adm_t, done_t, nst,
-                                                   req.n ** 3, info, err)
-                    if self.keep_fields:
-                        self.fields[rid] = {k2: sol.f[k2].numpy() for k2 in ("u", "v", "w", "p")}
-                    sol.close()
-                    del live[rid]
-                    self.adm.release(rid)
+        # Solvers are built on a worker thread: their host-side set-up
+        # (allocations, graph capture and instantiation) would otherwise
+        # hold up the next step of every case already resident.
+        pool = concurrent.futures.ThreadPoolExecutor(max_workers=1)
+        try:
+            while len(self.results) < total:
+                now = (time.perf_counter() - t0) / time_scale
+                for req in self.adm.admit(now):
+                    building[req.rid] = (req, pool.submit(self._build_on_worker, req), now)
+                for rid in [r for r, (_, fut, _) in building.items() if fut.done()]:
+                    req, fut, adm_t = building.pop(rid)
+                    live[rid] = [req, fut.result(), adm_t, 0]
+                if not live:
+                    if building:
+                        concurrent.futures.wait([fut for _, fut, _ in building.values()],
+                                                return_when=concurrent.futures.FIRST_COMPLETED)
+                    else:
+                        nxt = self.adm.queue[0].arrival if self.adm.queue else now
+                        time.sleep(max(0.0, (nxt - now) * time_scale))
+                    continue
+                self._step_batch(live, main, t0, time_scale)
+        finally:
+            pool.shutdown(wait=True)
         self.wall = time.perf_counter() - t0
         return [self.results[r.rid] for r in requests]
+
+    def _build_on_worker(self, req):
+        torch.cuda.set_device(self.device)   # the worker thread's current device
+        return self._build(req)
+
+    def _step_batch(self, live, main, t0, time_scale):
+        """One step of every live case, then their scalar blocks in one copy;
+        finished cases leave."""
+        rids = list(live)
+        start = torch.cuda.Event()
+        start.record(main)
+        used = set()
+        for slot, rid in enumerate(rids):
+            s = self.streams[slot % len(self.streams)]
+            used.add(s)
+            s.wait_event(start)
+            with torch.cuda.stream(s):
+                live[rid][1].launch_step()
+        for s in used:
+            main.wait_stream(s)
+        blob = torch.cat([live[rid][1]._sc for rid in rids])
+        if blob.numel() > self._host.numel():
+            self._host = torch.empty(blob.numel(), dtype=torch.uint8, pin_memory=True)
+        host = self._host[:blob.numel()]
+        host.copy_(blob, non_blocking=True)
+        main.synchronize()
+        self.step_batches += 1
+        done_t = (time.perf_counter() - t0) / time_scale
+        for k, rid in enumerate(rids):
+            req, sol, adm_t, nst = live[rid]
+            view = _abi.WfScalars.from_address(host.data_ptr() + k * self._nsc)
+            err = ""
+            try:
+                info = sol.apply_scalars(view)
+            except RuntimeError as e:
+                info, err = {}, str(e)
+            nst += 1
+            live[rid][3] = nst
+            self.cell_steps += req.n ** 3
+            if nst >= req.n_steps or err:
+                self.results[rid] = Completion(rid, req.arrival, adm_t, done_t, nst,
+                                               req.n ** 3, info, err)
+                if self.keep_fields:
+                    self.fields[rid] = {k2: sol.f[k2].numpy() for k2 in ("u", "v", "w", "p")}
+                sol.close()
+                del live[rid]
+                self.adm.release(rid)
 
     def summary(self):
         lat = np.array([c.latency for c in self.results.values()])
