@@ -201,11 +201,17 @@ WF_API int wf_mg_solve(const wf_case* c, void* stream);
  * buffer from their own fixed pool or memory budget.  The coarse levels live
  * in a 4 MiB array compiled into the library (held on every GPU that loads
  * it until the process exits), enough for n <= 112 at 3 levels; larger
- * problems return WF_EINVAL.  Nothing is allocated.  The first call on a
- * device looks up the array's address; make it before any stream capture.
- * Calls share the array: calls that overlap on the GPU race. */
+ * problems return WF_EINVAL.  Nothing is allocated.  The first call in a
+ * CUDA context looks up the array's address; make it before any stream
+ * capture.  Calls share the array: calls that overlap on the GPU race. */
 WF_API int wf_mg_solve_noalloc(const double* su, double* pp, int32_t n, int32_t nlev,
                                double dx, double dy, double dz, void* stream);
+/* No counterpart in the reference.  The device status word of the last
+ * wf_mg_solve_noalloc call (it clears the word when it starts): waits for
+ * `stream`, then *status = WF_ST_OK, or WF_ST_WAIT_TIMEOUT when a bounded
+ * device-side wait of its coarse-level kernels gave up (pp is then
+ * invalid).  Allocates nothing. */
+WF_API int wf_mg_noalloc_status(void* stream, int32_t* status);
 /* multigrid.py:301-322 one V-cycle on an explicit level-0 pair (phi, rhs)
  * of (n+2)^3 doubles each (the standalone harness of tests/test_mg.py). */
 WF_API int wf_mg_vcycle(const wf_case* c, double* phi0, const double* rhs0, void* stream);
@@ -221,6 +227,16 @@ WF_API int wf_mg_residual_max(const wf_case* c, const double* phi0, const double
                        double* out_dev, void* stream);
 /* bcs.py:326-360 _mk_neumann on all six faces of a level-0 pair. */
 WF_API int wf_mg_refill(const wf_case* c, double* phi0, void* stream);
+
+/* No counterpart in the reference: a check of the library's bounded
+ * device-side waits.  One CTA runs one wait that can never complete and
+ * must give up after `tries` tries (1 .. 2^22): kind 0 the grid barrier of
+ * the cooperative relax (gbar: two zeroed words, declared block count one
+ * above the launched one), kind 1 the mbarrier wait of the point-to-point
+ * coarse kernels on bytes that nobody sends.  *err (device) receives
+ * WF_ST_WAIT_TIMEOUT; the kernel returns with nothing in flight. */
+WF_API int wf_wait_probe(uint32_t* gbar, int32_t* err, int32_t kind, int32_t tries,
+                         void* stream);
 
 /* ---- whole step (solver.py:217-271) ------------------------------------ */
 typedef struct wf_stepper wf_stepper;

@@ -58,7 +58,12 @@ ALL_FIELDS = ("u", "v", "w", "p", "ustar", "vstar", "wstar", "uoo", "voo",
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) not in (2, 3) or not os.path.isdir(os.path.join(sys.argv[1], "warpflow")):
+        sys.exit("usage: python tests/golden/make_golden.py <path of the warpflow-les "
+                 "source tree, the directory holding warpflow/> [mg]\n"
+                 "  mg: regenerate only the multigrid harness file")
+    ref = sys.argv[1]
+    only_mg = len(sys.argv) == 3 and sys.argv[2] == "mg"
     sys.path.insert(0, os.path.join(HERE, "refshim"))
     sys.path.insert(0, ref)
     from warpflow.config import load_case
@@ -67,7 +72,7 @@ def main():
     from warpflow.topology import build_topology
 
     tmp = tempfile.mkdtemp()
-    for tag, n, lev, steps, re, sgs, noise, ulid, vdt, keep in CAVITY_CASES:
+    for tag, n, lev, steps, re, sgs, noise, ulid, vdt, keep in (() if only_mg else CAVITY_CASES):
         path = os.path.join(tmp, tag + ".yaml")
         with open(path, "w") as fh:
             fh.write(CASE.format(name=tag, n=n, re=re, sgs=sgs, noise=noise,
@@ -114,6 +119,16 @@ def main():
     lev0.phi.zero_()
     mg._refill(lev0)
     out = {"rhs": h}
+    # the coefficient arrays _mgcoeff writes (multigrid.py:23-67), at the
+    # harness spacing and at three different spacings per axis
+    coef = ("aw", "ae", "as_", "an", "ab", "at", "ap")
+    for l, lv in enumerate(mg.levels):
+        for name in coef:
+            out["coef%d_%s" % (l, name)] = getattr(lv, name).numpy().copy()
+    mgx = Multigrid(cfg, topo, "cpu", 0.1, 0.2, 0.3)
+    for l, lv in enumerate(mgx.levels):
+        for name in coef:
+            out["coefx%d_%s" % (l, name)] = getattr(lv, name).numpy().copy()
     for c in range(2):
         mg._vcycle()
         out["phi_c%d" % c] = lev0.phi.numpy().copy()

@@ -6,7 +6,8 @@ them with the coarse multigrid levels in a fixed array inside the library.
 This test calls it through the C ABI, twice in a row with different
 right-hand sides, and checks each result against the regular entry point
 wf_mg_solve (whose level buffers the caller allocates), within the same
-tolerance as the other multigrid tests.  It also checks the size limit.
+tolerance as the other multigrid tests, and reads the call's device status
+word (no bounded wait may have given up).  It also checks the size limit.
 """
 import ctypes
 
@@ -27,7 +28,9 @@ def _regular_solve(mg, su, pp):
     return pp.numpy()
 
 
-@pytest.mark.parametrize("n,levels", [(32, 3), (80, 3)])
+# (112, 3) fills the static array almost to its end; (16, 1) runs the 300
+# coarse sweeps on level 0 itself
+@pytest.mark.parametrize("n,levels", [(32, 3), (80, 3), (112, 3), (16, 1)])
 def test_noalloc_matches_regular_solve_twice(n, levels):
     from helpers import make_cfg
     from warpflow import Multigrid, _abi, build_topology
@@ -49,6 +52,9 @@ def test_noalloc_matches_regular_solve_twice(n, levels):
         pp_new.assign(rng.standard_normal(shape))  # must be overwritten
         rc = lib.wf_mg_solve_noalloc(su.ptr, pp_new.ptr, n, levels, h, h, h, _stream())
         assert rc == 0, lib.wf_last_error()
+        status = ctypes.c_int32(-1)
+        assert lib.wf_mg_noalloc_status(_stream(), ctypes.byref(status)) == 0
+        assert status.value == _abi.ST_OK, status.value
         torch.cuda.synchronize()
         got = pp_new.numpy()
         scale = np.abs(ref).max()

@@ -109,6 +109,8 @@ int set_coarse_strategy(int n, int fp32, int strategy);
 int mg_dc_cycle_pair(const wf_case& c, double* phi0, const double* rhs0, cudaStream_t s);
 int mg_solve_noalloc(const double* su, double* pp, int n, int nlev, double dx, double dy,
                      double dz, cudaStream_t s);
+int mg_noalloc_status(void* stream, int32_t* status);
+int wait_probe(unsigned* gbar, int* err, int kind, int tries, cudaStream_t s);
 int mg_residual_max_pair(const wf_case& c, const double* phi0, const double* rhs0,
                          double* out, cudaStream_t s);
 

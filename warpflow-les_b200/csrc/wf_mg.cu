@@ -18,6 +18,7 @@
 // Level 0 works in place: phi is the (n+2)^3 core of `pp` and rhs the core
 // of `su`, both with the padded (n+6) strides.
 #include <cooperative_groups.h>
+#include <cuda.h>
 
 #include <algorithm>
 #include <cstdlib>
@@ -1833,7 +1834,7 @@ static int launch_sweep2(const T* src, long sIs, long sJs, T* dst, long sId, lon
 constexpr int GBAR_SPINS = 1 << 22;
 
 __device__ __forceinline__ void grid_barrier(unsigned* gbar, unsigned nblocks, int* err,
-                                             bool& timed_out) {
+                                             bool& timed_out, int spins = GBAR_SPINS) {
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned* vgen = gbar + 1;
@@ -1846,7 +1847,7 @@ __device__ __forceinline__ void grid_barrier(unsigned* gbar, unsigned nblocks, i
     } else if (!timed_out) {
       int it = 0;
       while (*vgen == gen) {
-        if (++it > GBAR_SPINS) {
+        if (++it > spins) {
           timed_out = true;
           if (err) atomicExch(err, (int)WF_ST_WAIT_TIMEOUT);
           break;
@@ -1930,6 +1931,45 @@ static int persist_min_n() {
     v = e ? atoi(e) : 1 << 30;
   }
   return v;
+}
+
+// ---- a check of the bounded waits ------------------------------------------
+// kind 0: the grid barrier above, entered by the one launched CTA with a
+// declared count of two, so the barrier can never open; kind 1: the
+// mbarrier wait of the point-to-point coarse kernel on a barrier that
+// expects 8 bytes which nobody sends.  Either wait gives up after `tries`
+// tries and records WF_ST_WAIT_TIMEOUT in *err; nothing is in flight when
+// the kernel returns.
+__global__ void k_wait_probe(unsigned* gbar, int* err, int kind, int tries) {
+  if (kind == 0) {
+    bool timed_out = false;
+    grid_barrier(gbar, gridDim.x + 1, err, timed_out, tries);
+    return;
+  }
+  __shared__ __align__(8) unsigned long long mbar;
+  const uint32_t mb = smem_u32(&mbar);
+  if (threadIdx.x == 0) {
+    mbar_init(mb, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    mbar_arrive_expect_tx(mb, 8u);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    bool ok = false;
+    for (int it = 0; it < tries && !ok; ++it) ok = mbar_try_wait(mb, 0u, 1);
+    if (!ok && err) atomicExch(err, (int)WF_ST_WAIT_TIMEOUT);
+  }
+  __syncthreads();
+}
+
+int wait_probe(unsigned* gbar, int* err, int kind, int tries, cudaStream_t s) {
+  if (!gbar || !err) return fail(WF_EINVAL, "wf_wait_probe: null gbar or err");
+  if (kind != 0 && kind != 1) return fail(WF_EINVAL, "wf_wait_probe: kind must be 0 or 1");
+  if (tries < 1 || tries > MBAR_WAIT_TRIES)
+    return fail(WF_EINVAL, "wf_wait_probe: tries must be 1 .. 2^22");
+  k_wait_probe<<<1, 32, 0, s>>>(gbar, err, kind, tries);
+  WF_CKL("k_wait_probe");
+  return WF_OK;
 }
 
 // max |rhs - A phi| over a level (tests/test_mg.py:16-32)
@@ -2429,29 +2469,90 @@ int mg_residual_max_pair(const wf_case& c, const double* phi0, const double* rhs
 // loads the library, for the life of the process; that is enough for n up
 // to 112 at 3 levels.  Larger problems are rejected with WF_EINVAL.
 // Host code cannot use the array's name as a device address, so the first
-// call on each device looks the address up once (with that device current)
-// and caches it; make that first call before any stream capture.  All
-// calls share the array and only the last call's contents remain: every
-// level is rewritten before it is read, and calls that overlap on the GPU
-// (two streams, or two host threads) race on it.
+// call in each CUDA context looks the address up (with that context
+// current) and caches it per context; make that first call before any
+// stream capture.  The cache is keyed on the context's unique id, so a
+// context created after cudaDeviceReset, or a host program's own driver
+// context, gets its own lookup.  All calls share the array and only the
+// last call's contents remain: every level is rewritten before it is read,
+// and calls that overlap on the GPU (two streams, or two host threads) race
+// on it.
+//
+// A device-side wait that gives up in a coarse-level kernel (a bounded
+// wait, see WF_ST_WAIT_TIMEOUT) is recorded in a status word that sits next
+// to the array; each call clears it first, and wf_mg_noalloc_status reads
+// it after the caller's stream has finished.
 // ---------------------------------------------------------------------------
 constexpr long MG_NOALLOC_DOUBLES = 1L << 19;
 static __device__ __align__(256) double g_mg_noalloc_scratch[MG_NOALLOC_DOUBLES];
+static __device__ int g_mg_noalloc_status;
 
-static int noalloc_scratch(double** out) {
+struct NoallocAddrs {
+  unsigned long long ctx_id;
+  double* scratch;
+  int* status;
+};
+
+// unique id of the calling thread's current CUDA context (0: none current);
+// the driver functions are looked up through the runtime, so the library
+// does not link libcuda and still loads on a machine without a GPU
+static int current_ctx_id(unsigned long long* id) {
+  typedef CUresult (*GetCur)(CUcontext*);
+  typedef CUresult (*GetId)(CUcontext, unsigned long long*);
+  static GetCur get_cur = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess && q == cudaDriverEntryPointSuccess)
+      get_cur = reinterpret_cast<GetCur>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess && q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetId>(f);
+  });
+  if (!get_cur || !get_id) return fail(WF_EUNSUPPORTED, "driver lacks cuCtxGetCurrent/cuCtxGetId");
+  CUcontext ctx = nullptr;
+  *id = 0;
+  if (get_cur(&ctx) != CUDA_SUCCESS) return fail(WF_ECUDA, "cuCtxGetCurrent failed");
+  if (ctx && get_id(ctx, id) != CUDA_SUCCESS) return fail(WF_ECUDA, "cuCtxGetId failed");
+  return WF_OK;
+}
+
+static int noalloc_addrs(NoallocAddrs* out) {
   static std::mutex mu;
-  static double* addr[64] = {};
-  int dev = -1;
-  WF_CK(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64) return fail(WF_EUNSUPPORTED, "device ordinal beyond 63");
+  static std::vector<NoallocAddrs> cache;
+  unsigned long long id = 0;
+  WF_TRY(current_ctx_id(&id));
   std::lock_guard<std::mutex> lock(mu);
-  if (!addr[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_mg_noalloc_scratch);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(multigrid scratch)");
-    addr[dev] = static_cast<double*>(p);
-  }
-  *out = addr[dev];
+  if (id)
+    for (const NoallocAddrs& a : cache)
+      if (a.ctx_id == id) {
+        *out = a;
+        return WF_OK;
+      }
+  NoallocAddrs a{};
+  void* p = nullptr;
+  // the first runtime call of a thread without a current context makes the
+  // device's primary context current; its id is read after the lookup
+  cudaError_t e = cudaGetSymbolAddress(&p, g_mg_noalloc_scratch);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(multigrid scratch)");
+  a.scratch = static_cast<double*>(p);
+  e = cudaGetSymbolAddress(&p, g_mg_noalloc_status);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(multigrid status)");
+  a.status = static_cast<int*>(p);
+  if (!id) WF_TRY(current_ctx_id(&id));
+  if (!id) return fail(WF_ECUDA, "no current CUDA context after the symbol lookup");
+  a.ctx_id = id;
+  for (const NoallocAddrs& b : cache)
+    if (b.ctx_id == id) {
+      *out = b;
+      return WF_OK;
+    }
+  cache.push_back(a);
+  *out = a;
   return WF_OK;
 }
 
@@ -2459,9 +2560,7 @@ static int noalloc_scratch(double** out) {
 static int vcycle_fixed(Lvl<double>* lv, int L, const wf_case& c, cudaStream_t s) {
   for (int l = 0; l < L; ++l) {
     if (l > 0) {
-      const long m = (long)lv[l].n + 2;
-      WF_CK(launch_k(k_zero<double>, mg_blocks(m * m * m), MG_TPB, 0, s, lv[l].phi, m * m * m));
-      WF_CKL("k_zero");
+      // k_restrict also zeroes the coarse phi, ring included
       WF_CK(launch_k(k_restrict<double>, cells3(lv[l].n, lv[l].n, lv[l].n), cell_block(), 0, s,
           lv[l - 1], const_cast<double*>(lv[l].rhs), lv[l]));
       WF_CKL("k_restrict");
@@ -2495,8 +2594,9 @@ int mg_solve_noalloc(const double* su, double* pp, int n, int nlev, double dx, d
                                " doubles of multigrid scratch; the static array holds " +
                                std::to_string(MG_NOALLOC_DOUBLES) +
                                " (n <= 112 at 3 levels); use wf_mg_solve with caller buffers");
-  double* base = nullptr;
-  WF_TRY(noalloc_scratch(&base));
+  NoallocAddrs ad{};
+  WF_TRY(noalloc_addrs(&ad));
+  double* base = ad.scratch;
   const long P = padded(n);
   const long off = (long)(NPL - 1) * (P * P + P + 1);
   Lvl<double> lv[WF_MAX_LEVELS];
@@ -2505,7 +2605,7 @@ int mg_solve_noalloc(const double* su, double* pp, int n, int nlev, double dx, d
     const double s2 = (double)(1 << l);
     const double dxl = dx * s2, dyl = dy * s2, dzl = dz * s2;
     Lvl<double>& L = lv[l];
-    L.err = nullptr;
+    L.err = ad.status;
     L.tmp = nullptr;
     L.gbar = nullptr;
     L.ax = 1.0 / (dxl * dxl);
@@ -2532,9 +2632,21 @@ int mg_solve_noalloc(const double* su, double* pp, int n, int nlev, double dx, d
   c.n_post = 6;
   c.n_coarse = 300;
   c.n_vcycles = 4;
+  WF_CK(cudaMemsetAsync(ad.status, 0, sizeof(int), s));
   WF_CK(launch_k(k_zero<double>, mg_blocks(P * P * P), MG_TPB, 0, s, pp, P * P * P));
   WF_CKL("k_zero pp");
   for (int cyc = 0; cyc < c.n_vcycles; ++cyc) WF_TRY(vcycle_fixed(lv, nlev, c, s));
+  return WF_OK;
+}
+
+int mg_noalloc_status(void* stream, int32_t* status) {
+  if (!status) return fail(WF_EINVAL, "wf_mg_noalloc_status: null status");
+  NoallocAddrs ad{};
+  WF_TRY(noalloc_addrs(&ad));
+  WF_CK(cudaStreamSynchronize((cudaStream_t)stream));
+  int v = 0;
+  WF_CK(cudaMemcpy(&v, ad.status, sizeof(int), cudaMemcpyDeviceToHost));
+  *status = v;
   return WF_OK;
 }
 

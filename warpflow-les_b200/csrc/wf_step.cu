@@ -338,6 +338,10 @@ int wf_mg_solve_noalloc(const double* su, double* pp, int32_t n, int32_t nlev, d
                         double dy, double dz, void* s) {
   return mg_solve_noalloc(su, pp, n, nlev, dx, dy, dz, (cudaStream_t)s);
 }
+int wf_mg_noalloc_status(void* s, int32_t* status) { return mg_noalloc_status(s, status); }
+int wf_wait_probe(uint32_t* gbar, int32_t* err, int32_t kind, int32_t tries, void* s) {
+  return wait_probe(gbar, err, kind, tries, (cudaStream_t)s);
+}
 int wf_mg_vcycle(const wf_case* c, double* phi0, const double* rhs0, void* s) {
   if (!c || !phi0 || !rhs0) return fail(WF_EINVAL, "null argument");
   return mg_vcycle_pair(*c, phi0, rhs0, (cudaStream_t)s);

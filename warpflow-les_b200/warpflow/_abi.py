@@ -107,6 +107,8 @@ SIGNATURES = {
     "wf_add_ring": (_I32, [_VP, _VP, _I32, _VP]),
     "wf_mg_solve": (_I32, [_CP, _VP]),
     "wf_mg_solve_noalloc": (_I32, [_VP, _VP, _I32, _I32, _D, _D, _D, _VP]),
+    "wf_mg_noalloc_status": (_I32, [_VP, ctypes.POINTER(_I32)]),
+    "wf_wait_probe": (_I32, [_VP, _VP, _I32, _I32, _VP]),
     "wf_mg_vcycle": (_I32, [_CP, _VP, _VP, _VP]),
     "wf_mg_relax": (_I32, [_CP, _VP, _VP, _I32, _VP]),
     "wf_mg_dc_cycle": (_I32, [_CP, _VP, _VP, _VP]),

@@ -247,7 +247,11 @@ class CavityServer:
 
     def _build_on_worker(self, req):
         torch.cuda.set_device(self.device)   # the worker thread's current device
-        return self._build(req)
+        sol = self._build(req)
+        # the set-up kernels ran on this thread's current stream; finish them
+        # here so that a step on any stream sees initialised fields
+        torch.cuda.current_stream(self.device).synchronize()
+        return sol
 
     def _step_batch(self, live, main, t0, time_scale):
         """One step of every live case, then their scalar blocks in one copy;
