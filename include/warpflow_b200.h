@@ -108,7 +108,7 @@ typedef struct wf_case {
   wf_scalars* sc;                 /* device scalar block */
   void* mg_cop;                   /* optional coarse-level operator (may be shared
                                      by cases), see wf_mg_build_coarse_op; NULL = sweeps */
-  void* mg_cop_part;              /* this case's partial-sum scratch for it */
+  void* mg_cop_part;              /* this case's scratch for it (N/2 elements) */
 } wf_case;
 
 /* ---- library ---------------------------------------------------------- */
@@ -127,22 +127,26 @@ WF_API int wf_set_coarse_strategy(int32_t n, int32_t fp32, int32_t strategy);
 WF_API int wf_mg_level_elems(int32_t n, int32_t nlev, int32_t level, int64_t* elems);
 /* No counterpart in the reference.  The coarsest-level relax of a V-cycle
  * (multigrid.py:301-322: n_coarse RBGS sweeps starting from phi = 0) is a
- * fixed linear map of the level's rhs.  wf_mg_build_coarse_op stores it, for
- * the case's n, nlev, spacing, n_coarse and precision (c->mg_fp32 selects
- * FP32), in c->mg_cop: every cell neighbours only cells of the other
- * parity of i+j+k, so after the first sweep from zero the even-parity half
- * of phi evolves on its own, and the dense map from that half after sweep 1
- * to it after n_coarse - 1 sweeps ((n_c^3/2)^2 elements) is stored; row u =
- * the even-parity half of phi after n_coarse - 1 sweeps from zero with
- * rhs = unit vector at the u-th even-parity cell.  With c->mg_cop set,
- * V-cycles run the relax as the first sweep's even-parity numerators, one
- * matrix-vector product (HBM-bound) and the last sweep, instead of the
- * latency-bound sweeps; the results agree to rounding.  Coarsest edges 4, 8,
- * 12, 16, 20, 24 and n_coarse >= 2 only (WF_EUNSUPPORTED / WF_EINVAL).  The operator is read-only once built and can
- * be shared by cases of the same size; each case needs its own partial-sum
- * scratch (c->mg_cop_part).  wf_mg_coarse_op_elems gives both element counts. */
-WF_API int wf_mg_coarse_op_elems(int32_t n, int32_t nlev, int64_t* op_elems,
-                                 int64_t* scratch_elems);
+ * fixed linear map of the level's rhs.  Every cell neighbours only cells of
+ * the other parity of i+j+k, so after the first sweep from zero the
+ * even-parity half of phi evolves on its own: after n_coarse - 1 sweeps it
+ * is S v, v = the even-parity numerators of the first sweep, S a fixed
+ * symmetric (N/2)^2 matrix (N = n_c^3) that commutes with the level's
+ * colour-preserving symmetries (axis permutations between axes of equal
+ * spacing, reflections of two axes: 24 on a cube).  wf_mg_build_coarse_op
+ * stores, for the case's n, nlev, spacing, n_coarse and precision
+ * (c->mg_fp32 selects FP32), in c->mg_cop the columns of S at one
+ * representative cell of every orbit of those symmetries (about N/48
+ * columns of N/2 entries on a cube) followed by an integer table.  With
+ * c->mg_cop set, V-cycles run the coarse relax as v, the product S v formed
+ * from the stored columns in shared memory, and the last sweep, instead of
+ * the latency-bound sweeps; the results agree to rounding.  Coarsest edges
+ * 4, 8, 12, 16, 20, 24 and n_coarse >= 2 only (WF_EUNSUPPORTED /
+ * WF_EINVAL).  The operator is read-only once built and can be shared by
+ * cases of the same size and spacing; each case needs its own scratch of
+ * N/2 elements (c->mg_cop_part).  wf_mg_coarse_op_elems gives both element
+ * counts (they depend on which spacings are equal). */
+WF_API int wf_mg_coarse_op_elems(const wf_case* c, int64_t* op_elems, int64_t* scratch_elems);
 WF_API int wf_mg_build_coarse_op(const wf_case* c, void* stream);
 /* The coarsest-level solve of a V-cycle (multigrid.py:301-322, coarsest
  * level: phi from zero, n_coarse sweeps) on an explicit FP64 pair of

@@ -1,5 +1,5 @@
-"""The coarsest-level relax applied as a precomputed operator against the
-same relax run as sweeps: multigrid solves agree to rounding at every
+"""The coarsest-level relax applied through its precomputed symmetric
+operator (representative columns) against the same relax run as sweeps: multigrid solves agree to rounding at every
 supported coarse size, both match the FP64 oracle, the FP32 operator serves
 the mixed form, applications are deterministic, and whole steps reproduce the
 sweeping solver."""
@@ -12,7 +12,7 @@ from oracle import wf_oracle as O
 pytestmark = pytest.mark.gpu
 
 
-def _solve(n, L, prec, coarse, seed=3):
+def _solve(n, L, prec, coarse, seed=3, hs=(1.0, 1.0, 1.0)):
     from warpflow import Multigrid, build_topology
     from warpflow.config import case_from_dict
     from warpflow.fields import DeviceField
@@ -20,7 +20,7 @@ def _solve(n, L, prec, coarse, seed=3):
                           "numerics": {"mg_levels": L, "mg_precision": prec,
                                        "mg_coarse": coarse}})
     h = 1.0 / n
-    mg = Multigrid(cfg, build_topology(cfg), "cuda:0", h, h, h)
+    mg = Multigrid(cfg, build_topology(cfg), "cuda:0", h * hs[0], h * hs[1], h * hs[2])
     shape = (n + 6,) * 3
     rhs = np.random.default_rng(seed).standard_normal(shape)
     su = DeviceField.zeros(shape, "cuda:0")
@@ -42,6 +42,16 @@ def test_operator_matches_sweeps_and_oracle(n):
         ref = np.zeros_like(rhs)
         O.Multigrid(n, 3, h, h, h).solve(rhs, ref, n)
         assert np.abs(a - ref).max() <= 1e-11 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("hs", [(1.0, 1.3, 1.0), (1.0, 1.3, 0.7)], ids=["two_equal", "none_equal"])
+def test_operator_with_unequal_spacing(hs):
+    """Fewer symmetries (8 or 4 maps instead of 24): more stored columns, the
+    same product."""
+    _, a, mg = _solve(80, 3, "fp64", "operator", hs=hs)
+    assert mg._cop_part is not None
+    _, b, _ = _solve(80, 3, "fp64", "sweeps", hs=hs)
+    assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
 
 
 def test_operator_mixed_precision():

@@ -50,13 +50,14 @@ def test_case_bytes_matches_allocation():
 
 
 def test_server_stream_matches_alone_and_budget():
-    from warpflow.serve import CavityServer, Request, case_bytes
+    from warpflow.serve import CavityServer, Request, case_bytes, operator_bytes
     reqs = [Request(0, 16, 300.0, 1.0, 6, arrival=0.00),
             Request(1, 32, 700.0, 0.7, 3, arrival=0.01),
             Request(2, 16, 900.0, 1.2, 5, arrival=0.02),
             Request(3, 24, 200.0, 1.0, 4, arrival=0.03),
             Request(4, 16, 500.0, 0.9, 2, arrival=0.50)]
-    budget = case_bytes(32) + case_bytes(16) + 4096   # forces queueing
+    # forces queueing; the shared coarse operators are charged once each
+    budget = case_bytes(32) + case_bytes(16) + operator_bytes(32) + operator_bytes(16) + 4096
     srv = CavityServer(budget_bytes=budget, nstreams=4, keep_fields=True)
     srv.warmup(reqs)          # start-up cases leave no trace in the served ones
     done = srv.run(reqs)

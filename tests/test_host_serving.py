@@ -34,31 +34,49 @@ def test_levels_for_keeps_coarse_small():
 
 
 def test_admission_fifo_budget():
-    from warpflow.serve import Admission, Request, case_bytes
-    b32 = case_bytes(32)
-    adm = Admission(budget_bytes=int(2.5 * b32))
+    from warpflow.serve import Admission, Request, case_bytes, operator_bytes
+    b32, op = case_bytes(32), operator_bytes(32)
+    adm = Admission(budget_bytes=int(2.5 * b32) + op)
     reqs = [Request(i, 32, 400.0, 1.0, 10, arrival=0.1 * i) for i in range(4)]
     for r in reqs:
         adm.submit(r)
     assert adm.admit(0.05) == [reqs[0]]
     got = adm.admit(1.0)
     assert got == [reqs[1]]              # third does not fit
-    assert adm.used == 2 * b32 <= adm.budget
+    assert adm.used == 2 * b32 + op <= adm.budget
     adm.release(0)
     assert adm.admit(1.0) == [reqs[2]]   # freed memory admits the next, in order
     assert adm.peak <= adm.budget
 
 
 def test_admission_no_overtaking():
-    from warpflow.serve import Admission, Request, case_bytes
+    from warpflow.serve import Admission, Request, case_bytes, operator_bytes
     big, small = case_bytes(128), case_bytes(32)
-    adm = Admission(budget_bytes=big + small // 2)
+    adm = Admission(budget_bytes=big + small // 2 + operator_bytes(128) + operator_bytes(32))
     adm.submit(Request(0, 32, 400.0, 1.0, 10, arrival=0.0))
     adm.submit(Request(1, 128, 400.0, 1.0, 10, arrival=0.1))
     adm.submit(Request(2, 32, 400.0, 1.0, 10, arrival=0.2))
     assert [r.rid for r in adm.admit(1.0)] == [0]   # 1 blocks 2 (FIFO)
     adm.release(0)
     assert [r.rid for r in adm.admit(1.0)] == [1]
+
+
+def test_operator_bytes_and_shared_charge():
+    """The shared coarse-level operator (220 representative columns of 4000
+    entries plus its integer table at 20^3) is charged once per kind."""
+    from warpflow.serve import Admission, Request, case_bytes, operator_bytes
+    op = operator_bytes(80, 3, "fp64")
+    assert op == 220 * 4000 * 8 + (220 + 4000) * 4
+    assert operator_bytes(72, 3, "fp64") == 0          # coarsest 18: sweeps
+    adm = Admission(budget_bytes=2 * case_bytes(80, 3, "fp64") + op)
+    for rid in range(3):
+        adm.submit(Request(rid, 80, 400.0, 1.0, 10, arrival=0.0, precision="fp64"))
+    got = [r.rid for r in adm.admit(1.0)]
+    assert got == [0, 1]
+    assert adm.used == 2 * case_bytes(80, 3, "fp64") + op
+    adm.release(0)
+    assert [r.rid for r in adm.admit(1.0)] == [2]
+    assert adm.used == 2 * case_bytes(80, 3, "fp64") + op   # still charged once
 
 
 def test_admission_rejects_oversize():
@@ -75,7 +93,10 @@ def test_case_bytes_formula():
     vol = 82 ** 3 + 42 ** 3 + 22 ** 3
     mg64 = 2 * 8 * vol + 2 * 8 * vol      # phi, rhs + two-array scratch
     mg32 = 2 * 4 * vol + 2 * 4 * vol
-    cop64, cop32 = 32 * 20 ** 3 * 8, 32 * 20 ** 3 * 4   # coarse-operator scratch
+    # coarse-operator scratch: 24 permuted copies of the 4000 even cells and
+    # 8 slices x 220 representatives x 24 symmetries of partial sums
+    sc = 24 * 4000 + 8 * 220 * 24
+    cop64, cop32 = sc * 8, sc * 4
     assert 0 <= case_bytes(n, 3, "fp64") - f - mg64 - cop64 < 4096
     assert 0 <= case_bytes(n, 3, "mixed") - f - 2 * 8 * vol - mg32 - cop32 < 4096
     # a coarsest edge without an operator (18) adds no scratch

@@ -9,6 +9,15 @@ namespace wf {
 // allowing its successor to begin launching, then waits until its
 // predecessor has completed and its memory is visible.  Without the launch
 // attribute both instructions are no-ops.
+//
+// The wait orders a kernel's global loads only if the compiler cannot move
+// them above it.  It is an asm statement with a memory clobber, but a load
+// through a __restrict__ pointer (or the read-only path, __ldg) may legally
+// be hoisted above such a statement -- the asm does not name the pointer --
+// and would then read data the predecessor is still writing (this happened
+// to a coarse-level kernel whose whole input load was provably in bounds).
+// So no kernel of this library marks a global-memory pointer __restrict__
+// or loads through __ldg; shared-memory pointers may be restrict.
 __device__ __forceinline__ void pdl_entry() {
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   asm volatile("griddepcontrol.wait;" ::: "memory");

@@ -98,7 +98,7 @@ int launch_scalars_init(wf_scalars* sc, double dt0, cudaStream_t s);
 
 // ---- multigrid -----------------------------------------------------------
 int mg_solve(const wf_case& c, cudaStream_t s);
-int coarse_op_elems(int n, int nlev, int64_t* op_elems, int64_t* scratch_elems);
+int coarse_op_elems(const wf_case& c, int64_t* op_elems, int64_t* scratch_elems);
 int build_coarse_op_case(const wf_case& c, cudaStream_t s);
 int mg_coarse_solve_pair(const wf_case& c, double* phi, const double* rhs, cudaStream_t s);
 int mg_vcycle_pair(const wf_case& c, double* phi0, const double* rhs0, cudaStream_t s);

@@ -416,7 +416,8 @@ struct CoarseShape {
 template <class T, int NC, bool RHS_SMEM>
 __global__ void __launch_bounds__(CoarseShape<NC>::THREADS) k_coarse_cols(Lvl<T> L,
                                                                            int nsweeps,
-                                                                           T* unit_out) {
+                                                                           T* unit_out,
+                                                                           const int* unit_ids) {
   pdl_entry();
   constexpr int H = NC / 2;
   constexpr int HALF = NC * H;                  // columns per parity
@@ -449,9 +450,10 @@ __global__ void __launch_bounds__(CoarseShape<NC>::THREADS) k_coarse_cols(Lvl<T>
   T ph[NC];
   T rh[RHS_SMEM ? 1 : NC];
   const long c0 = lid(L, i + 1, j + 1, 1);
-  // the unit cell of this CTA: the one of cells 2b, 2b+1 with even i+j+k
-  const int unit = 2 * (int)blockIdx.x + (((2 * (int)blockIdx.x / NC) / NC +
-                                           (2 * (int)blockIdx.x / NC) % NC) & 1);
+  // the unit cell of this CTA: the one of cells 2b, 2b+1 with even i+j+k,
+  // b = unit_ids[blockIdx.x] (or blockIdx.x)
+  const int ub = unit_ids ? unit_ids[blockIdx.x] : (int)blockIdx.x;
+  const int unit = 2 * ub + (((2 * ub / NC) / NC + (2 * ub / NC) % NC) & 1);
 #pragma unroll
   for (int k = 0; k < NC; ++k) {
     T r;
@@ -503,14 +505,16 @@ __global__ void __launch_bounds__(CoarseShape<NC>::THREADS) k_coarse_cols(Lvl<T>
 }
 
 template <class T, int NC, bool RHS_SMEM>
-static int launch_coarse(const Lvl<T>& L, int nsweeps, cudaStream_t s, T* unit_out = nullptr) {
+static int launch_coarse(const Lvl<T>& L, int nsweeps, cudaStream_t s, T* unit_out = nullptr,
+                         const int* unit_ids = nullptr, int nunits = 0) {
   constexpr int HALF = NC * (NC / 2);
   constexpr int GROUP = ((HALF + 31) / 32) * 32;
   const size_t sb = (size_t)NC * NC * NC * sizeof(T) * (RHS_SMEM ? 2 : 1);
   WF_CK(cudaFuncSetAttribute(k_coarse_cols<T, NC, RHS_SMEM>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb));
-  const int nb = unit_out ? NC * NC * NC / 2 : 1;
-  WF_CK(launch_k(k_coarse_cols<T, NC, RHS_SMEM>, nb, 2 * GROUP, sb, s, L, nsweeps, unit_out));
+  const int nb = unit_out ? (unit_ids ? nunits : NC * NC * NC / 2) : 1;
+  WF_CK(launch_k(k_coarse_cols<T, NC, RHS_SMEM>, nb, 2 * GROUP, sb, s, L, nsweeps, unit_out,
+                 unit_ids));
   WF_CKL("k_coarse_cols");
   return WF_OK;
 }
@@ -1189,28 +1193,140 @@ static int try_coarse_tb(const Lvl<T>& L, int nsweeps, cudaStream_t s, int* rc) 
 // even i+j+k; every neighbour of a cell has the other colour.  From phi = 0
 // the first sweep gives x_A = b_A / ap and then x_B = v_B / ap with
 // v_B = b_B - sum_nb a_nb x_A(nb); every later sweep maps x_B linearly
-// (x_B <- x_B1 + G x_B).  So after m = n_coarse - 1 sweeps x_B = S v_B with
-// S fixed by the level (row u of S = the B part of m sweeps from zero with
-// rhs = e_u, built by k_coarse_cols in unit mode), and the n_coarse-th sweep
-// is run as such from that x_B.  Applying the relax therefore reads S once
-// ((N/2)^2 elements, N = n^3, a quarter of the full map's) in an HBM-bound
-// product instead of 2*n_coarse dependent half-sweeps.  The sum is split over
-// row chunks with partial sums in fixed order (chunk partials, then the
-// chunks in a fixed tree), so results do not depend on scheduling: a case
-// computes the same bits alone or beside other cases.  The chunk count is a
-// function of the size only (cop_chunks), at most COP_CH.
-constexpr int COP_CH = 64;
-// CTAs of k_cop_partial resident at once on a B200 (148 SMs x 3 CTAs of 256
-// threads at its register count): the chunk count fills one wave
-constexpr int COP_SLOTS = 148 * 3;
+// (x_B <- x_B1 + G x_B, G = D_B^-1 A_BA D_A^-1 A_AB).  So after
+// m = n_coarse - 1 sweeps x_B = S v_B with S = sum_{s<m} G^s D_B^-1, and the
+// n_coarse-th sweep is run as such from that x_B.
+//
+// S is symmetric (D_B G is, because A is), and it commutes with every map
+// of the level's cells onto themselves that keeps the colour of each cell
+// and the operator: the permutations of axes of equal coefficient combined
+// with reflections of an even number of axes (n is even, so one reflection
+// swaps the colours) -- 24 maps on a cube of equal spacings.  So S is fixed
+// by its columns at one representative B cell r of every orbit of these
+// maps, and for an output o = g(r):  x_B[o] = sum_u S[u, r] v_B[g(u)]
+// (S[g r, w] = S[r, g^-1 w] = S[g^-1 w, r]).  Only the representative
+// columns are stored (about N/48 of the (N/2)^2 entries of S, N = n^3:
+// 5.8 MB instead of 128 MB at 20^3), built like the full map was (one CTA
+// of the column kernel per representative, unit rhs), and the product runs
+// from shared memory: one CTA per representative holds v_B and its column
+// and forms the outputs of its orbit, each a dot product summed in a fixed
+// order (per thread over its cells, a warp butterfly, the warps in order),
+// so results do not depend on scheduling and a case computes the same bits
+// alone or beside other cases.  The stored columns equal the mathematical
+// S to rounding, so the relax agrees with the sweeps to rounding.
+constexpr int COP_GMAX = 24;
 
 static bool cop_size_ok(int nc) {
   return nc == 4 || nc == 8 || nc == 12 || nc == 16 || nc == 20 || nc == 24;
 }
 
-template <class T> struct Vec2;
-template <> struct Vec2<double> { using type = double2; };
-template <> struct Vec2<float> { using type = float2; };
+static bool cop_full(int nc, bool fp32) { return fp32 && nc <= 4; }
+
+// one colour-preserving symmetry of an n^3 level: c'_d = sgn_d * c[src_d] + off_d,
+// and its inverse (same form) in isrc/isgn/ioff
+struct CopSyms {
+  int ng;
+  int src[COP_GMAX][3], sgn[COP_GMAX][3], off[COP_GMAX][3];
+  int isrc[COP_GMAX][3], isgn[COP_GMAX][3], ioff[COP_GMAX][3];
+};
+
+// the orbit structure of the B cells of an n^3 level under the symmetries
+// its coefficients allow: the representatives, and for every B cell o the
+// (representative, symmetry) pair that produces it (o = g(r), every o once)
+struct CopPlan {
+  int n = 0, M = 0, nrep = 0;
+  int eq = 0;              // which coefficients are equal (bits: xy, xz, yz; 8 = full)
+  CopSyms G{};
+  std::vector<int> ints;   // nrep representative B indices, then for each B cell o
+                           // (representative index << 5) | symmetry
+  template <class T>
+  int64_t op_elems() const {
+    return (int64_t)nrep * M + ((int64_t)ints.size() * 4 + sizeof(T) - 1) / sizeof(T);
+  }
+};
+
+constexpr int COP_RB = 4;   // representatives per CTA of k_cop_gemm
+constexpr int COP_KS = 8;   // slices of the B cells (the product's sum) per output
+
+// per-case scratch of the operator product: the permuted copies of v_B
+// (COP_GMAX x M) and the slice partials (COP_KS x nrep x COP_GMAX)
+static int64_t cop_scratch_elems(const CopPlan& P) {
+  return (int64_t)COP_GMAX * P.M + (int64_t)COP_KS * P.nrep * COP_GMAX;
+}
+
+static void b_cell_host(int b, int n, int& i, int& j, int& k) {
+  const int rw = 2 * b / n;
+  i = rw / n;
+  j = rw - i * n;
+  k = 2 * b - rw * n + ((i + j) & 1);
+}
+
+// full: the identity map only (every column stored).  An FP32 operator of a
+// 4^3 level is kept full: after hundreds of sweeps its map is nearly the
+// rank-one projection on the constant mode of the Neumann problem, so the
+// product is a large cancellation, and columns that equal the wanted
+// entries only to FP32 rounding would not cancel (2e-1 relative error,
+// against 1e-7 from 8^3 up and 1e-14 in FP64 at 4^3).
+static const CopPlan& cop_plan(int n, double ax, double ay, double az, bool full) {
+  static std::mutex mu;
+  static std::vector<CopPlan*> plans;
+  const double a[3] = {ax, ay, az};
+  const int eq = full ? 8 : (a[0] == a[1]) | ((a[0] == a[2]) << 1) | ((a[1] == a[2]) << 2);
+  std::lock_guard<std::mutex> lock(mu);
+  for (CopPlan* p : plans)
+    if (p->n == n && p->eq == eq) return *p;
+  CopPlan* P = new CopPlan();
+  P->n = n;
+  P->M = n * n * n / 2;
+  P->eq = eq;
+  static const int perms[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+  static const int masks[4] = {0, 3, 5, 6};
+  int ng = 0;
+  for (const auto& pm : perms) {
+    if (a[pm[0]] != a[0] || a[pm[1]] != a[1] || a[pm[2]] != a[2]) continue;
+    if (full && (pm[0] != 0 || pm[1] != 1)) continue;
+    for (int mk : masks) {
+      if (full && mk != 0) continue;
+      for (int d = 0; d < 3; ++d) {
+        const int sg = (mk >> d) & 1 ? -1 : 1, of = (mk >> d) & 1 ? n - 1 : 0;
+        P->G.src[ng][d] = pm[d];
+        P->G.sgn[ng][d] = sg;
+        P->G.off[ng][d] = of;
+        // inverse: c[src_d] = sg * c'_d - sg * off
+        P->G.isrc[ng][pm[d]] = d;
+        P->G.isgn[ng][pm[d]] = sg;
+        P->G.ioff[ng][pm[d]] = -sg * of;
+      }
+      ++ng;
+    }
+  }
+  P->G.ng = ng;
+  const int M = P->M;
+  auto image = [&](int g, int b) {
+    int c[3];
+    b_cell_host(b, n, c[0], c[1], c[2]);
+    int q[3];
+    for (int d = 0; d < 3; ++d) q[d] = P->G.sgn[g][d] * c[P->G.src[g][d]] + P->G.off[g][d];
+    return ((q[0] * n + q[1]) * n + q[2]) >> 1;
+  };
+  std::vector<int> reps;
+  for (int b = 0; b < M; ++b) {
+    int r = b;
+    for (int g = 0; g < ng; ++g) r = std::min(r, image(g, b));
+    if (r == b) reps.push_back(b);
+  }
+  P->nrep = (int)reps.size();
+  P->ints.assign((size_t)P->nrep + M, -1);
+  for (int x = 0; x < P->nrep; ++x) {
+    P->ints[x] = reps[x];
+    for (int g = 0; g < ng; ++g) {
+      const int o = image(g, reps[x]);
+      if (P->ints[P->nrep + o] < 0) P->ints[P->nrep + o] = (x << 5) | g;
+    }
+  }
+  plans.push_back(P);
+  return *P;
+}
 
 // (i, j, k) of the B cell at position b of the B-only order (n even: cells
 // 2b and 2b+1 share i and j, and exactly one of them has even i+j+k)
@@ -1242,107 +1358,160 @@ __device__ __forceinline__ T first_sweep_v(const Lvl<T>& L, int i, int j, int k)
   return L.rhs[lid(L, i + 1, j + 1, k + 1)] - (W + E + S + N + B + U);
 }
 
-// chunks of the operator rows for M = N/2 outputs: as many as fill one wave
-// of k_cop_partial, at least enough that a chunk fits its 256-entry v_B
-// buffer, at most COP_CH
-static int cop_chunks(int M) {
-  const int gx = (M + 511) / 512;
-  return std::min(COP_CH, std::max((M + 255) / 256, COP_SLOTS / gx));
-}
-
-// grid (ceil(M/512), nch), M = N/2: a CTA forms v_B of its row chunk in
-// shared memory, then a thread owns outputs o, o+1 (one 2-vector load per
-// operator row) and runs 8 rows at a time, each row with its own pair of
-// accumulators, so 8 vector loads are in flight per thread
+// v_B of B cell w, stored into every permuted copy that holds it:
+// V[g][u] = v_B[g(u)], so V[g][g^-1(w)] = v_B[w].  Eight threads per cell:
+// thread t < 6 forms the t-th neighbour term of first_sweep_v (W, E, S, N,
+// B, U: one division each), thread 0 adds them in that order, and the eight
+// threads then store the copies (g = t, t+8, t+16)
 template <class T>
-__global__ void __launch_bounds__(256) k_cop_partial(const T* __restrict__ op, const Lvl<T> L,
-                                                     T* __restrict__ part) {
+__global__ void __launch_bounds__(256) k_cop_vg(const Lvl<T> L, T* V,
+                                                const __grid_constant__ CopSyms G) {
   pdl_entry();
-  using V = typename Vec2<T>::type;
-  constexpr int U = 8;
-  __shared__ T rs[256];
   const int n = L.n, M = n * n * n / 2;
-  const int jc = (M + gridDim.y - 1) / gridDim.y;
-  const int j0 = blockIdx.y * jc, j1 = min(M, j0 + jc);
-  for (int t = threadIdx.x; t < j1 - j0; t += 256) {
-    int a, bq, cq;
-    b_cell(j0 + t, n, a, bq, cq);
-    rs[t] = first_sweep_v(L, a, bq, cq);
-  }
-  __syncthreads();
-  const int o = 2 * (blockIdx.x * 256 + threadIdx.x);
-  if (o >= M) return;   // M is even: o+1 < M as well
-  const V* col = reinterpret_cast<const V*>(op + (long)j0 * M + o);
-  const long rowv = M / 2;   // one operator row in 2-vectors
-  T ax[U], ay[U];
-#pragma unroll
-  for (int u = 0; u < U; ++u) ax[u] = ay[u] = T(0);
-  const int cnt = j1 - j0;
-  int t = 0;
-  for (; t + U <= cnt; t += U) {
-    V v[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) v[u] = __ldg(col + (long)(t + u) * rowv);
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      ax[u] = fma(rs[t + u], v[u].x, ax[u]);
-      ay[u] = fma(rs[t + u], v[u].y, ay[u]);
+  const int t = threadIdx.x & 7;
+  const int w = blockIdx.x * 32 + (threadIdx.x >> 3);
+  const bool on = w < M;
+  int c[3] = {0, 0, 0};
+  if (on) b_cell(w, n, c[0], c[1], c[2]);
+  const int i = c[0], j = c[1], k = c[2];
+  // the neighbour of this thread's term and the coefficient towards it
+  T term = T(0);
+  if (on && t < 6) {
+    const int a = i + (t == 0 ? -1 : t == 1 ? 1 : 0);
+    const int bq = j + (t == 2 ? -1 : t == 3 ? 1 : 0);
+    const int cq = k + (t == 4 ? -1 : t == 5 ? 1 : 0);
+    const T coef = t < 2 ? L.ax : (t < 4 ? L.ay : L.az);
+    if (a >= 0 && a < n && bq >= 0 && bq < n && cq >= 0 && cq < n) {
+      const T aw = a > 0 ? L.ax : T(0), ae = a < n - 1 ? L.ax : T(0);
+      const T as = bq > 0 ? L.ay : T(0), an = bq < n - 1 ? L.ay : T(0);
+      const T ab = cq > 0 ? L.az : T(0), at = cq < n - 1 ? L.az : T(0);
+      term = coef * (L.rhs[lid(L, a + 1, bq + 1, cq + 1)] / (-(aw + ae + as + an + ab + at)));
     }
   }
-  for (; t < cnt; ++t) {
-    const V v = __ldg(col + (long)t * rowv);
-    ax[0] = fma(rs[t], v.x, ax[0]);
-    ay[0] = fma(rs[t], v.y, ay[0]);
-  }
-  T sx = T(0), sy = T(0);
+  T nb[6];
 #pragma unroll
-  for (int u = 0; u < U; ++u) {   // fixed order
-    sx += ax[u];
-    sy += ay[u];
+  for (int q = 0; q < 6; ++q) nb[q] = __shfl_sync(0xffffffffu, term, (threadIdx.x & 24) | q);
+  T x = T(0);
+  if (on) x = L.rhs[lid(L, i + 1, j + 1, k + 1)] - (nb[0] + nb[1] + nb[2] + nb[3] + nb[4] + nb[5]);
+  if (!on) return;
+  for (int g = t; g < G.ng; g += 8) {
+    int q[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int sd = G.isrc[g][d];
+      q[d] = G.isgn[g][d] * (sd == 0 ? i : (sd == 1 ? j : k)) + G.ioff[g][d];
+    }
+    V[(long)g * M + (((q[0] * n + q[1]) * n + q[2]) >> 1)] = x;
   }
-  part[(long)blockIdx.y * M + o] = sx;
-  part[(long)blockIdx.y * M + o + 1] = sy;
 }
 
-// x_B = the sum of the nch chunk partials: warp w of the CTA sums chunks
-// w, w+8, ... in ascending order for 32 outputs, then the 8 warp sums are
-// added in ascending order.  The A cell beside each B cell is zeroed (the
-// closing sweep overwrites it before reading it).
+template <class T> struct Vec2;
+template <> struct Vec2<double> { using type = double2; };
+template <> struct Vec2<float> { using type = float2; };
+
+// Y_s[x][g] = sum over the s-th slice of B cells u of C[x][u] * V[g][u]:
+// a CTA takes COP_RB representatives x and one slice; warp w the symmetries
+// 3w .. 3w+2; lanes step through the slice two cells at a time (2-vector
+// loads, two steps in flight), each summing its cells in ascending order,
+// then the lanes are added by a butterfly (fixed order)
 template <class T>
-__global__ void __launch_bounds__(256) k_cop_finish(const T* __restrict__ part, Lvl<T> L,
-                                                    int nch) {
+__global__ void __launch_bounds__(256) k_cop_gemm(const T* C, const T* V, T* Y, int nrep,
+                                                  int M, int ng) {
   pdl_entry();
-  __shared__ T ws[8][32];
-  const int n = L.n, M = n * n * n / 2;
+  using V2 = typename Vec2<T>::type;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int t = blockIdx.x * 32 + lane;
-  T x = T(0);
-  if (t < M)
-    for (int ch = w; ch < nch; ch += 8) x += part[(long)ch * M + t];
-  ws[w][lane] = x;
-  __syncthreads();
-  if (w != 0 || t >= M) return;
-  x = ws[0][lane];
+  const int x0 = blockIdx.x * COP_RB, s = blockIdx.y;
+  const int per = (((M + COP_KS - 1) / COP_KS) + 1) & ~1;   // even: 2-vector aligned
+  const int h0 = s * per / 2, h1 = min(M, s * per + per) / 2;   // 2-vector range
+  const int g0 = 3 * w;
+  T acc[COP_RB][3];
 #pragma unroll
-  for (int q = 1; q < 8; ++q) x += ws[q][lane];
+  for (int r = 0; r < COP_RB; ++r)
+#pragma unroll
+    for (int q = 0; q < 3; ++q) acc[r][q] = T(0);
+  if (g0 < ng) {
+    const V2* cr[COP_RB];
+#pragma unroll
+    for (int r = 0; r < COP_RB; ++r)
+      cr[r] = reinterpret_cast<const V2*>(C + (long)min(x0 + r, nrep - 1) * M);
+    const V2* vg[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) vg[q] = reinterpret_cast<const V2*>(V + (long)min(g0 + q, ng - 1) * M);
+#pragma unroll 2
+    for (int h = h0 + lane; h < h1; h += 32) {
+      V2 c[COP_RB], v[3];
+#pragma unroll
+      for (int r = 0; r < COP_RB; ++r) c[r] = cr[r][h];
+#pragma unroll
+      for (int q = 0; q < 3; ++q) v[q] = vg[q][h];
+#pragma unroll
+      for (int r = 0; r < COP_RB; ++r)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          acc[r][q] = fma(c[r].x, v[q].x, acc[r][q]);
+          acc[r][q] = fma(c[r].y, v[q].y, acc[r][q]);
+        }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < COP_RB; ++r)
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      T y = acc[r][q];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
+      acc[r][q] = y;
+    }
+  if (lane == 0 && g0 < ng) {
+#pragma unroll
+    for (int r = 0; r < COP_RB; ++r)
+#pragma unroll
+      for (int q = 0; q < 3; ++q)
+        if (x0 + r < nrep && g0 + q < ng)
+          Y[((long)s * nrep + x0 + r) * COP_GMAX + g0 + q] = acc[r][q];
+  }
+}
+
+// x_B[o] = the slices of Y[x][g] added in ascending order, (x, g) the pair
+// producing o; written into phi, and the A cell beside o zeroed (the
+// closing sweep overwrites it first)
+template <class T>
+__global__ void __launch_bounds__(256) k_cop_out(const T* Y, const int* prod, int nrep,
+                                                 Lvl<T> L) {
+  pdl_entry();
+  const int n = L.n, M = n * n * n / 2;
+  const int o = blockIdx.x * 256 + threadIdx.x;
+  if (o >= M) return;
+  const int pv = prod[o];
+  const long at = (long)(pv >> 5) * COP_GMAX + (pv & 31);
+  T y = Y[at];
+#pragma unroll
+  for (int s = 1; s < COP_KS; ++s) y += Y[(long)s * nrep * COP_GMAX + at];
   int i, j, k;
-  b_cell(t, n, i, j, k);
-  L.phi[lid(L, i + 1, j + 1, k + 1)] = x;
+  b_cell(o, n, i, j, k);
+  L.phi[lid(L, i + 1, j + 1, k + 1)] = y;
   L.phi[lid(L, i + 1, j + 1, (k ^ 1) + 1)] = T(0);
 }
 
 // phi of the coarsest level = the n_coarse-sweep relax of rhs from zero (the
-// level's phi is overwritten): the operator product for the B cells after
-// n_coarse - 1 sweeps, then the last sweep (k_rbgs, colour A then B, which
-// also writes the face-ring mirrors); part: this case's COP_CH x N/2 scratch
+// level's phi is overwritten): v_B and its permuted copies, the product of
+// the representative columns with them, the B cells from their producing
+// pairs, then the last sweep (k_rbgs, colour A then B, which also writes the
+// face-ring mirrors); part: this case's scratch (cop_scratch_elems)
 template <class T>
 static int apply_coarse_op(const Lvl<T>& L, const T* op, T* part, cudaStream_t s) {
-  const int M = L.n * L.n * L.n / 2;
-  const int nch = cop_chunks(M);
-  WF_CK(launch_k(k_cop_partial<T>, dim3((M + 511) / 512, nch), 256, 0, s, op, L, part));
-  WF_CKL("k_cop_partial");
-  WF_CK(launch_k(k_cop_finish<T>, (M + 31) / 32, 256, 0, s, (const T*)part, L, nch));
-  WF_CKL("k_cop_finish");
+  const CopPlan& P =
+      cop_plan(L.n, (double)L.ax, (double)L.ay, (double)L.az, cop_full(L.n, sizeof(T) == 4));
+  T* V = part;
+  T* Y = part + (long)COP_GMAX * P.M;
+  const int* prod = reinterpret_cast<const int*>(op + (long)P.nrep * P.M) + P.nrep;
+  WF_CK(launch_k(k_cop_vg<T>, (P.M + 31) / 32, 256, 0, s, L, V, P.G));
+  WF_CKL("k_cop_vg");
+  WF_CK(launch_k(k_cop_gemm<T>, dim3((P.nrep + COP_RB - 1) / COP_RB, COP_KS), 256, 0, s, op,
+                 (const T*)V, Y, P.nrep, P.M, P.G.ng));
+  WF_CKL("k_cop_gemm");
+  WF_CK(launch_k(k_cop_out<T>, (P.M + 255) / 256, 256, 0, s, (const T*)Y, prod, P.nrep, L));
+  WF_CKL("k_cop_out");
   for (int color = 0; color < 2; ++color) {
     WF_CK(launch_k(k_rbgs<T>, cells3(L.n, L.n, (L.n + 1) / 2), cell_block(), 0, s, L, color));
     WF_CKL("k_rbgs");
@@ -1350,19 +1519,28 @@ static int apply_coarse_op(const Lvl<T>& L, const T* op, T* part, cudaStream_t s
   return WF_OK;
 }
 
-// the operator rows: n_coarse - 1 sweeps from zero per unit B cell
+// the representative columns: n_coarse - 1 sweeps from zero per unit
+// representative B cell; the plan's integers go after them
 template <class T>
 static int build_coarse_op(const Lvl<T>& L, int n_coarse, T* op, cudaStream_t s) {
   if (n_coarse < 2) return fail(WF_EINVAL, "coarse operator needs n_coarse >= 2");
+  if (!cop_size_ok(L.n))
+    return fail(WF_EUNSUPPORTED, "coarse operator: coarsest edge must be 4..24, step 4");
+  const CopPlan& P =
+      cop_plan(L.n, (double)L.ax, (double)L.ay, (double)L.az, cop_full(L.n, sizeof(T) == 4));
+  int* ints = reinterpret_cast<int*>(op + (long)P.nrep * P.M);
+  WF_CK(cudaMemcpyAsync(ints, P.ints.data(), P.ints.size() * sizeof(int),
+                        cudaMemcpyHostToDevice, s));
+  // the copy reads host memory that outlives it (the plan is kept for the
+  // process), so it may stay asynchronous
   const int nsweeps = n_coarse - 1;
   switch (L.n) {
-    case 4: return launch_coarse<T, 4, false>(L, nsweeps, s, op);
-    case 8: return launch_coarse<T, 8, false>(L, nsweeps, s, op);
-    case 12: return launch_coarse<T, 12, false>(L, nsweeps, s, op);
-    case 16: return launch_coarse<T, 16, false>(L, nsweeps, s, op);
-    case 20: return launch_coarse<T, 20, false>(L, nsweeps, s, op);
-    case 24: return launch_coarse<T, 24, true>(L, nsweeps, s, op);
-    default: return fail(WF_EUNSUPPORTED, "coarse operator: coarsest edge must be 4..24, step 4");
+    case 4: return launch_coarse<T, 4, false>(L, nsweeps, s, op, ints, P.nrep);
+    case 8: return launch_coarse<T, 8, false>(L, nsweeps, s, op, ints, P.nrep);
+    case 12: return launch_coarse<T, 12, false>(L, nsweeps, s, op, ints, P.nrep);
+    case 16: return launch_coarse<T, 16, false>(L, nsweeps, s, op, ints, P.nrep);
+    case 20: return launch_coarse<T, 20, false>(L, nsweeps, s, op, ints, P.nrep);
+    default: return launch_coarse<T, 24, true>(L, nsweeps, s, op, ints, P.nrep);
   }
 }
 
@@ -1436,7 +1614,7 @@ constexpr int SPLIT_ROWS = 8;  // rows (one warp each) per CTA
 // level phi (all (n+2)^3 cells) and rhs -> split copies sp, sr (dense strides)
 template <class T>
 __global__ void __launch_bounds__(32 * SPLIT_ROWS)
-    k_split_in(const Lvl<T> L, T* __restrict__ sp, T* __restrict__ sr, int with_rhs) {
+    k_split_in(const Lvl<T> L, T* sp, T* sr, int with_rhs) {
   pdl_entry();
   const int m = L.n + 2, H = m >> 1;
   const int row = blockIdx.x * SPLIT_ROWS + (threadIdx.x >> 5);
@@ -1458,7 +1636,7 @@ __global__ void __launch_bounds__(32 * SPLIT_ROWS)
 // reads only the other colour and rhs, which it does not write.
 template <class T, int CPT>
 __global__ void __launch_bounds__(32 * SPLIT_ROWS)
-    k_rbgs_split(const Lvl<T> L, T* __restrict__ sp, const T* __restrict__ sr, int color,
+    k_rbgs_split(const Lvl<T> L, T* sp, const T* sr, int color,
                  const __grid_constant__ ApRecip<T> rt) {
   pdl_entry();
   const int n = L.n, nh = n >> 1;
@@ -1514,7 +1692,7 @@ static int split_cpt() {
 // split copy -> real cells of the level and their face-ring mirrors
 template <class T>
 __global__ void __launch_bounds__(32 * SPLIT_ROWS)
-    k_split_out(const Lvl<T> L, const T* __restrict__ sp) {
+    k_split_out(const Lvl<T> L, const T* sp) {
   pdl_entry();
   const int n = L.n, H = (n + 2) >> 1;
   const int row = blockIdx.x * SPLIT_ROWS + (threadIdx.x >> 5);
@@ -1664,8 +1842,8 @@ struct SweepTile {
 // is a contiguous run, free of bank conflicts.
 template <class T, int TJ, int TK>
 __global__ void __launch_bounds__(SweepTile<TJ, TK>::THREADS)
-    k_sweep2(const T* __restrict__ src, long sIs, long sJs, T* __restrict__ dst, long sId,
-             long sJd, const T* __restrict__ rhs, long sIr, long sJr, int n, T ax, T ay,
+    k_sweep2(const T* src, long sIs, long sJs, T* dst, long sId,
+             long sJd, const T* rhs, long sIr, long sJr, int n, T ax, T ay,
              T az, int seg, int write_ring) {
   pdl_entry();
   using W = SweepTile<TJ, TK>;
@@ -2230,7 +2408,7 @@ __global__ void __launch_bounds__(MG_TPB) k_defect(const Lvl<double> F, float* r
     phi_f[t] = 0.0f;
 }
 
-__global__ void k_correct(const Lvl<double> F, const float* __restrict__ phi_f, int n) {
+__global__ void k_correct(const Lvl<double> F, const float* phi_f, int n) {
   pdl_entry();
   const long m = (long)n + 2;
   const long tot = m * m * m;
@@ -2305,37 +2483,53 @@ int mg_dc_cycle_pair(const wf_case& c, double* phi0, const double* rhs0, cudaStr
   return dc_cycle(level0_view(c, phi0, rhs0, m * m, m), lvf, c, s);
 }
 
-int coarse_op_elems(int n, int nlev, int64_t* op_elems, int64_t* scratch_elems) {
+// the coarsest level's coefficients 1/h^2 of case c, in the level's precision
+static void coarse_coeffs(const wf_case& c, double a[3]) {
+  const int l = c.nlev - 1;
+  const double s2 = (double)(1 << l);
+  const double dxl = c.dx * s2, dyl = c.dy * s2, dzl = c.dz * s2;
+  a[0] = 1.0 / (dxl * dxl);
+  a[1] = 1.0 / (dyl * dyl);
+  a[2] = 1.0 / (dzl * dzl);
+  if (c.mg_fp32)
+    for (int d = 0; d < 3; ++d) a[d] = (double)(float)a[d];
+}
+
+int coarse_op_elems(const wf_case& c, int64_t* op_elems, int64_t* scratch_elems) {
+  const int n = c.n, nlev = c.nlev;
   if (nlev < 2 || nlev > WF_MAX_LEVELS || n < 1) return fail(WF_EINVAL, "bad n or nlev");
   const int nc = n >> (nlev - 1);
   if ((nc << (nlev - 1)) != n) return fail(WF_EINVAL, "n must be divisible by 2^(nlev-1)");
   if (!cop_size_ok(nc))
     return fail(WF_EUNSUPPORTED, "coarse operator: coarsest edge must be 4..24, step 4");
-  const int64_t N = (int64_t)nc * nc * nc;
-  if (op_elems) *op_elems = (N / 2) * (N / 2);
-  if (scratch_elems) *scratch_elems = (int64_t)COP_CH * (N / 2);
+  if (!(c.dx > 0 && c.dy > 0 && c.dz > 0)) return fail(WF_EINVAL, "cell sizes must be > 0");
+  double a[3];
+  coarse_coeffs(c, a);
+  const CopPlan& P = cop_plan(nc, a[0], a[1], a[2], cop_full(nc, c.mg_fp32 != 0));
+  if (op_elems) *op_elems = c.mg_fp32 ? P.op_elems<float>() : P.op_elems<double>();
+  if (scratch_elems) *scratch_elems = cop_scratch_elems(P);
   return WF_OK;
 }
 
 int build_coarse_op_case(const wf_case& c, cudaStream_t s) {
   if (!c.mg_cop) return fail(WF_EINVAL, "mg_cop is null");
-  WF_TRY(coarse_op_elems(c.n, c.nlev, nullptr, nullptr));
+  WF_TRY(coarse_op_elems(c, nullptr, nullptr));
   const int l = c.nlev - 1;
-  const double s2 = (double)(1 << l);
-  const double dxl = c.dx * s2, dyl = c.dy * s2, dzl = c.dz * s2;
+  double a[3];
+  coarse_coeffs(c, a);
   if (c.mg_fp32) {
     Lvl<float> L = {};
     L.n = c.n >> l;
-    L.ax = (float)(1.0 / (dxl * dxl));
-    L.ay = (float)(1.0 / (dyl * dyl));
-    L.az = (float)(1.0 / (dzl * dzl));
+    L.ax = (float)a[0];
+    L.ay = (float)a[1];
+    L.az = (float)a[2];
     return build_coarse_op<float>(L, c.n_coarse, (float*)c.mg_cop, s);
   }
   Lvl<double> L = {};
   L.n = c.n >> l;
-  L.ax = 1.0 / (dxl * dxl);
-  L.ay = 1.0 / (dyl * dyl);
-  L.az = 1.0 / (dzl * dzl);
+  L.ax = a[0];
+  L.ay = a[1];
+  L.az = a[2];
   return build_coarse_op<double>(L, c.n_coarse, (double*)c.mg_cop, s);
 }
 

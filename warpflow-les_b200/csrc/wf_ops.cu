@@ -73,7 +73,7 @@ static inline int nblocks(long work, int tpb = TPB, int cap = 148 * 16) {
   return (int)b;
 }
 
-#define LD(p, idx) __ldg((p) + (idx))
+#define LD(p, idx) ((p)[(idx)])
 
 // --------------------------------------------------------------------------
 // scalar block
@@ -228,16 +228,16 @@ int launch_checkdt(const wf_case& c, cudaStream_t s) {
 // --------------------------------------------------------------------------
 // uoo/voo/woo = u/v/w over the full padded arrays (solver.py:223-225)
 // --------------------------------------------------------------------------
-__global__ void k_copy3(const double2* __restrict__ a0, double2* __restrict__ b0,
-                        const double2* __restrict__ a1, double2* __restrict__ b1,
-                        const double2* __restrict__ a2, double2* __restrict__ b2,
+__global__ void k_copy3(const double2* a0, double2* b0,
+                        const double2* a1, double2* b1,
+                        const double2* a2, double2* b2,
                         long n2) {
   pdl_entry();
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n2;
        t += (long)gridDim.x * blockDim.x) {
-    b0[t] = __ldg(a0 + t);
-    b1[t] = __ldg(a1 + t);
-    b2[t] = __ldg(a2 + t);
+    b0[t] = a0[t];
+    b1[t] = a1[t];
+    b2[t] = a2[t];
   }
 }
 __global__ void k_copy_tail(const double* a0, double* b0, const double* a1, double* b1,
@@ -420,7 +420,7 @@ __device__ __forceinline__ void diff_cell(const wf_case& c, const Geo& g, double
 // the same star.
 template <int COMP, bool DIFF>
 __global__ void __launch_bounds__(TPB) k_conv(const wf_case c, Geo g, double alpha,
-                                             const double* __restrict__ dtp, const Divs dv) {
+                                             const double* dtp, const Divs dv) {
   pdl_entry();
   const double* u = c.fld[WF_U];
   const double* v = c.fld[WF_V];
@@ -503,7 +503,7 @@ __global__ void __launch_bounds__(TPB) k_conv(const wf_case c, Geo g, double alp
 
 template <int COMP>
 __global__ void __launch_bounds__(TPB) k_diff(const wf_case c, Geo g, double alpha,
-                                             const double* __restrict__ dtp, const Divs dv) {
+                                             const double* dtp, const Divs dv) {
   pdl_entry();
   int ni, nj, nk;
   op_dims(COMP, g.n, ni, nj, nk);
@@ -552,7 +552,7 @@ int launch_diff(const wf_case& c, int comp, double alpha, const double* dt,
 // calvel (kernels.py:232-264): the three components in one launch
 // --------------------------------------------------------------------------
 __global__ void __launch_bounds__(TPB) k_calvel(const wf_case c, Geo g, double alpha,
-                                               const double* __restrict__ dtp, const Divs dv) {
+                                               const double* dtp, const Divs dv) {
   pdl_entry();
   const double* p = c.fld[WF_P];
   const double dt = *dtp;

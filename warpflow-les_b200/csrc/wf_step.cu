@@ -359,8 +359,9 @@ int wf_mg_residual_max(const wf_case* c, const double* phi0, const double* rhs0,
   if (!c || !phi0 || !rhs0 || !out) return fail(WF_EINVAL, "null argument");
   return mg_residual_max_pair(*c, phi0, rhs0, out, (cudaStream_t)s);
 }
-int wf_mg_coarse_op_elems(int32_t n, int32_t nlev, int64_t* op_elems, int64_t* scratch_elems) {
-  return coarse_op_elems(n, nlev, op_elems, scratch_elems);
+int wf_mg_coarse_op_elems(const wf_case* c, int64_t* op_elems, int64_t* scratch_elems) {
+  if (!c) return fail(WF_EINVAL, "null case");
+  return coarse_op_elems(*c, op_elems, scratch_elems);
 }
 
 int wf_mg_coarse_solve(const wf_case* c, double* phi, const double* rhs, void* s) {

@@ -86,7 +86,7 @@ SIGNATURES = {
     "wf_scalars_init": (_I32, [_VP, _D, _VP]),
     "wf_set_coarse_strategy": (_I32, [_I32, _I32, _I32]),
     "wf_mg_level_elems": (_I32, [_I32, _I32, _I32, ctypes.POINTER(ctypes.c_int64)]),
-    "wf_mg_coarse_op_elems": (_I32, [_I32, _I32, ctypes.POINTER(ctypes.c_int64),
+    "wf_mg_coarse_op_elems": (_I32, [_CP, ctypes.POINTER(ctypes.c_int64),
                                      ctypes.POINTER(ctypes.c_int64)]),
     "wf_mg_build_coarse_op": (_I32, [_CP, _VP]),
     "wf_mg_coarse_solve": (_I32, [_CP, _VP, _VP, _VP]),

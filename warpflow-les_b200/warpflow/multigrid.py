@@ -138,7 +138,7 @@ class Multigrid:
         if self.coarse != "operator" or c.nlev < 2 or c.n_coarse < 2:
             return None
         op_e, sc_e = ctypes.c_int64(), ctypes.c_int64()
-        if _abi.load().wf_mg_coarse_op_elems(c.n, c.nlev, ctypes.byref(op_e),
+        if _abi.load().wf_mg_coarse_op_elems(ctypes.byref(c), ctypes.byref(op_e),
                                             ctypes.byref(sc_e)) != 0:
             return None
         dt = torch.float32 if c.mg_fp32 else torch.float64

@@ -34,14 +34,40 @@ from .topology import build_topology
 NFIELDS = 13
 
 
+def coarse_op_elems(n, levels=3, precision="mixed"):
+    """(shared operator elements, per-case scratch elements) of the
+    coarse-level operator of an n^3 unit-cube case, from the library's own
+    sizing (wf_mg_coarse_op_elems, host-only), or (0, 0) when the coarsest
+    level runs as sweeps."""
+    if levels < 2:
+        return 0, 0
+    c = _abi.WfCase()
+    c.n, c.nlev, c.n_coarse = n, levels, 300
+    c.dx = c.dy = c.dz = 1.0 / n
+    c.mg_fp32 = 1 if precision == "mixed" else 0
+    op, sc = ctypes.c_int64(), ctypes.c_int64()
+    if _abi.load().wf_mg_coarse_op_elems(ctypes.byref(c), ctypes.byref(op),
+                                         ctypes.byref(sc)) != 0:
+        return 0, 0
+    word = 4 if precision == "mixed" else 8
+    if op.value * word > COARSE_OP_MAX_BYTES:
+        return 0, 0
+    return op.value, sc.value
+
+
+def operator_bytes(n, levels=3, precision="mixed"):
+    """Device bytes of the coarse-level operator shared by every case of
+    the same size, depth and precision (kept for the life of the process)."""
+    return coarse_op_elems(n, levels, precision)[0] * (4 if precision == "mixed" else 8)
+
+
 def case_bytes(n, levels=3, precision="mixed"):
-    """Device bytes a FlowSolver of an n^3 case allocates: 13 padded FP64
-    fields, FP64 multigrid levels (phi, rhs with one ring, level 0
-    included), the FP32 copies of every level in mixed precision, a scratch
-    of two level arrays per level in the multigrid's precision, the
-    partial-sum scratch of the coarse-level operator (32 coarse-level
-    arrays; the operator itself is shared by every case of the size), and
-    two scalar blocks plus one residual slot."""
+    """Device bytes a FlowSolver of an n^3 case allocates for itself: 13
+    padded FP64 fields, FP64 multigrid levels (phi, rhs with one ring, level
+    0 included), the FP32 copies of every level in mixed precision, a
+    scratch of two level arrays per level in the multigrid's precision, the
+    coarse-level operator's per-case scratch (the operator itself is shared:
+    operator_bytes), and two scalar blocks plus one residual slot."""
     fields = NFIELDS * (n + 6) ** 3 * 8
     mg = 0
     for l in range(levels):
@@ -51,11 +77,8 @@ def case_bytes(n, levels=3, precision="mixed"):
             mg += 2 * m ** 3 * 4 + 2 * m ** 3 * 4
         else:
             mg += 2 * m ** 3 * 8
-    nc = n >> (levels - 1)
     word = 4 if precision == "mixed" else 8
-    if levels > 1 and nc in OPERATOR_EDGES and \
-            (nc ** 3 // 2) ** 2 * word <= COARSE_OP_MAX_BYTES:
-        mg += 32 * nc ** 3 * word
+    mg += coarse_op_elems(n, levels, precision)[1] * word
     return fields + mg + 2 * ctypes.sizeof(_abi.WfScalars) + 8
 
 
@@ -111,21 +134,29 @@ class Completion:
 
 
 class Admission:
-    """FIFO admission against a memory budget (no GPU needed)."""
+    """FIFO admission against a memory budget (no GPU needed).  The ledger
+    holds every resident case's own bytes and, once per (N, levels,
+    precision), the shared coarse-level operator, which stays allocated for
+    the life of the process once a case of that kind has been built."""
 
     def __init__(self, budget_bytes, max_active=None):
         self.budget = int(budget_bytes)
         self.max_active = max_active
         self.queue = collections.deque()
         self.resident = {}     # rid -> bytes
+        self.shared = {}       # (n, levels, precision) -> operator bytes
         self.peak = 0
 
     @property
     def used(self):
-        return sum(self.resident.values())
+        return sum(self.resident.values()) + sum(self.shared.values())
+
+    def _extra(self, req):
+        key = (req.n, req.levels, req.precision)
+        return 0 if key in self.shared else operator_bytes(*key)
 
     def submit(self, req):
-        if req.bytes > self.budget:
+        if req.bytes + self._extra(req) + sum(self.shared.values()) > self.budget:
             raise ValueError("request %d needs %d bytes, more than the whole budget %d"
                              % (req.rid, req.bytes, self.budget))
         self.queue.append(req)
@@ -138,10 +169,13 @@ class Admission:
             req = self.queue[0]
             if self.max_active is not None and len(self.resident) >= self.max_active:
                 break
-            if self.used + req.bytes > self.budget:
+            extra = self._extra(req)
+            if self.used + req.bytes + extra > self.budget:
                 break
             self.queue.popleft()
             self.resident[req.rid] = req.bytes
+            if extra:
+                self.shared[(req.n, req.levels, req.precision)] = extra
             self.peak = max(self.peak, self.used)
             out.append(req)
         return out
