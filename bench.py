@@ -264,76 +264,153 @@ def _events():
     return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
 
-def bench_ensemble(args):
-    """Ensemble: 64 seeded cavity cases (N in {32..96}, Re in [100, 1000], lid
-    in [0.5, 1.5]), mixed-precision multigrid, advanced together; compared
-    with the plain FP64 per-case loop (one case after another) on the same
-    cases."""
+def ensemble_compare(ncases, steps, warmup, streams=32, single_graph=True, seed=0):
+    """The seeded cavity ensemble (N in {32..96}, Re in [100, 1000], lid in
+    [0.5, 1.5]) advanced together with mixed-precision multigrid (one graph
+    launch per batch step), and the plain FP64 per-case loop on the same
+    cases (every case's own step graph launched one after another on one
+    stream), each timed over the same number of batch steps; every batch
+    step ends with one gather of all cases' scalar blocks."""
     import torch
     from warpflow.ensemble import Ensemble, cavity_case, random_ensemble
-    specs = random_ensemble(args.cases, seed=0)
-    K, W = args.steps, max(3, args.warmup)
+    specs = random_ensemble(ncases, seed=seed)
 
-    def run(precision, concurrent, steps, warm):
+    def run(precision, concurrent):
         cfgs = [cavity_case(sp.n, sp.re, sp.ulid, precision=precision) for sp in specs]
         if concurrent:
-            ens = Ensemble(cfgs, nstreams=args.streams or 32, single_graph=args.single_graph)
+            ens = Ensemble(cfgs, nstreams=streams, single_graph=single_graph)
         else:
             ens = Ensemble(cfgs, nstreams=1, single_graph=False)
-        for _ in range(warm):
+        for _ in range(warmup):
             ens.step()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(steps):
-            if concurrent:
-                ens.step()
-            else:
-                for i in range(len(ens)):
-                    ens.step([i])
+            ens.step()
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         cells = ens.cells(range(len(ens)))
         iters = sum(s.outer_iters for s in ens.solvers) / len(ens)
         ens.close()
+        del ens
+        torch.cuda.empty_cache()
         return cells * steps / dt / 1e6, dt, iters
 
-    val, dt, iters = run("mixed", True, K, W)
-    plain, pdt, _ = run("fp64", False, max(2, K // 4), 2)
-    print(json.dumps({
-        "mode": "ensemble", "metric": "Mcell-steps/s (64-case cavity ensemble, mixed MG)",
-        "value": round(val, 2), "unit": "Mcell-steps/s", "steps": K, "warmup": W,
-        "ms_per_batch_step": round(1e3 * dt / K, 3), "iters_mean": round(iters, 2),
-        "plain_fp64_per_case_loop": round(plain, 2),
-        "speedup_vs_plain": round(val / plain, 2),
-        "config": {"cases": args.cases, "streams": args.streams or 32,
-                   "single_graph": bool(args.single_graph),
-                   "sizes": sorted({sp.n for sp in specs}),
-                   "seed": 0, "timing": "wall clock around whole batch steps, synced"}}),
-        flush=True)
+    val, dt, iters = run("mixed", True)
+    plain, pdt, piters = run("fp64", False)
+    return {"cases": ncases, "steps": steps, "warmup": warmup, "seed": seed,
+            "sizes": sorted({sp.n for sp in specs}),
+            "mixed_batched_Mcell_steps_per_s": round(val, 2),
+            "ms_per_batch_step": round(1e3 * dt / steps, 3), "iters_mean": round(iters, 2),
+            "plain_fp64_per_case_loop_Mcell_steps_per_s": round(plain, 2),
+            "plain_ms_per_batch_step": round(1e3 * pdt / steps, 3),
+            "plain_iters_mean": round(piters, 2),
+            "speedup_vs_plain": round(val / plain, 3),
+            "timing": "wall clock around the timed batch steps, synced on both sides"}
+
+
+def bench_ensemble(args):
+    """Ensemble mode: ensemble_compare on --cases cases for --steps steps."""
+    out = ensemble_compare(args.cases, args.steps, max(3, args.warmup),
+                           streams=args.streams or 32, single_graph=bool(args.single_graph))
+    out.update({"mode": "ensemble", "metric": "Mcell-steps/s (cavity ensemble, mixed MG)",
+                "value": out["mixed_batched_Mcell_steps_per_s"], "unit": "Mcell-steps/s"})
+    print(json.dumps(out), flush=True)
+
+
+def step256_extra(peak, peak_kind, steps=10, warmup=3):
+    """The 256^3 cavity with 5 multigrid levels (FP64), device-timed like the
+    main line (CUDA events around each step's graph launch, L2 flushed
+    between steps)."""
+    import torch
+    from warpflow import FlowSolver, build_topology
+    from warpflow.config import case_from_dict
+    n, levels = 256, 5
+    cfg = case_from_dict(case_raw(n, levels, "fp64"))
+    sol = FlowSolver(cfg, build_topology(cfg), "cuda:0")
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda:0")
+    for _ in range(warmup):
+        sol.step()
+    torch.cuda.synchronize()
+    ms, its, nmgs = [], [], []
+    for _ in range(steps):
+        flush.zero_()
+        a, b = _events()
+        a.record()
+        sol.launch_step()
+        b.record()
+        sol.finish_step()
+        ms.append(a.elapsed_time(b))
+        its.append(sol.outer_iters)
+        nmgs.append(sol.last_nmg)
+    sol.close()
+    del sol, flush
+    torch.cuda.empty_cache()
+    tot = sum(ms) / 1e3
+    byts = sum(step_bytes(n, it, m, levels, 8) for it, m in zip(its, nmgs))
+    ach = byts / tot / 1e9
+    return {"workload": "lid-driven cavity 256^3, Re 400, WALE, variable dt, 5-level RBGS "
+                        "multigrid 6/6/300 x4, FP64", "steps": steps, "warmup": warmup,
+            "ms_per_step": round(sum(ms) / steps, 4),
+            "value": round(n ** 3 * steps / tot / 1e6, 2), "unit": "Mcell-steps/s",
+            "iters_mean": round(sum(its) / steps, 3),
+            "roofline_step": {"bound": "hbm", "achieved": round(ach, 1), "peak": peak,
+                              "peak_kind": peak_kind, "unit": "GB/s",
+                              "frac": round(ach / peak, 4)}}
 
 
 def bench_serve(args):
-    """Serving: a seeded Poisson request stream (20 req/s, N in {32..128},
-    Re in [100, 1000], steps in [100, 2000] scaled by --step-scale) served
-    with continuous batching under a 150 GB budget."""
+    """Serving: seeded Poisson request streams (20 req/s, N in {32..128},
+    Re in [100, 1000], steps in [100, 2000] scaled by --step-scale: a
+    reduced form of the served-stream configuration) served with continuous
+    batching under a 150 GB budget, one stream per seed; then the first
+    seed's requests all at once (the saturation throughput)."""
+    import numpy as np
+    import torch
     from warpflow.serve import CavityServer, poisson_stream
-    reqs = poisson_stream(count=args.requests, rate=20.0, seed=0,
-                          step_scale=args.step_scale)
+    runs = []
+    for seed in range(args.seeds):
+        reqs = poisson_stream(count=args.requests, rate=20.0, seed=seed,
+                              step_scale=args.step_scale)
+        srv = CavityServer(budget_bytes=150 * 10 ** 9, nstreams=args.streams or 16)
+        srv.warmup(reqs)
+        srv.run(reqs)
+        s = srv.summary()
+        srv.close()
+        span = max(r.arrival for r in reqs) - min(r.arrival for r in reqs)
+        offered = sum(r.n ** 3 * r.n_steps for r in reqs) / span / 1e6
+        runs.append({"seed": seed, "p50_s": round(s["p50_s"], 4), "p99_s": round(s["p99_s"], 4),
+                     "Mcell_steps_per_s": round(s["mcell_steps_per_s"], 2),
+                     "offered_Mcell_steps_per_s": round(offered, 2),
+                     "wall_s": round(s["wall_s"], 2), "step_batches": s["step_batches"],
+                     "solvers_built": s["solvers_built"], "solver_reuses": s["solver_reuses"],
+                     "peak_resident_GB": round(s["peak_resident_bytes"] / 1e9, 3)})
+        del srv
+        torch.cuda.empty_cache()
+    reqs = poisson_stream(count=args.requests, rate=20.0, seed=0, step_scale=args.step_scale)
     srv = CavityServer(budget_bytes=150 * 10 ** 9, nstreams=args.streams or 16)
     srv.warmup(reqs)
-    srv.run(reqs)
-    s = srv.summary()
+    srv.run(reqs, time_scale=1e-9)    # every request arrives at once
+    sat = srv.summary()
+    srv.close()
+    p50s = [r["p50_s"] for r in runs]
     print(json.dumps({
         "mode": "serve", "metric": "served cavity stream: p50/p99 latency, Mcell-steps/s",
-        "p50_s": round(s["p50_s"], 4), "p99_s": round(s["p99_s"], 4),
-        "value": round(s["mcell_steps_per_s"], 2), "unit": "Mcell-steps/s",
-        "wall_s": round(s["wall_s"], 2), "step_batches": s["step_batches"],
-        "peak_resident_GB": round(s["peak_resident_bytes"] / 1e9, 3),
-        "config": {"requests": args.requests, "rate_per_s": 20.0, "seed": 0,
-                   "step_scale": args.step_scale, "budget_GB": 150, "streams": args.streams or 16,
+        "p50_s_median": round(float(np.median(p50s)), 4),
+        "p50_s_spread": round(max(p50s) / min(p50s), 3),
+        "p99_s_median": round(float(np.median([r["p99_s"] for r in runs])), 4),
+        "value": round(float(np.median([r["Mcell_steps_per_s"] for r in runs])), 2),
+        "unit": "Mcell-steps/s",
+        "saturation_Mcell_steps_per_s": round(sat["mcell_steps_per_s"], 2),
+        "runs": runs,
+        "config": {"requests": args.requests, "rate_per_s": 20.0, "seeds": args.seeds,
+                   "step_scale": args.step_scale, "budget_GB": 150,
+                   "streams": args.streams or 16,
+                   "reduced": "step counts x %g and %d requests per stream (the full "
+                              "configuration: x1, 256)" % (args.step_scale, args.requests),
                    "latency": "arrival to end of last step, wall clock",
-                   "startup": "one case per size built and stepped before the stream starts"}}),
-          flush=True)
+                   "startup": "one solver per kind built and stepped before the stream "
+                              "starts, kept resident for reuse"}}), flush=True)
 
 
 def bench_poisson(args):
@@ -411,7 +488,11 @@ def main():
                     help="stream pool (default: 32 for --mode ensemble, 16 for --mode serve)")
     ap.add_argument("--single-graph", type=int, default=1,
                     help="ensemble: all cases in one CUDA graph (1) or a stream pool (0)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the 256^3 step and the ensemble comparison added to the line")
+    ap.add_argument("--ens-steps", type=int, default=50)
     ap.add_argument("--requests", type=int, default=48)
+    ap.add_argument("--seeds", type=int, default=5)
     ap.add_argument("--step-scale", type=float, default=0.05)
     args = ap.parse_args()
     if args.mode != "step":
@@ -579,6 +660,11 @@ def main():
                "sample": "first 2 steps of the %d^3 cavity (NumPy FP64 oracle, %.1f s); the "
                          "reference's Warp CPU path is unavailable here" % (args.n, cdt)}
 
+    extras = {}
+    if world == 1 and not args.no_extras and args.n == 80:
+        extras["extra_step256_L5_fp64"] = step256_extra(peak, peak_kind)
+        extras["extra_ensemble64_mixed_vs_plain"] = ensemble_compare(64, args.ens_steps, 3)
+
     if rank == 0:
         line = {"metric": metric, "value": round(value, 2), "unit": "Mcell-steps/s",
                 "n_gpus": world, "steps": K, "warmup": W,
@@ -591,6 +677,7 @@ def main():
                 "clocks": clocks, "roofline": roofline, "roofline_step": roofline_step,
                 "roofline_coarse": roofline_coarse,
                 "cpu_baseline": cpu, "e2e": e2e}
+        line.update(extras)
         print(json.dumps(line), flush=True)
     sol.close()
     if world > 1:

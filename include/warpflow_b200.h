@@ -73,6 +73,8 @@ typedef struct wf_scalars {
   double cfl;         /* dt_old / dtmax (FlowSolver.cfl) */
   double dtmax;       /* min(dtvisc, dtcfl) of the last checkdt */
   double umax, vmax, wmax, dtvisc;      /* last checkdt reductions */
+  double rrey, ulid;  /* 1/Re and lid velocity: the step reads them here, so a built step
+                         serves a new case of the same size after wf_scalars_init */
   double rmax_trace[32];                /* rmax of every outer iteration */
   unsigned long long red[6];            /* reduction scratch (bit patterns) */
   int32_t itime;      /* step counter (FlowSolver.itime) */
@@ -116,8 +118,10 @@ WF_API int wf_version(void);
 WF_API const char* wf_last_error(void);
 /* sizeof(wf_scalars), sizeof(wf_case) as compiled, for binding checks */
 WF_API int wf_struct_sizes(int64_t* scalars, int64_t* casebytes);
-/* solver.py:60-65 initial scalars: dt = dt0, ctime = 0, itime = 0, ... */
-WF_API int wf_scalars_init(wf_scalars* sc, double dt0, void* stream);
+/* solver.py:60-65 initial scalars: dt = dt0, ctime = 0, itime = 0, ...,
+ * and the case's 1/Re and lid velocity (sc->rrey, sc->ulid), which the step
+ * of wf_stepper_create reads from the block rather than from its wf_case */
+WF_API int wf_scalars_init(wf_scalars* sc, double dt0, double rrey, double ulid, void* stream);
 /* Tuning knob (no reference counterpart): how a many-sweep relax of an n^3
  * level (n <= 64) runs -- 0 one CTA, 1 cluster with a barrier per
  * half-sweep, 2 cluster with point-to-point halo pushes.  Process-wide;

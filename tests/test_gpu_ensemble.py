@@ -39,6 +39,28 @@ def test_ensemble_matches_alone(precision, single_graph):
             np.testing.assert_array_equal(sol.f[name].numpy(), arr)
 
 
+@pytest.mark.parametrize("serial", [False, True])
+def test_reset_matches_fresh_solver(serial):
+    """A solver reset on the device for a new case (Re, lid velocity) steps
+    exactly like a solver built for that case (the server's reuse)."""
+    from warpflow import FlowSolver, build_topology
+    from warpflow.ensemble import cavity_case
+    a_cfg = cavity_case(24, 300.0, 0.8, precision="mixed")
+    b_cfg = cavity_case(24, 700.0, 1.2, precision="mixed")
+    a = FlowSolver(a_cfg, build_topology(a_cfg), "cuda:0", serial=serial)
+    for _ in range(3):
+        a.step()
+    a.reset(b_cfg)
+    b = FlowSolver(b_cfg, build_topology(b_cfg), "cuda:0", serial=serial)
+    for _ in range(5):
+        assert a.step() == b.step()
+    for name in ("u", "v", "w", "p", "vis", "su", "pp", "uoo"):
+        np.testing.assert_array_equal(a.f[name].numpy(), b.f[name].numpy(), err_msg=name)
+    assert (a.itime, a.rey, a.ulid) == (b.itime, b.rey, b.ulid)
+    with pytest.raises(ValueError):
+        a.reset(cavity_case(32, 700.0, 1.2, precision="mixed"))
+
+
 def test_case_bytes_matches_allocation():
     from warpflow import FlowSolver, build_topology
     from warpflow.ensemble import cavity_case

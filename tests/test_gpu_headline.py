@@ -160,9 +160,15 @@ def test_served_case_matches_fp64_oracle():
     reqs = [Request(rid=0, n=24, re=300.0, ulid=1.0, n_steps=15, arrival=0.0,
                     levels=levels_for(24)),
             Request(rid=1, n=16, re=900.0, ulid=0.7, n_steps=25, arrival=0.0,
-                    levels=levels_for(16))]
+                    levels=levels_for(16)),
+            Request(rid=2, n=24, re=600.0, ulid=1.3, n_steps=10, arrival=0.05,
+                    levels=levels_for(24))]
     srv = CavityServer(nstreams=2, keep_fields=True)
+    srv.warmup(reqs)
     done = srv.run(reqs)
+    # the start-up solvers and finished ones were reset and reused
+    assert srv.summary()["solver_reuses"] >= 2
+    srv.close()
     for req, c in zip(reqs, done):
         assert not c.error, c.error
         assert c.info["rmax"] < 1e-6

@@ -79,6 +79,36 @@ def test_operator_bytes_and_shared_charge():
     assert adm.used == 2 * case_bytes(80, 3, "fp64") + op   # still charged once
 
 
+def test_idle_solvers_reused_and_evicted():
+    """A finished case's solver stays charged as idle and serves the next
+    request of its kind with no new bytes; a request of another kind that
+    does not fit evicts idle solvers (largest first)."""
+    from warpflow.serve import Admission, Request, case_bytes, operator_bytes
+    k32, k48 = (32, 3, "mixed"), (48, 3, "mixed")
+    b32, b48 = case_bytes(32), case_bytes(48)
+    o32, o48 = operator_bytes(32), operator_bytes(48)
+    adm = Admission(budget_bytes=b32 + b48 + o32 + o48)
+    adm.submit(Request(0, 32, 400.0, 1.0, 5, arrival=0.0))
+    assert [r.rid for r in adm.admit(0.0)] == [0] and not adm.reused
+    adm.release(0, keep=k32)
+    assert adm.idle[k32] == 1 and adm.used == b32 + o32
+    adm.submit(Request(1, 32, 700.0, 0.8, 5, arrival=0.1))
+    assert [r.rid for r in adm.admit(0.2)] == [1] and adm.reused == {1}
+    assert adm.idle[k32] == 0 and adm.used == b32 + o32     # no new bytes
+    adm.release(1, keep=k32)
+    # two 48^3 cases need the idle 32^3 solver's memory
+    adm.submit(Request(2, 48, 400.0, 1.0, 5, arrival=0.3))
+    assert [r.rid for r in adm.admit(0.3)] == [2]
+    assert adm.evicted == [] and adm.idle[k32] == 1
+    adm.submit(Request(3, 48, 400.0, 1.0, 5, arrival=0.4))
+    adm.budget = 2 * b48 + o32 + o48
+    assert [r.rid for r in adm.admit(0.4)] == [3]
+    assert adm.evicted == [k32] and adm.idle[k32] == 0
+    assert adm.used == 2 * b48 + o32 + o48 <= adm.budget
+    # keep_idle respects the budget
+    assert not adm.keep_idle(k32)
+
+
 def test_admission_rejects_oversize():
     from warpflow.serve import Admission, Request
     adm = Admission(budget_bytes=1000)

@@ -17,6 +17,7 @@ struct FaceOp {
   int g0, s0;
   double val;  // sign for lin, value for const
   int a0, na, b0, nb;
+  const double* valp;  // const: the value read on the device instead, when set
 };
 
 constexpr int MAX_OPS_PER_PHASE = 4;
@@ -70,7 +71,7 @@ __global__ void k_fill_phase(const PhaseArgs args) {
         }
         f[gi] = op.val * f[si];
       } else {
-        f[gi] = op.val;
+        f[gi] = op.valp ? *op.valp : op.val;
       }
     }
   }
@@ -79,15 +80,15 @@ __global__ void k_fill_phase(const PhaseArgs args) {
 // ---- fill programs: the reference launch lists, split into axis phases ----
 static FaceOp lin(int axis, int high, int g0, int s0, double sign, int a0, int na,
                   int b0, int nb, int nlay) {
-  return FaceOp{axis, high, 1, nlay, g0, s0, sign, a0, na, b0, nb};
+  return FaceOp{axis, high, 1, nlay, g0, s0, sign, a0, na, b0, nb, nullptr};
 }
 static FaceOp cst(int axis, int high, int g0, double val, int a0, int na, int b0,
-                  int nb, int nlay) {
-  return FaceOp{axis, high, 0, nlay, g0, 0, val, a0, na, b0, nb};
+                  int nb, int nlay, const double* valp = nullptr) {
+  return FaceOp{axis, high, 0, nlay, g0, 0, val, a0, na, b0, nb, valp};
 }
 
 // phase ops of one fill kind; returns op count for `phase` (0 = x, 1 = y, 2 = z)
-static int program(int kind, int n, double val, int phase, FaceOp* out) {
+static int program(int kind, int n, double val, const double* valp, int phase, FaceOp* out) {
   const int P = NPL;
   int k = 0;
   switch (kind) {
@@ -100,7 +101,7 @@ static int program(int kind, int n, double val, int phase, FaceOp* out) {
         out[k++] = lin(1, 1, P + n, P + n - 1, 1.0, P - 1, n + 1, P - 1, n + 2, 3);
       } else {
         out[k++] = lin(2, 0, P - 1, P, -1.0, P - 1, n + 1, P - 1, n + 2, 3);
-        out[k++] = cst(2, 1, P + n, val, P - 1, n + 1, P - 1, n + 2, 3);
+        out[k++] = cst(2, 1, P + n, val, P - 1, n + 1, P - 1, n + 2, 3, valp);
       }
       break;
     case FILL_V:  // bcs.py:225-244
@@ -129,15 +130,15 @@ static int program(int kind, int n, double val, int phase, FaceOp* out) {
       break;
     case FILL_VIS:  // bcs.py:267-293
       if (phase == 0) {
-        out[k++] = cst(0, 0, P, val, P - 1, n + 2, P - 1, n + 2, 1);
+        out[k++] = cst(0, 0, P, val, P - 1, n + 2, P - 1, n + 2, 1, valp);
         out[k++] = lin(0, 0, P - 1, P, 1.0, P - 1, n + 2, P - 1, n + 2, 1);
-        out[k++] = cst(0, 1, P + n - 1, val, P - 1, n + 2, P - 1, n + 2, 1);
+        out[k++] = cst(0, 1, P + n - 1, val, P - 1, n + 2, P - 1, n + 2, 1, valp);
         out[k++] = lin(0, 1, P + n, P + n - 1, 1.0, P - 1, n + 2, P - 1, n + 2, 1);
       } else if (phase == 1) {
         out[k++] = lin(1, 0, P - 1, P, 1.0, P - 1, n + 2, P - 1, n + 2, 1);
         out[k++] = lin(1, 1, P + n, P + n - 1, 1.0, P - 1, n + 2, P - 1, n + 2, 1);
       } else {
-        out[k++] = cst(2, 0, P, val, P - 1, n + 2, P - 1, n + 2, 1);
+        out[k++] = cst(2, 0, P, val, P - 1, n + 2, P - 1, n + 2, 1, valp);
         out[k++] = lin(2, 0, P - 1, P, 1.0, P - 1, n + 2, P - 1, n + 2, 1);
         out[k++] = lin(2, 1, P + n, P + n - 1, 1.0, P - 1, n + 2, P - 1, n + 2, 1);
       }
@@ -165,7 +166,7 @@ int launch_fills(const FillReq* reqs, int nreq, int n, cudaStream_t s) {
     for (int r = 0; r < nreq; ++r) {
       if (!reqs[r].fld) return fail(WF_EINVAL, "launch_fills: null field");
       a.job[r].fld = reqs[r].fld;
-      a.job[r].nops = program(reqs[r].kind, n, reqs[r].val, phase, a.job[r].ops);
+      a.job[r].nops = program(reqs[r].kind, n, reqs[r].val, reqs[r].valp, phase, a.job[r].ops);
       for (int o = 0; o < a.job[r].nops; ++o) {
         a.amax = a.job[r].ops[o].na > a.amax ? a.job[r].ops[o].na : a.amax;
         a.bmax = a.job[r].ops[o].nb > a.bmax ? a.job[r].ops[o].nb : a.bmax;

@@ -75,7 +75,8 @@ enum FillKind { FILL_U = 0, FILL_V, FILL_W, FILL_VIS, FILL_PBOUND, FILL_PMIRROR 
 struct FillReq {
   double* fld;
   int kind;
-  double val;   // ulid for u, 1/Re for vis
+  double val;               // ulid for u, 1/Re for vis
+  const double* valp = nullptr;  // the same value read on the device, when set
 };
 // up to 3 independent field fills, executed as 3 ordered axis phases
 int launch_fills(const FillReq* reqs, int nreq, int n, cudaStream_t s);
@@ -85,7 +86,8 @@ int launch_init_noise(double* u, double* v, double* w, int n, double amp,
                       int seed, cudaStream_t s);
 int launch_checkdt(const wf_case& c, cudaStream_t s);
 int launch_copy_oo(const wf_case& c, cudaStream_t s);
-int launch_wale(const wf_case& c, cudaStream_t s);
+// rrey_dev: 1/Re read on the device (the step), or null for c.rrey
+int launch_wale(const wf_case& c, cudaStream_t s, const double* rrey_dev = nullptr);
 int launch_conv(const wf_case& c, int comp, double alpha, const double* dt, cudaStream_t s,
                 bool with_diff = false);
 int launch_diff(const wf_case& c, int comp, double alpha, const double* dt, cudaStream_t s);
@@ -94,7 +96,7 @@ int launch_calvel(const wf_case& c, double alpha, const double* dt, cudaStream_t
 int launch_calmas(const wf_case& c, unsigned long long h_if,
                   unsigned long long h_loop, cudaStream_t s);
 int launch_add_ring(double* p, const double* pp, int n, cudaStream_t s);
-int launch_scalars_init(wf_scalars* sc, double dt0, cudaStream_t s);
+int launch_scalars_init(wf_scalars* sc, double dt0, double rrey, double ulid, cudaStream_t s);
 
 // ---- multigrid -----------------------------------------------------------
 int mg_solve(const wf_case& c, cudaStream_t s);

@@ -78,10 +78,12 @@ static inline int nblocks(long work, int tpb = TPB, int cap = 148 * 16) {
 // --------------------------------------------------------------------------
 // scalar block
 // --------------------------------------------------------------------------
-__global__ void k_scalars_init(wf_scalars* sc, double dt0) {
+__global__ void k_scalars_init(wf_scalars* sc, double dt0, double rrey, double ulid) {
   pdl_entry();
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   sc->dt = dt0;
+  sc->rrey = rrey;
+  sc->ulid = ulid;
   sc->ctime = 0.0;
   sc->rmax = 0.0;
   sc->cfl = 0.0;
@@ -102,9 +104,9 @@ __global__ void k_scalars_init(wf_scalars* sc, double dt0) {
   sc->gbar[0] = sc->gbar[1] = 0u;
 }
 
-int launch_scalars_init(wf_scalars* sc, double dt0, cudaStream_t s) {
+int launch_scalars_init(wf_scalars* sc, double dt0, double rrey, double ulid, cudaStream_t s) {
   if (!sc) return fail(WF_EINVAL, "null scalar block");
-  WF_CK(launch_k(k_scalars_init, 1, 32, 0, s, sc, dt0));
+  WF_CK(launch_k(k_scalars_init, 1, 32, 0, s, sc, dt0, rrey, ulid));
   WF_CKL("k_scalars_init");
   return WF_OK;
 }
@@ -270,7 +272,7 @@ int launch_copy_oo(const wf_case& c, cudaStream_t s) {
 // it in every thread; one host pow gives the same value without a device
 // pow per cell)
 __global__ void __launch_bounds__(TPB) k_wale(const wf_case c, Geo g, const Divs dv,
-                                             const double ls) {
+                                             const double ls, const double* rrey_dev) {
   pdl_entry();
   const double* u = c.fld[WF_U];
   const double* v = c.fld[WF_V];
@@ -330,13 +332,14 @@ __global__ void __launch_bounds__(TPB) k_wale(const wf_case c, Geo g, const Divs
       const double denom = as * as * sqrt(as) + sdsd * sqrt(rs);
       nut = ls * ls * sdsd15 / denom;
     }
-    vis[id] = c.rrey + nut;
+    vis[id] = (rrey_dev ? *rrey_dev : c.rrey) + nut;
   }
 }
 
 // vis = 1/Re on real cells (kernels.py:442-449)
-__global__ void k_fill_real(double* f, Geo g, double val) {
+__global__ void k_fill_real(double* f, Geo g, double val, const double* valp) {
   pdl_entry();
+  if (valp) val = *valp;
   const long tot = (long)g.n * g.n * g.n;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
        t += (long)gridDim.x * blockDim.x) {
@@ -347,17 +350,18 @@ __global__ void k_fill_real(double* f, Geo g, double val) {
   }
 }
 
-int launch_wale(const wf_case& c, cudaStream_t s) {
+int launch_wale(const wf_case& c, cudaStream_t s, const double* rrey_dev) {
   Geo g = geo_of(c.n);
   const long tot = (long)c.n * c.n * c.n;
   if (c.sgs) {
     const double ls = c.cw * std::pow(c.dx * c.dy * c.dz, 1.0 / 3.0);
-    WF_CK(launch_k(k_wale, cells3(c.n, c.n, c.n), cell_block(), 0, s, c, g, divs_of(c), ls));
+    WF_CK(launch_k(k_wale, cells3(c.n, c.n, c.n), cell_block(), 0, s, c, g, divs_of(c), ls,
+                   rrey_dev));
     WF_CKL("k_wale");
-    FillReq r{c.fld[WF_VIS], FILL_VIS, c.rrey};
+    FillReq r{c.fld[WF_VIS], FILL_VIS, c.rrey, rrey_dev};
     return launch_fills(&r, 1, c.n, s);
   }
-  WF_CK(launch_k(k_fill_real, nblocks(tot), TPB, 0, s, c.fld[WF_VIS], g, c.rrey));
+  WF_CK(launch_k(k_fill_real, nblocks(tot), TPB, 0, s, c.fld[WF_VIS], g, c.rrey, rrey_dev));
   WF_CKL("k_fill_real");
   return WF_OK;
 }

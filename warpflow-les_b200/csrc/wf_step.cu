@@ -71,15 +71,25 @@ int validate_case(const wf_case& c) {
   return WF_OK;
 }
 
+// The step reads 1/Re and the lid velocity from the case's scalar block
+// (wf_scalars_init writes them), so that a built step can serve a new case
+// of the same size without being rebuilt.
 static int fill_comp(const wf_case& c, int comp, cudaStream_t s) {
-  FillReq r{c.fld[WF_U + comp], comp == 0 ? FILL_U : (comp == 1 ? FILL_V : FILL_W), c.ulid};
+  FillReq r{c.fld[WF_U + comp], comp == 0 ? FILL_U : (comp == 1 ? FILL_V : FILL_W), c.ulid,
+            comp == 0 ? &c.sc->ulid : nullptr};
   return launch_fills(&r, 1, c.n, s);
+}
+
+static int fill_uvw(const wf_case& c, cudaStream_t s) {
+  FillReq r[3] = {{c.fld[WF_U], FILL_U, c.ulid, &c.sc->ulid}, {c.fld[WF_V], FILL_V, 0.0},
+                  {c.fld[WF_W], FILL_W, 0.0}};
+  return launch_fills(r, 3, c.n, s);
 }
 
 static int step_prologue(const wf_case& c, cudaStream_t s) {
   WF_TRY(launch_checkdt(c, s));
   WF_TRY(launch_copy_oo(c, s));
-  WF_TRY(launch_wale(c, s));
+  WF_TRY(launch_wale(c, s, &c.sc->rrey));
   const double* dt = &c.sc->dt;
   const double alfark[2] = {0.5, 1.0};  // solver.py:26
   for (int st = 0; st < 2; ++st) {
@@ -91,9 +101,7 @@ static int step_prologue(const wf_case& c, cudaStream_t s) {
     }
     // the fills solver.py:258-263 runs before each diffusion still set the
     // ghost edges and corners that later fills read
-    FillReq r[3] = {{c.fld[WF_U], FILL_U, c.ulid}, {c.fld[WF_V], FILL_V, 0.0},
-                    {c.fld[WF_W], FILL_W, 0.0}};
-    WF_TRY(launch_fills(r, 3, c.n, s));
+    WF_TRY(fill_uvw(c, s));
     if (st == 0) WF_TRY(launch_calvel(c, alfark[st], dt, s));
   }
   return launch_calvel(c, 1.0, dt, s);
@@ -107,11 +115,7 @@ static int step_mg_part(const wf_case& c, cudaStream_t s) {
   return launch_calvel(c, 1.0, &c.sc->dt, s);
 }
 
-static int step_epilogue(const wf_case& c, cudaStream_t s) {
-  FillReq r[3] = {{c.fld[WF_U], FILL_U, c.ulid}, {c.fld[WF_V], FILL_V, 0.0},
-                  {c.fld[WF_W], FILL_W, 0.0}};
-  return launch_fills(r, 3, c.n, s);
-}
+static int step_epilogue(const wf_case& c, cudaStream_t s) { return fill_uvw(c, s); }
 
 }  // namespace wf
 
@@ -266,8 +270,8 @@ int wf_mg_level_elems(int32_t n, int32_t nlev, int32_t level, int64_t* elems) {
   return WF_OK;
 }
 
-int wf_scalars_init(wf_scalars* sc, double dt0, void* stream) {
-  return launch_scalars_init(sc, dt0, (cudaStream_t)stream);
+int wf_scalars_init(wf_scalars* sc, double dt0, double rrey, double ulid, void* stream) {
+  return launch_scalars_init(sc, dt0, rrey, ulid, (cudaStream_t)stream);
 }
 
 int wf_init_noise(double* u, double* v, double* w, int32_t n, double amp, int32_t seed,

@@ -30,6 +30,8 @@ class WfScalars(ctypes.Structure):
         ("vmax", ctypes.c_double),
         ("wmax", ctypes.c_double),
         ("dtvisc", ctypes.c_double),
+        ("rrey", ctypes.c_double),
+        ("ulid", ctypes.c_double),
         ("rmax_trace", ctypes.c_double * 32),
         ("red", ctypes.c_uint64 * 6),
         ("itime", ctypes.c_int32),
@@ -83,7 +85,7 @@ SIGNATURES = {
     "wf_version": (_I32, []),
     "wf_last_error": (ctypes.c_char_p, []),
     "wf_struct_sizes": (_I32, [ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
-    "wf_scalars_init": (_I32, [_VP, _D, _VP]),
+    "wf_scalars_init": (_I32, [_VP, _D, _D, _D, _VP]),
     "wf_set_coarse_strategy": (_I32, [_I32, _I32, _I32]),
     "wf_mg_level_elems": (_I32, [_I32, _I32, _I32, ctypes.POINTER(ctypes.c_int64)]),
     "wf_mg_coarse_op_elems": (_I32, [_CP, ctypes.POINTER(ctypes.c_int64),

@@ -126,7 +126,7 @@ class Multigrid:
         self._sc = torch.zeros(ctypes.sizeof(_abi.WfScalars), dtype=torch.uint8,
                                device=self.device)
         self._out = torch.zeros(1, dtype=torch.float64, device=self.device)
-        _abi.call("wf_scalars_init", self._sc.data_ptr(), 0.0, self._stream())
+        _abi.call("wf_scalars_init", self._sc.data_ptr(), 0.0, 0.0, 0.0, self._stream())
         self.case()   # builds (or finds) the coarse operator now, not in a timed call
 
     def _stream(self):

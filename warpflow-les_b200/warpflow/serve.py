@@ -2,10 +2,16 @@
 
 Requests (N, Re, lid velocity, step count) arrive over time.  The server
 admits a queued request as soon as its device memory -- fields plus
-multigrid hierarchy, computed exactly by ``case_bytes`` -- fits in the HBM
-budget next to the cases already resident, keeps every admitted case
-resident until its last step, and advances all resident cases together one
-step at a time (``Ensemble``-style concurrent graph launches).  Requests
+multigrid hierarchy, computed exactly by ``case_bytes``, and the shared
+coarse-level operator of its kind -- fits in the HBM budget next to the
+cases already resident, keeps every admitted case resident until its last
+step, and advances all resident cases together one step at a time
+(``Ensemble``-style concurrent graph launches).  A finished case's solver
+stays resident and serves the next request of the same size: it is reset
+on the device (``FlowSolver.reset``: fields re-initialised, 1/Re and the
+lid velocity written to its scalar block), so steady-state admission
+allocates nothing and captures no graph; only requests of a kind with no
+idle solver build one, on a worker thread.  Requests
 that arrive while others run join at the next step boundary; finished
 cases leave at a step boundary and free their memory for the queue.
 Latency is measured from arrival to the end of the request's last step.
@@ -134,10 +140,17 @@ class Completion:
 
 
 class Admission:
-    """FIFO admission against a memory budget (no GPU needed).  The ledger
-    holds every resident case's own bytes and, once per (N, levels,
-    precision), the shared coarse-level operator, which stays allocated for
-    the life of the process once a case of that kind has been built."""
+    """FIFO admission against a memory budget (no GPU needed).
+
+    The ledger holds every running case's own bytes, the idle solvers kept
+    resident for reuse (a finished case's solver serves the next request of
+    its size: ``idle`` counts them per (N, levels, precision)), and, once
+    per kind, the shared coarse-level operator, which stays allocated for
+    the life of the process once a case of that kind has been built.  A
+    request of a kind with an idle solver takes it and needs no new bytes;
+    otherwise idle solvers of other kinds are evicted (largest first) until
+    the request fits; the caller drains ``evicted`` and frees those
+    solvers, and ``reused`` tells which admitted requests take an idle one."""
 
     def __init__(self, budget_bytes, max_active=None):
         self.budget = int(budget_bytes)
@@ -145,11 +158,31 @@ class Admission:
         self.queue = collections.deque()
         self.resident = {}     # rid -> bytes
         self.shared = {}       # (n, levels, precision) -> operator bytes
+        self.idle = collections.Counter()   # (n, levels, precision) -> idle solvers
+        self.evicted = []      # kinds whose idle solver the caller must free
+        self.reused = set()    # rids admitted onto an idle solver
         self.peak = 0
+
+    @staticmethod
+    def kind(req):
+        return (req.n, req.levels, req.precision)
 
     @property
     def used(self):
-        return sum(self.resident.values()) + sum(self.shared.values())
+        return (sum(self.resident.values()) + sum(self.shared.values()) +
+                sum(cnt * case_bytes(*k) for k, cnt in self.idle.items()))
+
+    def keep_idle(self, kind):
+        """Charge one more idle solver of `kind` (built before the stream,
+        for instance); False if it does not fit the budget."""
+        extra = 0 if kind in self.shared else operator_bytes(*kind)
+        if self.used + case_bytes(*kind) + extra > self.budget:
+            return False
+        self.idle[kind] += 1
+        if extra:
+            self.shared[kind] = extra
+        self.peak = max(self.peak, self.used)
+        return True
 
     def _extra(self, req):
         key = (req.n, req.levels, req.precision)
@@ -169,19 +202,33 @@ class Admission:
             req = self.queue[0]
             if self.max_active is not None and len(self.resident) >= self.max_active:
                 break
-            extra = self._extra(req)
-            if self.used + req.bytes + extra > self.budget:
-                break
+            kind = self.kind(req)
+            if self.idle[kind] > 0:
+                self.idle[kind] -= 1
+                self.reused.add(req.rid)
+            else:
+                extra = self._extra(req)
+                while self.used + req.bytes + extra > self.budget:
+                    others = [k for k, cnt in self.idle.items() if cnt > 0]
+                    if not others:
+                        break
+                    big = max(others, key=lambda k: case_bytes(*k))
+                    self.idle[big] -= 1
+                    self.evicted.append(big)
+                if self.used + req.bytes + extra > self.budget:
+                    break
+                if extra:
+                    self.shared[kind] = extra
             self.queue.popleft()
             self.resident[req.rid] = req.bytes
-            if extra:
-                self.shared[(req.n, req.levels, req.precision)] = extra
             self.peak = max(self.peak, self.used)
             out.append(req)
         return out
 
-    def release(self, rid):
-        self.resident.pop(rid, None)
+    def release(self, rid, keep=None):
+        """A case left; with `keep` (its kind) its solver stays resident idle."""
+        if self.resident.pop(rid, None) is not None and keep is not None:
+            self.idle[keep] += 1
 
 
 def poisson_stream(count=256, rate=20.0, seed=0, sizes=tuple(range(32, 129, 16)),
@@ -215,22 +262,31 @@ class CavityServer:
         self.keep_fields = keep_fields
         self.results = {}
         self.fields = {}
+        self.pool = {}         # (n, levels, precision) -> idle resident solvers
+        self.built = 0         # solvers constructed (start-up included)
         self.cell_steps = 0
         self.step_batches = 0
         self._nsc = ctypes.sizeof(_abi.WfScalars)
         self._host = torch.empty(4096 * self._nsc, dtype=torch.uint8, pin_memory=True)
 
+    @staticmethod
+    def _cfg(req):
+        return cavity_case(req.n, req.re, req.ulid, levels=req.levels,
+                           precision=req.precision, name="req%d" % req.rid)
+
     def _build(self, req):
-        cfg = cavity_case(req.n, req.re, req.ulid, levels=req.levels,
-                          precision=req.precision, name="req%d" % req.rid)
+        cfg = self._cfg(req)
+        self.built += 1
         return FlowSolver(cfg, build_topology(cfg), self.device,
                           serial=len(self.streams) > 1)
 
     def warmup(self, requests):
         """Server start-up, before the stream's clock runs: build and step
-        once a case of every (N, levels, precision) that `requests` use, so
+        once a solver of every (N, levels, precision) that `requests` use, so
         that the CUDA context, the library's kernels and the shared
-        coarse-level operators are loaded when the first request arrives."""
+        coarse-level operators are loaded when the first request arrives;
+        each such solver stays resident as an idle one for the first request
+        of its kind, as far as the budget allows."""
         seen = set()
         for r in requests:
             key = (r.n, r.levels, r.precision)
@@ -240,8 +296,22 @@ class CavityServer:
             sol = self._build(Request(rid=-1, n=r.n, re=r.re, ulid=r.ulid, n_steps=1,
                                       arrival=0.0, levels=r.levels, precision=r.precision))
             sol.step()
-            sol.close()
+            if self.adm.keep_idle(key):
+                self.pool.setdefault(key, []).append(sol)
+            else:
+                sol.close()
         torch.cuda.synchronize(self.device)
+
+    def _take(self, req):
+        """An idle solver of the request's kind, reset on the device for it."""
+        sol = self.pool[Admission.kind(req)].pop()
+        sol.reset(self._cfg(req))
+        return sol
+
+    def _evict(self):
+        for key in self.adm.evicted:
+            self.pool[key].pop().close()
+        self.adm.evicted.clear()
 
     def run(self, requests, time_scale=1.0):
         """Serve `requests` (arrival times in seconds, compressed by
@@ -260,8 +330,13 @@ class CavityServer:
         try:
             while len(self.results) < total:
                 now = (time.perf_counter() - t0) / time_scale
-                for req in self.adm.admit(now):
-                    building[req.rid] = (req, pool.submit(self._build_on_worker, req), now)
+                admitted = self.adm.admit(now)
+                self._evict()
+                for req in admitted:
+                    if req.rid in self.adm.reused:
+                        live[req.rid] = [req, self._take(req), now, 0]
+                    else:
+                        building[req.rid] = (req, pool.submit(self._build_on_worker, req), now)
                 for rid in [r for r, (_, fut, _) in building.items() if fut.done()]:
                     req, fut, adm_t = building.pop(rid)
                     live[rid] = [req, fut.result(), adm_t, 0]
@@ -326,9 +401,14 @@ class CavityServer:
                                                req.n ** 3, info, err)
                 if self.keep_fields:
                     self.fields[rid] = {k2: sol.f[k2].numpy() for k2 in ("u", "v", "w", "p")}
-                sol.close()
                 del live[rid]
-                self.adm.release(rid)
+                if err:      # a failed case's solver is not reused
+                    sol.close()
+                    self.adm.release(rid)
+                else:        # the solver stays resident for the next request of its kind
+                    kind = Admission.kind(req)
+                    self.pool.setdefault(kind, []).append(sol)
+                    self.adm.release(rid, keep=kind)
 
     def summary(self):
         lat = np.array([c.latency for c in self.results.values()])
@@ -337,4 +417,13 @@ class CavityServer:
                 "p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
                 "mcell_steps_per_s": self.cell_steps / self.wall / 1e6 if self.wall else None,
                 "wall_s": self.wall, "step_batches": self.step_batches,
-                "peak_resident_bytes": self.adm.peak}
+                "peak_resident_bytes": self.adm.peak, "solvers_built": self.built,
+                "solver_reuses": len(self.adm.reused)}
+
+    def close(self):
+        """Free the idle solvers kept for reuse."""
+        for sols in self.pool.values():
+            for sol in sols:
+                sol.close()
+        self.pool.clear()
+        self.adm.idle.clear()

@@ -76,15 +76,8 @@ class FlowSolver:
         self.outer_iters = 0
         self.rmax_trace = []
 
-        s = self._stream()
-        _abi.call("wf_scalars_init", self._sc.data_ptr(), float(self._dt), s)
-        amp = cfg.initial.noise if cfg.initial.type == "rest" else 0.0
-        if amp > 0.0:
-            _abi.call("wf_init_noise", self.f["u"].ptr, self.f["v"].ptr, self.f["w"].ptr,
-                      ni, float(amp), 1, s)
-        self.f["vis"].fill_(self.rey)
         self.case = self._make_case()
-        _abi.call("wf_fill_initial", ctypes.byref(self.case), s)
+        self._init_state()
 
         mode = step_mode or os.environ.get("WF_STEP_MODE", "graph")
         if mode not in STEP_MODES:
@@ -95,6 +88,55 @@ class FlowSolver:
         _abi.call("wf_stepper_create", ctypes.byref(self.case),
                   STEP_MODES[mode] | (STEP_SERIAL if serial else 0),
                   ctypes.byref(self._stepper))
+
+    def _init_state(self):
+        """solver.py:30-83 initial state on the device: scalars (with 1/Re and
+        the lid velocity the step reads), hash noise, vis = 1/Re, initial
+        ghost fills."""
+        cfg, ni = self.cfg, self.n
+        s = self._stream()
+        _abi.call("wf_scalars_init", self._sc.data_ptr(), float(self._dt), float(self.rey),
+                  float(self.ulid), s)
+        amp = cfg.initial.noise if cfg.initial.type == "rest" else 0.0
+        if amp > 0.0:
+            _abi.call("wf_init_noise", self.f["u"].ptr, self.f["v"].ptr, self.f["w"].ptr,
+                      ni, float(amp), 1, s)
+        self.f["vis"].fill_(self.rey)
+        _abi.call("wf_fill_initial", ctypes.byref(self.case), s)
+
+    def reset(self, cfg):
+        """Start over as the case `cfg`, which may differ from this solver's
+        only in its Reynolds number, lid velocity, initial dt and step count:
+        every field is zeroed and re-initialised on the device, and the
+        built step is reused (it reads 1/Re and the lid velocity from the
+        scalar block).  No allocation, no graph capture.  Used by the server
+        to serve a new request from a resident solver of the same size."""
+        same = (cfg.grid, cfg.domain, cfg.numerics, cfg.initial, cfg.physics.sgs_enabled,
+                cfg.physics.sgs_cw, cfg.time.variable_dt, cfg.time.dt_growth,
+                cfg.time.safety_factor)
+        old = (self.cfg.grid, self.cfg.domain, self.cfg.numerics, self.cfg.initial,
+               self.cfg.physics.sgs_enabled, self.cfg.physics.sgs_cw, self.cfg.time.variable_dt,
+               self.cfg.time.dt_growth, self.cfg.time.safety_factor)
+        b, ob = cfg.boundaries, self.cfg.boundaries
+        if same != old or (b.west, b.east, b.south, b.north, b.bottom, b.top) != \
+                (ob.west, ob.east, ob.south, ob.north, ob.bottom, ob.top):
+            raise ValueError("reset: the new case must match this solver's grid, "
+                             "boundaries and numerics")
+        self.cfg = cfg
+        self.rey = 1.0 / cfg.physics.reynolds
+        self.ulid = b.lid_velocity
+        self._dt = cfg.time.dt_init
+        self._ctime = 0.0
+        self.itime = 0
+        self.rmax = 0.0
+        self.cfl = 0.0
+        self.outer_iters = 0
+        self.rmax_trace = []
+        self.case.rrey = self.rey
+        self.case.ulid = float(self.ulid)
+        for f in self.f.values():
+            f.zero_()
+        self._init_state()
 
     # ------------------------------------------------------------------ #
     def _stream(self):
