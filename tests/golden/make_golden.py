@@ -5,7 +5,7 @@ stand-in for NVIDIA Warp and a one-rank mpi4py.
 
 Run once, in a container that has the reference checkout:
 
-    python tests/golden/make_golden.py /path/to/warpflow-les
+    python tests/golden/make_golden.py /path/to/warpflow-les [mg|tecbin]
 
 Writes ``golden_*.npz`` next to this file.  Nothing at test time reads the
 reference; tests only read the committed ``.npz`` files.
@@ -61,9 +61,16 @@ def main():
     if len(sys.argv) not in (2, 3) or not os.path.isdir(os.path.join(sys.argv[1], "warpflow")):
         sys.exit("usage: python tests/golden/make_golden.py <path of the warpflow-les "
                  "source tree, the directory holding warpflow/> [mg]\n"
-                 "  mg: regenerate only the multigrid harness file")
+                 "  mg: regenerate only the multigrid harness file\n"
+                 "  tecbin: regenerate only the Hydro3D exchange file")
     ref = sys.argv[1]
-    only_mg = len(sys.argv) == 3 and sys.argv[2] == "mg"
+    only = sys.argv[2] if len(sys.argv) == 3 else None
+    only_mg = only == "mg"
+    if only == "tecbin":
+        sys.path.insert(0, os.path.join(HERE, "refshim"))
+        sys.path.insert(0, ref)
+        tecbin_golden(ref)
+        return
     sys.path.insert(0, os.path.join(HERE, "refshim"))
     sys.path.insert(0, ref)
     from warpflow.config import load_case
@@ -136,6 +143,42 @@ def main():
         out["phi2_c%d" % c] = mg.levels[2].phi.numpy().copy()
     np.savez_compressed(os.path.join(HERE, "golden_mg16_l3.npz"), **out)
     print("mg16 done", flush=True)
+
+
+def tecbin_golden(ref):
+    """The reference's own Hydro3D exchange (tests/h3d_bridge.py) on an 8^3
+    cavity: the tecbin file its ``export`` writes from a freshly initialised
+    case, the real cells it started from, and what its ``read_tecbin``
+    returns for the file (golden_tecbin_8.npz)."""
+    sys.path.insert(0, os.path.join(ref, "tests"))
+    import h3d_bridge as hb
+    from warpflow import NPL
+    from warpflow.config import load_case
+    from warpflow.solver import FlowSolver
+    from warpflow.topology import build_topology
+
+    tmp = tempfile.mkdtemp()
+    path = os.path.join(tmp, "c8.yaml")
+    with open(path, "w") as fh:
+        fh.write(CASE.format(name="tecbin8", n=8, re=400, sgs="true", noise=0.01,
+                             ulid=1.0, levels=2, steps=1, vdt="true"))
+    hb.export(tmp, case=path)
+    cfg = load_case(path)
+    sol = FlowSolver(cfg, build_topology(cfg), "cpu")
+    n = 8
+    s = slice(NPL, NPL + n)
+    out = {"tecbin": np.fromfile(os.path.join(tmp, "tecbin0000.bin"), np.uint8),
+           "final_ctime": np.array(open(os.path.join(tmp, "final_ctime.dat")).read()),
+           "n": np.array(n), "dx": np.array(sol.dx), "rey": np.array(sol.rey),
+           "ulid": np.array(sol.ulid), "bnd": np.array(list(sol.bnd.items()))}
+    for name in ("u", "v", "w", "p"):
+        out["real_" + name] = sol.f[name].numpy()[s, s, s].copy()
+    for raw in (False, True):
+        got = hb.read_tecbin(os.path.join(tmp, "tecbin0000.bin"), n, raw=raw)
+        for name, a in got.items():
+            out[("raw_" if raw else "core_") + name] = a
+    np.savez_compressed(os.path.join(HERE, "golden_tecbin_8.npz"), **out)
+    print("tecbin done", flush=True)
 
 
 if __name__ == "__main__":
