@@ -84,6 +84,8 @@ typedef struct wf_scalars {
   uint32_t ticket;    /* last-block-done counter */
   int32_t nmg;        /* multigrid solves run in the last step */
   uint32_t gbar[2];   /* grid barrier of the persistent relax (count, generation) */
+  uint32_t bticket;   /* bucket stepping (first case of a bucket): cases reported */
+  int32_t bflags;     /* bucket stepping: OR of the cases' loop decisions */
 } wf_scalars;
 
 /* One cavity case: geometry, physics, numerics and the caller's buffers. */
@@ -127,6 +129,17 @@ WF_API int wf_scalars_init(wf_scalars* sc, double dt0, double rrey, double ulid,
  * half-sweep, 2 cluster with point-to-point halo pushes.  Process-wide;
  * set before graphs are built.  fp32 selects the mixed-precision table. */
 WF_API int wf_set_coarse_strategy(int32_t n, int32_t fp32, int32_t strategy);
+/* Tuning knob (no reference counterpart): the launch shape of a kernel for
+ * size n.  kind 0 = the convection pass (k_conv): a x b threads per CTA, a
+ * along k (a power of two), b along j, a*b a multiple of 32 and <= 256;
+ * default 32 x 8.  kind 1 = the split red-black half-sweep of an n^3 level
+ * (k_rbgs_split): a = cells per thread (1, 2, 4), b = rows per CTA (1, 2,
+ * 4, 8); default 2 x 8.  a = b = 0 restores the default.  Results do not
+ * depend on the shape (each cell's arithmetic is the same).  Process-wide;
+ * read when a launch is issued, so set it before steppers are built.
+ * wf_launch_shape reads the shape in force. */
+WF_API int wf_set_launch_shape(int32_t kind, int32_t n, int32_t a, int32_t b);
+WF_API int wf_launch_shape(int32_t kind, int32_t n, int32_t* a, int32_t* b);
 /* bytes of MG workspace a case needs at each level (caller allocates) */
 WF_API int wf_mg_level_elems(int32_t n, int32_t nlev, int32_t level, int64_t* elems);
 /* No counterpart in the reference.  The coarsest-level relax of a V-cycle
@@ -220,6 +233,14 @@ WF_API int wf_mg_solve_noalloc(const double* su, double* pp, int32_t n, int32_t 
  * device-side wait of its coarse-level kernels gave up (pp is then
  * invalid).  Allocates nothing. */
 WF_API int wf_mg_noalloc_status(void* stream, int32_t* status);
+/* No counterpart in the reference.  wf_mg_solve for `ncases` cases of the
+ * same size and numerics at once: every launch of the solve serves all of
+ * them (grids stacked along z), each case computing what wf_mg_solve
+ * computes for it alone.  `table` is caller-owned device memory of
+ * wf_mg_bucket_table_bytes(ncases) bytes, which receives the cases' buffer
+ * pointers (the call waits for that copy, then enqueues the solve). */
+WF_API int wf_mg_solve_bucket(const wf_case* cases, int32_t ncases, void* table, void* stream);
+WF_API int wf_mg_bucket_table_bytes(int32_t ncases, int64_t* bytes);
 /* multigrid.py:301-322 one V-cycle on an explicit level-0 pair (phi, rhs)
  * of (n+2)^3 doubles each (the standalone harness of tests/test_mg.py). */
 WF_API int wf_mg_vcycle(const wf_case* c, double* phi0, const double* rhs0, void* stream);
@@ -270,11 +291,31 @@ WF_API int wf_stepper_destroy(wf_stepper* s);
  * every case's step (as wf_stepper_create builds it) to a single CUDA graph
  * as independent branches, so the device schedules all cases' kernels
  * concurrently without a stream per case.  `cases` are copied; mode 0 or
- * WF_STEP_SERIAL.  wf_ensemble_step enqueues one step of every case; read
- * each case's scalar block after the stream finishes. */
+ * WF_STEP_SERIAL, optionally | WF_ENS_BUCKETS: cases of the same size and
+ * numerics (any Re and lid velocity; the same shared coarse operator) then
+ * form buckets, and each bucket is ONE branch whose every kernel launch
+ * serves all its cases (grids stacked along z, a device table of the cases'
+ * buffers allocated at creation and freed by wf_ensemble_destroy); the
+ * bucket's projection loop runs while any of its cases' loops does, each
+ * case's multigrid part only while its own loop runs it, so every case
+ * computes what it computes alone.  wf_ensemble_step enqueues one step of
+ * every case; read each case's scalar block after the stream finishes.
+ * wf_ensemble_layout gives the bucket count (the case count without
+ * buckets), each case's bucket (-1 without buckets) and 4 launch counts
+ * per bucket or case (prologue, calmas pass, multigrid part, epilogue).
+ * A bucket holds at most wf_bucket_cap(n, mg_fp32) cases of its size: by
+ * default as many as keep their finest multigrid level within half the L2
+ * below n = 64, and 1 (a branch per case, measured faster there) from 64
+ * on; wf_set_bucket_cap(n, fp32, cap) overrides it per size (cap 0
+ * restores the default; process-wide, read when an ensemble is created). */
+#define WF_ENS_BUCKETS 4
+WF_API int wf_set_bucket_cap(int32_t n, int32_t fp32, int32_t cap);
+WF_API int wf_bucket_cap(int32_t n, int32_t fp32, int32_t* cap);
 typedef struct wf_ensemble wf_ensemble;
 WF_API int wf_ensemble_create(const wf_case* cases, int32_t ncases, int32_t mode,
                               wf_ensemble** out);
+WF_API int wf_ensemble_layout(const wf_ensemble* e, int32_t* nbuckets, int32_t* bucket_of_case,
+                              int32_t* counts);
 WF_API int wf_ensemble_step(wf_ensemble* e, void* stream);
 WF_API int wf_ensemble_destroy(wf_ensemble* e);
 

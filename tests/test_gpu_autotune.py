@@ -16,7 +16,61 @@ def test_autotune_small_sizes(tmp_path):
     p = tmp_path / "tune.json"
     autotune.save(table, p)
     back = autotune.load_and_apply(p)
-    assert back["20"]["best"] == table[20]["best"]
+    assert back["coarse"]["20"]["best"] == table[20]["best"]
+
+
+def test_tune_buckets_installs_faster_form(tmp_path):
+    """The ensemble tuner times a bucket against a branch per case, keeps
+    the faster one per size, and its cache re-installs the same caps."""
+    from warpflow import autotune
+    try:
+        table = autotune.tune_buckets(sizes=(16, 24), ncases=3, reps=2)
+        assert set(table) == {16, 24}
+        for n, rec in table.items():
+            t = rec["ms"]
+            assert rec["cap"] == (3 if t["bucket"] < t["branches"] else 1)
+            assert autotune.bucket_cap(n) == rec["cap"]
+        p = tmp_path / "tune.json"
+        autotune.save({}, p, buckets=table)
+        for n in table:
+            autotune.set_bucket_cap(n, 0)
+        autotune.load_and_apply(p)
+        assert all(autotune.bucket_cap(n) == rec["cap"] for n, rec in table.items())
+    finally:
+        for n in (16, 24):
+            autotune.set_bucket_cap(n, 0)
+
+
+def test_tune_shapes_and_bit_identical_step():
+    """The shape tuner times k_conv and k_rbgs_split shapes at 80^3 (each
+    checked bit-identical to the default), installs the fastest, and a
+    solver built with non-default shapes steps exactly like one built with
+    the defaults."""
+    from warpflow import FlowSolver, autotune, build_topology
+    from warpflow.ensemble import cavity_case
+    try:
+        table = autotune.tune_shapes(sizes=(80,), conv=((32, 8), (16, 16), (64, 4)),
+                                     split=((2, 8), (1, 4), (4, 2)), reps=3)
+        for kind in ("conv", "split"):
+            rec = table[kind][80]
+            assert tuple(autotune.shape(kind, 80)) == tuple(rec["best"])
+            assert min(rec["us"].values()) == rec["us"]["%dx%d" % tuple(rec["best"])]
+        cfg = cavity_case(80, precision="fp64")
+        autotune.set_shape("conv", 80, 16, 16)
+        autotune.set_shape("split", 80, 4, 2)
+        a = FlowSolver(cfg, build_topology(cfg), "cuda:0")
+        autotune.set_shape("conv", 80, 0, 0)
+        autotune.set_shape("split", 80, 0, 0)
+        b = FlowSolver(cfg, build_topology(cfg), "cuda:0")
+        for _ in range(2):
+            assert a.step() == b.step()
+        for name in ("u", "v", "w", "p", "pp", "ustar"):
+            np.testing.assert_array_equal(a.f[name].numpy(), b.f[name].numpy(), err_msg=name)
+        a.close()
+        b.close()
+    finally:
+        autotune.set_shape("conv", 80, 0, 0)
+        autotune.set_shape("split", 80, 0, 0)
 
 
 @pytest.mark.parametrize("n", [8, 12, 16, 20, 24])

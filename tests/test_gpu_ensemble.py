@@ -24,7 +24,7 @@ def _alone(n, re, ulid, steps, precision):
 def test_ensemble_matches_alone(precision, single_graph):
     from warpflow.ensemble import Ensemble, cavity_case
     cfgs = [cavity_case(n, re, u, precision=precision) for n, re, u in SPECS]
-    ens = Ensemble(cfgs, nstreams=3, single_graph=single_graph)
+    ens = Ensemble(cfgs, nstreams=3, single_graph=single_graph, buckets=False)
     assert (ens._graph is not None) == single_graph
     steps = 4
     for _ in range(steps):
@@ -61,6 +61,43 @@ def test_reset_matches_fresh_solver(serial):
         a.reset(cavity_case(32, 700.0, 1.2, precision="mixed"))
 
 
+BUCKET_SPECS = [(16, 150.0, 0.8, 0.01), (24, 900.0, 1.3, 0.01), (16, 600.0, 0.6, 0.05),
+                (24, 300.0, 1.0, 0.002), (16, 950.0, 1.4, 0.02), (32, 400.0, 1.0, 0.01)]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_bucketed_ensemble_matches_alone(precision):
+    """Cases of the same size share every launch of their bucket; each case
+    still computes exactly what it computes alone, step by step, including
+    when cases of one bucket need different numbers of outer iterations."""
+    from warpflow import FlowSolver, build_topology
+    from warpflow.ensemble import Ensemble, cavity_case
+    cfgs = [cavity_case(n, re, u, precision=precision, noise=nz) for n, re, u, nz in BUCKET_SPECS]
+    ens = Ensemble(cfgs, nstreams=2)
+    bucket, counts = ens.layout()
+    assert len(counts) == 3 and bucket[0] == bucket[2] == bucket[4] != bucket[1]
+    alone = [FlowSolver(c, build_topology(c), "cuda:0") for c in cfgs]
+    differing = 0
+    for _ in range(5):
+        infos = ens.step()
+        refs = [s.step() for s in alone]
+        assert infos == refs
+        its = [i["iters"] for i, b in zip(infos, bucket) if b == bucket[0]]
+        differing += len(set(its)) > 1
+    for sol, ref in zip(ens.solvers, alone):
+        for name in ("u", "v", "w", "p", "vis", "su", "pp"):
+            np.testing.assert_array_equal(sol.f[name].numpy(), ref.f[name].numpy(),
+                                          err_msg=name)
+    assert differing >= 1, "no step had cases of one bucket at different iteration counts"
+    # the same step with a branch per case launches every kernel per case
+    per_case = 0
+    for s in ens.solvers:
+        c0, c1, c2, c3 = s.launch_counts()
+        per_case += c0 + c3 + s.outer_iters * c1 + s.last_nmg * c2
+    assert ens.launches_per_step() < per_case
+    ens.close()
+
+
 def test_case_bytes_matches_allocation():
     from warpflow import FlowSolver, build_topology
     from warpflow.ensemble import cavity_case
@@ -93,3 +130,31 @@ def test_server_stream_matches_alone_and_budget():
         _, ref = _alone(r.n, r.re, r.ulid, r.n_steps, r.precision)
         for name in ("u", "v", "w", "p"):
             np.testing.assert_array_equal(srv.fields[r.rid][name], ref[name])
+
+
+def test_bucket_with_cluster_coarse_sweeps():
+    """A bucket whose coarsest level relaxes by sweeps at a size where a
+    lone case would use a thread-block-cluster kernel (24^3: cluster
+    kernels cannot serve a bucket's case table) falls back to the one-CTA
+    kernel: the bucket is built and each case agrees with its lone run to
+    rounding (a different sweep kernel, the same sweeps)."""
+    from warpflow import FlowSolver, build_topology
+    from warpflow.ensemble import Ensemble, cavity_case
+    cfgs = []
+    for re in (200.0, 500.0, 800.0):
+        c = cavity_case(48, re, 1.0, levels=2, precision="fp64")
+        c.numerics.mg_coarse = "sweeps"
+        cfgs.append(c)
+    ens = Ensemble(cfgs, nstreams=1)
+    bucket, counts = ens.layout()
+    assert len(counts) == 1 and bucket == [0, 0, 0]
+    alone = [FlowSolver(c, build_topology(c), "cuda:0") for c in cfgs]
+    for _ in range(2):
+        infos = ens.step()
+        refs = [s.step() for s in alone]
+        assert [i["iters"] for i in infos] == [r["iters"] for r in refs]
+    for sol, ref in zip(ens.solvers, alone):
+        for name in ("u", "v", "w", "p"):
+            a, b = sol.f[name].numpy(), ref.f[name].numpy()
+            assert np.abs(a - b).max() <= 1e-10 * max(1.0, np.abs(b).max()), name
+    ens.close()

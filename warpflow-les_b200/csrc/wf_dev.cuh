@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "wf_internal.h"
+
 namespace wf {
 
 // Programmatic dependent launch: every kernel of this library starts by
@@ -21,6 +23,27 @@ namespace wf {
 __device__ __forceinline__ void pdl_entry() {
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+// ---- bucket batching (see Batch in wf_internal.h) -------------------------
+// the case of this block, its z index within the case's grid, the case's z
+// extent; a case's buffers
+__device__ __forceinline__ int bt_case(const Batch& b) {
+  return b.tab ? (int)(blockIdx.z / (unsigned)b.nz) : 0;
+}
+__device__ __forceinline__ int bt_z(const Batch& b) {
+  return b.tab ? (int)(blockIdx.z % (unsigned)b.nz) : (int)blockIdx.z;
+}
+__device__ __forceinline__ int bt_gz(const Batch& b) { return b.tab ? b.nz : (int)gridDim.z; }
+__device__ __forceinline__ double* bt_fld(const wf_case& c, const Batch& b, int f) {
+  return b.tab ? b.tab[bt_case(b)].fld[f] : c.fld[f];
+}
+__device__ __forceinline__ wf_scalars* bt_sc(const wf_case& c, const Batch& b) {
+  return b.tab ? b.tab[bt_case(b)].sc : c.sc;
+}
+// true when this block's case does not take part in the launch
+__device__ __forceinline__ bool bt_skip(const Batch& b) {
+  return b.tab && b.skip && !(b.tab[bt_case(b)].sc->loop & b.skip);
 }
 
 __device__ __forceinline__ unsigned long long dbits(double x) {
@@ -78,15 +101,16 @@ __device__ __forceinline__ double block_min(double v, double* sm, double ident) 
   return sm[0];
 }
 
-// "last block done": returns true in exactly one block, after every other
-// block's preceding global writes are visible; resets the ticket.
-__device__ __forceinline__ bool last_block(unsigned int* ticket) {
+// "last block done" among `count` blocks: returns true in exactly one block,
+// after every other block's preceding global writes are visible; resets the
+// ticket.
+__device__ __forceinline__ bool last_block(unsigned int* ticket, unsigned count) {
   __shared__ bool is_last;
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
     const unsigned int t = atomicAdd(ticket, 1u);
-    is_last = (t == gridDim.x * gridDim.y * gridDim.z - 1);
+    is_last = (t == count - 1);
     if (is_last) {
       __threadfence();
       *ticket = 0u;

@@ -25,6 +25,7 @@ constexpr int MAX_JOBS = 3;
 
 struct PhaseJob {
   double* fld;
+  int fid, vsrc;   // bucket launches: the field's slot, the source of valp (1 ulid, 2 rrey)
   int nops;
   FaceOp ops[MAX_OPS_PER_PHASE];
 };
@@ -36,16 +37,23 @@ struct PhaseArgs {
   int P;  // padded extent n + 6
 };
 
-__global__ void k_fill_phase(const PhaseArgs args) {
+__global__ void k_fill_phase(const PhaseArgs args, const Batch bt) {
   pdl_entry();
+  if (bt_skip(bt)) return;
   // b (k for x/y faces) is the fast lane index so stores coalesce
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   const int a = blockIdx.y * blockDim.y + threadIdx.y;
-  const int jb = blockIdx.z;
+  const int jb = bt_z(bt);
   if (jb >= args.njob) return;
   const PhaseJob& J = args.job[jb];
   const long P = args.P;
   double* f = J.fld;
+  const double* valp = nullptr;
+  if (bt.tab) {
+    const CasePtrs& cp = bt.tab[bt_case(bt)];
+    f = cp.fld[J.fid];
+    valp = J.vsrc == 1 ? &cp.sc->ulid : (J.vsrc == 2 ? &cp.sc->rrey : nullptr);
+  }
   for (int o = 0; o < J.nops; ++o) {
     const FaceOp& op = J.ops[o];
     if (a >= op.na || b >= op.nb) continue;
@@ -71,7 +79,7 @@ __global__ void k_fill_phase(const PhaseArgs args) {
         }
         f[gi] = op.val * f[si];
       } else {
-        f[gi] = op.valp ? *op.valp : op.val;
+        f[gi] = op.valp ? *(valp ? valp : op.valp) : op.val;
       }
     }
   }
@@ -165,7 +173,11 @@ int launch_fills(const FillReq* reqs, int nreq, int n, cudaStream_t s) {
     a.amax = a.bmax = 0;
     for (int r = 0; r < nreq; ++r) {
       if (!reqs[r].fld) return fail(WF_EINVAL, "launch_fills: null field");
+      if (batch_ctx().tab && reqs[r].fid < 0)
+        return fail(WF_EUNSUPPORTED, "launch_fills: a bucket fill needs field slots");
       a.job[r].fld = reqs[r].fld;
+      a.job[r].fid = reqs[r].fid;
+      a.job[r].vsrc = reqs[r].vsrc;
       a.job[r].nops = program(reqs[r].kind, n, reqs[r].val, reqs[r].valp, phase, a.job[r].ops);
       for (int o = 0; o < a.job[r].nops; ++o) {
         a.amax = a.job[r].ops[o].na > a.amax ? a.job[r].ops[o].na : a.amax;

@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string>
+#include <tuple>
+#include <type_traits>
 
 #include "warpflow_b200.h"
 
@@ -46,8 +48,54 @@ bool pdl_enabled();
 inline dim3 cells3(int ni, int nj, int nk) { return dim3((nk + 31) / 32, (nj + 7) / 8, ni); }
 inline dim3 cell_block() { return dim3(32, 8); }
 
+// ---- bucket batching ------------------------------------------------------
+// A bucket is a set of cases of the same size and numerics stepped together:
+// one launch of a kernel serves every case of the bucket.  The cases differ
+// only in their buffers (1/Re and the lid velocity live in each case's
+// scalar block), so a launch carries the first case's arguments and a device
+// table of every case's buffers; a kernel takes its case from blockIdx.z
+// (grid z = cases x the single case's z extent) and rebuilds its pointers
+// from that case's row.
+struct CasePtrs {
+  double* fld[WF_NFIELDS];
+  wf_scalars* sc;
+  void* mg_phi[WF_MAX_LEVELS];
+  void* mg_rhs[WF_MAX_LEVELS];
+  void* mg_tmp[WF_MAX_LEVELS];
+  void* mg_cop_part;
+};
+
+// the batch argument every bucket-capable kernel takes last: tab null = one
+// case; nz = the single case's grid z extent; skip = a bit of wf_scalars.loop
+// a case must have set for the launch to work on it (0: every case)
+struct Batch {
+  const CasePtrs* tab;
+  int nz;
+  int skip;
+};
+
+// the bucket the calling thread is building launches for (tab null: none)
+struct BatchCtx {
+  const CasePtrs* tab = nullptr;
+  int ncases = 1;
+  int skip = 0;
+};
+BatchCtx& batch_ctx();
+
+template <typename... E>
+constexpr bool takes_batch() {
+  if constexpr (sizeof...(E) == 0) {
+    return false;
+  } else {
+    return std::is_same<typename std::tuple_element<sizeof...(E) - 1, std::tuple<E...>>::type,
+                        Batch>::value;
+  }
+}
+
 // launch a kernel of this library, with the programmatic-serialization
-// attribute when enabled and an optional cluster shape
+// attribute when enabled.  A kernel whose last parameter is a Batch gets the
+// calling thread's bucket (grid z multiplied by its case count); any other
+// kernel refuses to launch while a bucket is being built.
 template <typename... ExpTypes, typename... ActTypes>
 inline cudaError_t launch_k(void (*kernel)(ExpTypes...), dim3 grid, dim3 block, size_t smem,
                             cudaStream_t s, ActTypes&&... args) {
@@ -65,7 +113,15 @@ inline cudaError_t launch_k(void (*kernel)(ExpTypes...), dim3 grid, dim3 block, 
   }
   cfg.attrs = at;
   cfg.numAttrs = na;
-  return cudaLaunchKernelEx(&cfg, kernel, static_cast<ActTypes&&>(args)...);
+  const BatchCtx& bc = batch_ctx();
+  if constexpr (takes_batch<ExpTypes...>()) {
+    Batch b{bc.tab, (int)grid.z, bc.skip};
+    if (bc.tab) cfg.gridDim.z = grid.z * (unsigned)bc.ncases;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<ActTypes&&>(args)..., b);
+  } else {
+    if (bc.tab) return cudaErrorNotSupported;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<ActTypes&&>(args)...);
+  }
 }
 
 int validate_case(const wf_case& c);
@@ -77,6 +133,8 @@ struct FillReq {
   int kind;
   double val;               // ulid for u, 1/Re for vis
   const double* valp = nullptr;  // the same value read on the device, when set
+  int fid = -1;             // the field's slot (enum wf_field), for bucket launches
+  int vsrc = 0;             // valp in the scalar block: 1 ulid, 2 rrey (bucket launches)
 };
 // up to 3 independent field fills, executed as 3 ordered axis phases
 int launch_fills(const FillReq* reqs, int nreq, int n, cudaStream_t s);
@@ -97,6 +155,15 @@ int launch_calmas(const wf_case& c, unsigned long long h_if,
                   unsigned long long h_loop, cudaStream_t s);
 int launch_add_ring(double* p, const double* pp, int n, cudaStream_t s);
 int launch_scalars_init(wf_scalars* sc, double dt0, double rrey, double ulid, cudaStream_t s);
+
+// ---- launch shapes chosen per size --------------------------------------
+// kind SHAPE_CONV: k_conv's CTA, a = extent along k (x), b = along j (y);
+// kind SHAPE_SPLIT: k_rbgs_split, a = cells per thread, b = rows per CTA.
+// Process-wide, read when a launch is issued (a graph keeps the shapes it
+// was captured with); set by wf_set_launch_shape (the autotuner).
+constexpr int SHAPE_CONV = 0, SHAPE_SPLIT = 1;
+void launch_shape(int kind, int n, int* a, int* b);
+int set_launch_shape(int kind, int n, int a, int b);
 
 // ---- multigrid -----------------------------------------------------------
 int mg_solve(const wf_case& c, cudaStream_t s);

@@ -45,7 +45,41 @@ struct Lvl {
   long tI, tJ;   // its strides
   unsigned* gbar;  // two words of grid-barrier state (may be null)
   int split = 0;   // phi/rhs stored row-parity split (see k_rbgs_split)
+  // where the level's arrays sit in a case's buffers, so that a bucket launch
+  // can find them for every case: bits 0-3 the level; LV_PP the FP64 level 0
+  // inside pp (phi) and su (rhs); LV_SPLIT the split copies in mg_tmp;
+  // otherwise mg_phi / mg_rhs of the level
+  int role = 0;
 };
+constexpr int LV_PP = 16, LV_SPLIT = 32;
+
+// the level L of the case this block serves in a bucket launch (L itself
+// outside one)
+template <class T>
+__device__ __forceinline__ Lvl<T> rebase(const Lvl<T>& L, const Batch& bt) {
+  if (!bt.tab) return L;
+  const CasePtrs& cp = bt.tab[bt_case(bt)];
+  Lvl<T> R = L;
+  const int l = L.role & 15;
+  const long m = (long)L.n + 2;
+  T* tmp = (T*)cp.mg_tmp[l];
+  if (L.role & LV_SPLIT) {
+    R.phi = tmp;
+    R.rhs = tmp + m * m * m;
+  } else if (L.role & LV_PP) {
+    const long P = (long)L.n + 2 * NPL;
+    const long off = (long)(NPL - 1) * (P * P + P + 1);
+    R.phi = (T*)(cp.fld[WF_PP] + off);
+    R.rhs = (const T*)(cp.fld[WF_SU] + off);
+  } else {
+    R.phi = (T*)cp.mg_phi[l];
+    R.rhs = (const T*)cp.mg_rhs[l];
+  }
+  R.tmp = tmp;
+  R.err = &cp.sc->status;
+  R.gbar = cp.sc->gbar;
+  return R;
+}
 
 // position of array index a within a row of the row-parity-split layout
 __host__ __device__ __forceinline__ int spos(int a, int H) { return (a & 1) * H + (a >> 1); }
@@ -95,8 +129,10 @@ static ApRecip<T> ap_recip(const Lvl<T>& L) {
 
 // one colour half-sweep (multigrid.py:70-90): update where (i+j+k+color)%2==1
 template <class T>
-__global__ void __launch_bounds__(MG_TPB) k_rbgs(const Lvl<T> L, int color) {
+__global__ void __launch_bounds__(MG_TPB) k_rbgs(const Lvl<T> L0, int color, const Batch bt) {
   pdl_entry();
+  if (bt_skip(bt)) return;
+  const Lvl<T> L = rebase(L0, bt);
   const int n = L.n;
   const int nh = (n + 1) >> 1;
   {  // one thread per cell: x = kk (runs of 32), y = j (groups of 8), z = i
@@ -104,7 +140,7 @@ __global__ void __launch_bounds__(MG_TPB) k_rbgs(const Lvl<T> L, int color) {
     if (kx_ >= nh || jy_ >= n) return;
     const int kk = kx_;
     const int j = jy_;
-    const int i = (int)blockIdx.z;
+    const int i = bt_z(bt);
     const int k = 2 * kk + ((1 + i + j + color) & 1);
     if (k >= n) return;
     const long c = lid(L, i + 1, j + 1, k + 1);
@@ -124,15 +160,20 @@ __global__ void __launch_bounds__(MG_TPB) k_rbgs(const Lvl<T> L, int color) {
 // restriction (multigrid.py:93-119): rhs_c = 1/8 sum of the 8 fine residuals;
 // also zeroes the coarse level's phi, ring included
 template <class T>
-__global__ void __launch_bounds__(MG_TPB) k_restrict(const Lvl<T> F, T* rhs_c, Lvl<T> C) {
+__global__ void __launch_bounds__(MG_TPB) k_restrict(const Lvl<T> F0, T* rhs_c, Lvl<T> C0,
+                                                     const Batch bt) {
   pdl_entry();
+  if (bt_skip(bt)) return;
+  const Lvl<T> F = rebase(F0, bt);
+  const Lvl<T> C = rebase(C0, bt);
+  if (bt.tab) rhs_c = const_cast<T*>(C.rhs);
   const int nc = C.n, n = F.n;
   {  // one thread per cell: x = ck (runs of 32), y = cj (groups of 8), z = ci
     const int kx_ = blockIdx.x * 32 + threadIdx.x, jy_ = blockIdx.y * 8 + threadIdx.y;
     if (kx_ >= nc || jy_ >= nc) return;
     const int ck = kx_;
     const int cj = jy_;
-    const int ci = (int)blockIdx.z;
+    const int ci = bt_z(bt);
     // the fine phi values the 8 residuals read -- the 2x2x2 block and its
     // face neighbours, P[a][b][c] at fine cell (2ci-1+a, 2cj-1+b, 2ck-1+c)
     // -- each loaded once (32 loads instead of 56)
@@ -184,10 +225,12 @@ __global__ void __launch_bounds__(MG_TPB) k_restrict(const Lvl<T> F, T* rhs_c, L
   }
 }
 
-// zero a whole (n+2)^3 ring-layout level array
+// zero a whole array (in a bucket launch: field slot `fid` of every case)
 template <class T>
-__global__ void k_zero(T* a, long cnt) {
+__global__ void k_zero(T* a, long cnt, int fid, const Batch bt) {
   pdl_entry();
+  if (bt_skip(bt)) return;
+  if (bt.tab) a = (T*)bt.tab[bt_case(bt)].fld[fid];
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < cnt;
        t += (long)gridDim.x * blockDim.x)
     a[t] = T(0);
@@ -209,15 +252,18 @@ __global__ void k_zero_strided(T* a, int m, long sI, long sJ) {
 
 // prolongation (multigrid.py:122-146) + the ring refill that follows it
 template <class T>
-__global__ void __launch_bounds__(MG_TPB) k_prolong(const Lvl<T> C, Lvl<T> F) {
+__global__ void __launch_bounds__(MG_TPB) k_prolong(const Lvl<T> C0, Lvl<T> F0, const Batch bt) {
   pdl_entry();
+  if (bt_skip(bt)) return;
+  const Lvl<T> C = rebase(C0, bt);
+  const Lvl<T> F = rebase(F0, bt);
   const int n = F.n;
   {  // one thread per cell: x = k (runs of 32), y = j (groups of 8), z = i
     const int kx_ = blockIdx.x * 32 + threadIdx.x, jy_ = blockIdx.y * 8 + threadIdx.y;
     if (kx_ >= n || jy_ >= n) return;
     const int k = kx_;
     const int j = jy_;
-    const int i = (int)blockIdx.z;
+    const int i = bt_z(bt);
     const int c0x = (i % 2 == 0) ? i / 2 - 1 : i / 2;
     const T wx0 = (i % 2 == 0) ? T(0.25) : T(0.75);
     const int c0y = (j % 2 == 0) ? j / 2 - 1 : j / 2;
@@ -250,12 +296,15 @@ __global__ void __launch_bounds__(MG_TPB) k_prolong(const Lvl<T> C, Lvl<T> F) {
 // for 8 outputs instead of 64); every output sums the same terms in the
 // same order as k_prolong, so the results are the same bits
 template <class T>
-__global__ void __launch_bounds__(MG_TPB) k_prolong8(const Lvl<T> C, Lvl<T> F) {
+__global__ void __launch_bounds__(MG_TPB) k_prolong8(const Lvl<T> C0, Lvl<T> F0, const Batch bt) {
   pdl_entry();
+  if (bt_skip(bt)) return;
+  const Lvl<T> C = rebase(C0, bt);
+  const Lvl<T> F = rebase(F0, bt);
   const int nc = C.n;
   const int ck = blockIdx.x * 32 + threadIdx.x, cj = blockIdx.y * 8 + threadIdx.y;
   if (ck >= nc || cj >= nc) return;
-  const int ci = (int)blockIdx.z;
+  const int ci = bt_z(bt);
   const int Hc = (nc + 2) >> 1;
   long kq[3];
 #pragma unroll
@@ -304,8 +353,10 @@ __global__ void __launch_bounds__(MG_TPB) k_prolong8(const Lvl<T> C, Lvl<T> F) {
 // ring is not needed there because every ring term has a zero coefficient.
 // After the last sweep the interior and the face rings go back to global.
 template <class T>
-__global__ void __launch_bounds__(1024) k_relax_smem(Lvl<T> L, int nsweeps) {
+__global__ void __launch_bounds__(1024) k_relax_smem(Lvl<T> L0, int nsweeps, const Batch bt) {
   pdl_entry();
+  if (bt_skip(bt)) return;
+  const Lvl<T> L = rebase(L0, bt);
   extern __shared__ __align__(16) unsigned char smraw[];
   T* sphi = reinterpret_cast<T*>(smraw);
   const int n = L.n;
@@ -414,11 +465,14 @@ struct CoarseShape {
 // even-parity cells of the result as row b of unit_out (position = cell
 // index / 2): the rows of the coarse-level operator.
 template <class T, int NC, bool RHS_SMEM>
-__global__ void __launch_bounds__(CoarseShape<NC>::THREADS) k_coarse_cols(Lvl<T> L,
+__global__ void __launch_bounds__(CoarseShape<NC>::THREADS) k_coarse_cols(Lvl<T> L0,
                                                                            int nsweeps,
                                                                            T* unit_out,
-                                                                           const int* unit_ids) {
+                                                                           const int* unit_ids,
+                                                                           const Batch bt) {
   pdl_entry();
+  if (bt_skip(bt)) return;
+  const Lvl<T> L = rebase(L0, bt);
   constexpr int H = NC / 2;
   constexpr int HALF = NC * H;                  // columns per parity
   constexpr int GROUP = ((HALF + 31) / 32) * 32;
@@ -647,6 +701,7 @@ __global__ void __launch_bounds__(ClusterShape<NC, NCL>::THREADS)
 
 template <class T, int NC, int NCL>
 static int launch_coarse_cluster(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
+  if (batch_ctx().tab) return fail(WF_EUNSUPPORTED, "cluster and cooperative relaxes do not run in a bucket");
   using S = ClusterShape<NC, NCL>;
   const size_t sb = 2ull * NC * S::PL * sizeof(T);
   auto kern = k_coarse_cluster<T, NC, NCL>;
@@ -880,6 +935,7 @@ __global__ void __launch_bounds__(ClusterShape<NC, NCL>::THREADS)
 
 template <class T, int NC, int NCL>
 static int launch_coarse_p2p(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
+  if (batch_ctx().tab) return fail(WF_EUNSUPPORTED, "cluster and cooperative relaxes do not run in a bucket");
   using S = ClusterShape<NC, NCL>;
   const size_t sb = 2ull * NC * S::PL * sizeof(T);
   auto kern = k_coarse_p2p<T, NC, NCL>;
@@ -1149,6 +1205,7 @@ __global__ void __launch_bounds__(TbShape<NC, NCL>::THREADS)
 
 template <class T, int NC, int NCL>
 static int launch_coarse_tb(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
+  if (batch_ctx().tab) return fail(WF_EUNSUPPORTED, "cluster and cooperative relaxes do not run in a bucket");
   using S = TbShape<NC, NCL>;
   const size_t sb = (2ull * NC * S::PL + 4ull * S::SIDE) * sizeof(T);
   auto kern = k_coarse_tb<T, NC, NCL>;
@@ -1207,13 +1264,15 @@ static int try_coarse_tb(const Lvl<T>& L, int nsweeps, cudaStream_t s, int* rc) 
 // (S[g r, w] = S[r, g^-1 w] = S[g^-1 w, r]).  Only the representative
 // columns are stored (about N/48 of the (N/2)^2 entries of S, N = n^3:
 // 5.8 MB instead of 128 MB at 20^3), built like the full map was (one CTA
-// of the column kernel per representative, unit rhs), and the product runs
-// from shared memory: one CTA per representative holds v_B and its column
-// and forms the outputs of its orbit, each a dot product summed in a fixed
-// order (per thread over its cells, a warp butterfly, the warps in order),
-// so results do not depend on scheduling and a case computes the same bits
-// alone or beside other cases.  The stored columns equal the mathematical
-// S to rounding, so the relax agrees with the sweeps to rounding.
+// of the column kernel per representative, unit rhs).  The product is a
+// small GEMM: with the permuted copies V[g][u] = v_B[g(u)] (k_cop_vg),
+// Y[r][g] = sum_u C[r][u] V[g][u] over slices of u (k_cop_gemm), and
+// x_B[g(r)] = the slices of Y[r][g] added in order (k_cop_out).  Every sum
+// runs in a fixed order (per lane over its cells, a lane butterfly, the
+// slices in order), so results do not depend on scheduling and a case
+// computes the same bits alone or beside other cases.  The stored columns
+// equal the mathematical S to rounding, so the relax agrees with the
+// sweeps to rounding.
 constexpr int COP_GMAX = 24;
 
 static bool cop_size_ok(int nc) {
@@ -1364,9 +1423,13 @@ __device__ __forceinline__ T first_sweep_v(const Lvl<T>& L, int i, int j, int k)
 // B, U: one division each), thread 0 adds them in that order, and the eight
 // threads then store the copies (g = t, t+8, t+16)
 template <class T>
-__global__ void __launch_bounds__(256) k_cop_vg(const Lvl<T> L, T* V,
-                                                const __grid_constant__ CopSyms G) {
+__global__ void __launch_bounds__(256) k_cop_vg(const Lvl<T> L0, T* V,
+                                                const __grid_constant__ CopSyms G,
+                                                const Batch bt) {
   pdl_entry();
+  if (bt_skip(bt)) return;
+  const Lvl<T> L = rebase(L0, bt);
+  if (bt.tab) V = (T*)bt.tab[bt_case(bt)].mg_cop_part;
   const int n = L.n, M = n * n * n / 2;
   const int t = threadIdx.x & 7;
   const int w = blockIdx.x * 32 + (threadIdx.x >> 3);
@@ -1416,8 +1479,13 @@ template <> struct Vec2<float> { using type = float2; };
 // then the lanes are added by a butterfly (fixed order)
 template <class T>
 __global__ void __launch_bounds__(256) k_cop_gemm(const T* C, const T* V, T* Y, int nrep,
-                                                  int M, int ng) {
+                                                  int M, int ng, const Batch bt) {
   pdl_entry();
+  if (bt_skip(bt)) return;
+  if (bt.tab) {
+    V = (const T*)bt.tab[bt_case(bt)].mg_cop_part;
+    Y = (T*)bt.tab[bt_case(bt)].mg_cop_part + (long)COP_GMAX * M;
+  }
   using V2 = typename Vec2<T>::type;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int x0 = blockIdx.x * COP_RB, s = blockIdx.y;
@@ -1477,9 +1545,12 @@ __global__ void __launch_bounds__(256) k_cop_gemm(const T* C, const T* V, T* Y, 
 // closing sweep overwrites it first)
 template <class T>
 __global__ void __launch_bounds__(256) k_cop_out(const T* Y, const int* prod, int nrep,
-                                                 Lvl<T> L) {
+                                                 Lvl<T> L0, const Batch bt) {
   pdl_entry();
+  if (bt_skip(bt)) return;
+  const Lvl<T> L = rebase(L0, bt);
   const int n = L.n, M = n * n * n / 2;
+  if (bt.tab) Y = (const T*)bt.tab[bt_case(bt)].mg_cop_part + (long)COP_GMAX * M;
   const int o = blockIdx.x * 256 + threadIdx.x;
   if (o >= M) return;
   const int pv = prod[o];
@@ -1614,8 +1685,14 @@ constexpr int SPLIT_ROWS = 8;  // rows (one warp each) per CTA
 // level phi (all (n+2)^3 cells) and rhs -> split copies sp, sr (dense strides)
 template <class T>
 __global__ void __launch_bounds__(32 * SPLIT_ROWS)
-    k_split_in(const Lvl<T> L, T* sp, T* sr, int with_rhs) {
+    k_split_in(const Lvl<T> L0, T* sp, T* sr, int with_rhs, const Batch bt) {
   pdl_entry();
+  if (bt_skip(bt)) return;
+  const Lvl<T> L = rebase(L0, bt);
+  if (bt.tab) {
+    sp = L.tmp;
+    sr = L.tmp + (long)(L.n + 2) * (L.n + 2) * (L.n + 2);
+  }
   const int m = L.n + 2, H = m >> 1;
   const int row = blockIdx.x * SPLIT_ROWS + (threadIdx.x >> 5);
   if (row >= m * m) return;
@@ -1631,18 +1708,24 @@ __global__ void __launch_bounds__(32 * SPLIT_ROWS)
 
 // one colour half-sweep on the split copy: a warp updates CPT runs of 32
 // consecutive cells of one colour in one real row (cells h, h+32, ...); grid
-// x = chunk of 32*CPT cells of the half-row, y = group of SPLIT_ROWS rows j,
-// z = plane i.  All loads of a thread come before its stores: a half-sweep
+// x = chunk of 32*CPT cells of the half-row, y = group of blockDim.y rows j
+// (at most SPLIT_ROWS; CPT and the rows are chosen per size), z = plane i.  All loads of a thread come before its stores: a half-sweep
 // reads only the other colour and rhs, which it does not write.
 template <class T, int CPT>
 __global__ void __launch_bounds__(32 * SPLIT_ROWS)
-    k_rbgs_split(const Lvl<T> L, T* sp, const T* sr, int color,
-                 const __grid_constant__ ApRecip<T> rt) {
+    k_rbgs_split(const Lvl<T> L0, T* sp, const T* sr, int color,
+                 const __grid_constant__ ApRecip<T> rt, const Batch bt) {
   pdl_entry();
+  if (bt_skip(bt)) return;
+  const Lvl<T> L = rebase(L0, bt);
+  if (bt.tab) {
+    sp = L.tmp;
+    sr = L.tmp + (long)(L.n + 2) * (L.n + 2) * (L.n + 2);
+  }
   const int n = L.n, nh = n >> 1;
   const int h0 = blockIdx.x * 32 * CPT + threadIdx.x;
-  const int j = blockIdx.y * SPLIT_ROWS + threadIdx.y;
-  const int i = blockIdx.z;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = bt_z(bt);
   if (j >= n || h0 >= nh) return;
   const int H = (n + 2) >> 1, tI = (int)L.tI, tJ = (int)L.tJ;
   const int pr = (i + j + color) & 1;       // parity of a = k+1 of this row's colour
@@ -1678,22 +1761,14 @@ __global__ void __launch_bounds__(32 * SPLIT_ROWS)
   }
 }
 
-// cells per thread of the split half-sweep (WF_SPLIT_CPT = 1, 2 or 4 overrides)
-static int split_cpt() {
-  static int v = -1;
-  if (v < 0) {
-    const char* e = getenv("WF_SPLIT_CPT");
-    v = e ? atoi(e) : 2;
-    if (v != 1 && v != 2 && v != 4) v = 2;
-  }
-  return v;
-}
-
 // split copy -> real cells of the level and their face-ring mirrors
 template <class T>
 __global__ void __launch_bounds__(32 * SPLIT_ROWS)
-    k_split_out(const Lvl<T> L, const T* sp) {
+    k_split_out(const Lvl<T> L0, const T* sp, const Batch bt) {
   pdl_entry();
+  if (bt_skip(bt)) return;
+  const Lvl<T> L = rebase(L0, bt);
+  if (bt.tab) sp = L.tmp;
   const int n = L.n, H = (n + 2) >> 1;
   const int row = blockIdx.x * SPLIT_ROWS + (threadIdx.x >> 5);
   if (row >= n * n) return;
@@ -1737,14 +1812,14 @@ static int split_sweeps(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
   const int m = L.n + 2;
   T* sp = L.tmp;
   const T* sr = L.tmp + (long)m * m * m;
-  const int cpt = split_cpt();
-  const dim3 grid((L.n / 2 + 32 * cpt - 1) / (32 * cpt), (L.n + SPLIT_ROWS - 1) / SPLIT_ROWS,
-                  L.n);
+  int cpt, rows;
+  launch_shape(SHAPE_SPLIT, L.n, &cpt, &rows);   // cpt in {1, 2, 4}, rows <= SPLIT_ROWS
+  const dim3 grid((L.n / 2 + 32 * cpt - 1) / (32 * cpt), (L.n + rows - 1) / rows, L.n);
   const ApRecip<T> rt = ap_recip(L);
   auto kern = cpt == 4 ? k_rbgs_split<T, 4> : cpt == 2 ? k_rbgs_split<T, 2> : k_rbgs_split<T, 1>;
   for (int it = 0; it < nsweeps; ++it) {
     for (int color = 0; color < 2; ++color) {
-      WF_CK(launch_k(kern, grid, dim3(32, SPLIT_ROWS), 0, s, L, sp, sr, color, rt));
+      WF_CK(launch_k(kern, grid, dim3(32, rows), 0, s, L, sp, sr, color, rt));
       WF_CKL("k_rbgs_split");
     }
   }
@@ -1776,6 +1851,7 @@ static int relax_split(const Lvl<T>& L, int nsweeps, bool rhs_ready, cudaStream_
 template <class T>
 static Lvl<T> split_view(const Lvl<T>& L) {
   Lvl<T> V = L;
+  V.role = L.role | LV_SPLIT;
   const long m = (long)L.n + 2;
   V.phi = L.tmp;
   V.rhs = L.tmp + m * m * m;
@@ -1788,8 +1864,10 @@ static Lvl<T> split_view(const Lvl<T>& L) {
 // face-ring mirrors of a split view (what k_rbgs leaves in the ring; the
 // prolongation out of this level reads them)
 template <class T>
-__global__ void __launch_bounds__(256) k_split_ring(const Lvl<T> V) {
+__global__ void __launch_bounds__(256) k_split_ring(const Lvl<T> V0, const Batch bt) {
   pdl_entry();
+  if (bt_skip(bt)) return;
+  const Lvl<T> V = rebase(V0, bt);
   const int n = V.n;
   const int t = blockIdx.x * 256 + threadIdx.x;
   if (t >= 6 * n * n) return;
@@ -2072,6 +2150,7 @@ __global__ void __launch_bounds__(MG_TPB) k_relax_persist(const Lvl<T> L, int ns
 
 template <class T>
 static int launch_relax_persist(const Lvl<T>& L, int nsweeps, cudaStream_t s, bool* done) {
+  if (batch_ctx().tab) return fail(WF_EUNSUPPORTED, "cluster and cooperative relaxes do not run in a bucket");
   *done = false;
   static int blocks_per_sm[2] = {-1, -1};
   int& bps = blocks_per_sm[sizeof(T) == 4 ? 1 : 0];
@@ -2175,7 +2254,7 @@ __global__ void k_resmax(const Lvl<double> L, double* out, unsigned int* ticket,
   }
   m = block_max(m, sm);
   if (threadIdx.x == 0) atomicMax(acc, okey(m));
-  if (!last_block(ticket)) return;
+  if (!last_block(ticket, gridDim.x * gridDim.y * gridDim.z)) return;
   if (threadIdx.x == 0) {
     *out = okey_inv(atomicAdd(acc, 0ull));
     *acc = okey(0.0);
@@ -2203,11 +2282,15 @@ constexpr size_t SMEM_CAP = 220 * 1024;
 template <class T>
 static int relax(const Lvl<T>& L, int nsweeps, cudaStream_t s, bool rhs_ready = false) {
   if (nsweeps <= 0) return WF_OK;
+  // a bucket launch serves many cases through their table: only kernels that
+  // take one (the one-CTA column kernel, split and plain sweeps, the
+  // shared-memory relax) run there
+  const bool bucket = batch_ctx().tab != nullptr;
   // small levels with many sweeps: the column kernel
   if (nsweeps > 12 || L.n <= 24) {
     // small levels: one CTA, or a cluster when there are many sweeps
     int rc = WF_OK;
-    const int strat = coarse_strategy(L.n, sizeof(T) == 4);
+    const int strat = bucket ? 0 : coarse_strategy(L.n, sizeof(T) == 4);
     if (nsweeps > 12 && strat == 4 && try_coarse_p2p_thin<T>(L, nsweeps, s, &rc)) return rc;
     if (nsweeps > 12 && strat == 3 && try_coarse_tb<T>(L, nsweeps, s, &rc)) return rc;
     if (nsweeps > 12 && strat == 2 && try_coarse_p2p<T>(L, nsweeps, s, &rc)) return rc;
@@ -2216,11 +2299,11 @@ static int relax(const Lvl<T>& L, int nsweeps, cudaStream_t s, bool rhs_ready = 
   }
   if (L.tmp && (L.n & 1) == 0 && L.n >= split_min_n(sizeof(T) == 4))
     return relax_split<T>(L, nsweeps, rhs_ready, s);
-  {
+  if (!bucket) {
     int rc = WF_OK;
     if (try_relax_mid<T>(L, nsweeps, s, &rc)) return rc;
   }
-  if (L.tmp && nsweeps >= 2 && L.n >= sweep2_min_n()) {
+  if (!bucket && L.tmp && nsweeps >= 2 && L.n >= sweep2_min_n()) {
     // pairs of one-launch sweeps: phi -> tmp -> phi
     const int pairs = nsweeps / 2;
     for (int p = 0; p < pairs; ++p) {
@@ -2238,7 +2321,7 @@ static int relax(const Lvl<T>& L, int nsweeps, cudaStream_t s, bool rhs_ready = 
     }
     return WF_OK;
   }
-  if (L.gbar && nsweeps >= 1 && L.n >= persist_min_n()) {
+  if (!bucket && L.gbar && nsweeps >= 1 && L.n >= persist_min_n()) {
     bool done = false;
     WF_TRY(launch_relax_persist<T>(L, nsweeps, s, &done));
     if (done) return WF_OK;
@@ -2351,6 +2434,7 @@ static int build_levels(const wf_case& c, T* phi0, const T* rhs0, long sI, long 
     L.err = c.sc ? &c.sc->status : nullptr;
     L.tmp = (T*)c.mg_tmp[l];
     L.gbar = c.sc ? c.sc->gbar : nullptr;
+    L.role = l;
     L.tJ = L.n + 2;
     L.tI = (long)(L.n + 2) * (L.n + 2);
     if ((L.n << l) != c.n || L.n < 1)
@@ -2380,9 +2464,15 @@ static int build_levels(const wf_case& c, T* phi0, const T* rhs0, long sI, long 
 // In exact arithmetic a V-cycle from phi equals phi + V(rhs - A phi), so the
 // FP64 schedule of n_vcycles cycles is reproduced up to FP32 rounding of the
 // corrections; residual and accumulation stay FP64.
-__global__ void __launch_bounds__(MG_TPB) k_defect(const Lvl<double> F, float* rhs_f,
-                                                   float* phi_f, int n) {
+__global__ void __launch_bounds__(MG_TPB) k_defect(const Lvl<double> F0, float* rhs_f,
+                                                   float* phi_f, int n, const Batch bt) {
   pdl_entry();
+  if (bt_skip(bt)) return;
+  const Lvl<double> F = rebase(F0, bt);
+  if (bt.tab) {
+    rhs_f = (float*)bt.tab[bt_case(bt)].mg_rhs[0];
+    phi_f = (float*)bt.tab[bt_case(bt)].mg_phi[0];
+  }
   const long m = (long)n + 2;
   const long tot = (long)n * n * n;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
@@ -2408,8 +2498,11 @@ __global__ void __launch_bounds__(MG_TPB) k_defect(const Lvl<double> F, float* r
     phi_f[t] = 0.0f;
 }
 
-__global__ void k_correct(const Lvl<double> F, const float* phi_f, int n) {
+__global__ void k_correct(const Lvl<double> F0, const float* phi_f, int n, const Batch bt) {
   pdl_entry();
+  if (bt_skip(bt)) return;
+  const Lvl<double> F = rebase(F0, bt);
+  if (bt.tab) phi_f = (const float*)bt.tab[bt_case(bt)].mg_phi[0];
   const long m = (long)n + 2;
   const long tot = m * m * m;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
@@ -2435,6 +2528,7 @@ static int build_levels_f32(const wf_case& c, std::vector<Lvl<float>>& lv) {
     L.err = c.sc ? &c.sc->status : nullptr;
     L.tmp = (float*)c.mg_tmp[l];
     L.gbar = c.sc ? c.sc->gbar : nullptr;
+    L.role = l;
     L.tJ = L.n + 2;
     L.tI = (long)(L.n + 2) * (L.n + 2);
     L.phi = (float*)c.mg_phi[l];
@@ -2540,8 +2634,9 @@ int mg_solve(const wf_case& c, cudaStream_t s) {
     double* pp = c.fld[WF_PP];
     std::vector<Lvl<float>> lvf;
     WF_TRY(build_levels_f32(c, lvf));
-    const Lvl<double> F = level0_view(c, pp + off, c.fld[WF_SU] + off, P * P, P);
-    WF_CK(launch_k(k_zero<double>, mg_blocks(P * P * P), MG_TPB, 0, s, pp, P * P * P));
+    Lvl<double> F = level0_view(c, pp + off, c.fld[WF_SU] + off, P * P, P);
+    F.role = LV_PP;
+    WF_CK(launch_k(k_zero<double>, mg_blocks(P * P * P), MG_TPB, 0, s, pp, P * P * P, (int)WF_PP));
     WF_CKL("k_zero pp");
     for (int cyc = 0; cyc < c.n_vcycles; ++cyc) WF_TRY(dc_cycle(F, lvf, c, s));
     return WF_OK;
@@ -2552,8 +2647,9 @@ int mg_solve(const wf_case& c, cudaStream_t s) {
   const double* su = c.fld[WF_SU];
   std::vector<Lvl<double>> lv;
   WF_TRY(build_levels<double>(c, pp + off, su + off, P * P, P, lv));
+  lv[0].role = LV_PP;   // level 0 is the core of pp and su
   // multigrid.py:332-333: pp and level-0 phi start from zero
-  WF_CK(launch_k(k_zero<double>, mg_blocks(P * P * P), MG_TPB, 0, s, pp, P * P * P));
+  WF_CK(launch_k(k_zero<double>, mg_blocks(P * P * P), MG_TPB, 0, s, pp, P * P * P, (int)WF_PP));
   WF_CKL("k_zero pp");
   // a level 0 kept in the split layout stays there from the first V-cycle's
   // copy-in to the last one's copy-out
@@ -2600,7 +2696,7 @@ int mg_coarse_solve_pair(const wf_case& c, double* phi, const double* rhs, cudaS
   L.err = c.sc ? &c.sc->status : nullptr;
   L.gbar = c.sc ? c.sc->gbar : nullptr;
   const long m = (long)L.n + 2;
-  WF_CK(launch_k(k_zero<double>, mg_blocks(m * m * m), MG_TPB, 0, s, phi, m * m * m));
+  WF_CK(launch_k(k_zero<double>, mg_blocks(m * m * m), MG_TPB, 0, s, phi, m * m * m, -1));
   WF_CKL("k_zero");
   if (c.mg_cop && c.mg_cop_part && !c.mg_fp32 && c.n_coarse >= 2 && cop_size_ok(L.n))
     return apply_coarse_op<double>(L, (const double*)c.mg_cop, (double*)c.mg_cop_part, s);
@@ -2827,7 +2923,7 @@ int mg_solve_noalloc(const double* su, double* pp, int n, int nlev, double dx, d
   c.n_coarse = 300;
   c.n_vcycles = 4;
   WF_CK(cudaMemsetAsync(ad.status, 0, sizeof(int), s));
-  WF_CK(launch_k(k_zero<double>, mg_blocks(P * P * P), MG_TPB, 0, s, pp, P * P * P));
+  WF_CK(launch_k(k_zero<double>, mg_blocks(P * P * P), MG_TPB, 0, s, pp, P * P * P, (int)WF_PP));
   WF_CKL("k_zero pp");
   for (int cyc = 0; cyc < c.n_vcycles; ++cyc) WF_TRY(vcycle_fixed(lv, nlev, c, s));
   return WF_OK;

@@ -150,20 +150,21 @@ int launch_init_noise(double* u, double* v, double* w, int n, double amp, int se
 // and the viscous/advective min in one pass; the last block finishes the
 // dt update on the device.
 // --------------------------------------------------------------------------
-__global__ void __launch_bounds__(TPB) k_checkdt(const wf_case c, Geo g, const Divs dv) {
+__global__ void __launch_bounds__(TPB) k_checkdt(const wf_case c, Geo g, const Divs dv,
+                                                const Batch bt) {
   pdl_entry();
   __shared__ double sm[32];
-  const double* u = c.fld[WF_U];
-  const double* v = c.fld[WF_V];
-  const double* w = c.fld[WF_W];
-  const double* vis = c.fld[WF_VIS];
+  const double* u = bt_fld(c, bt, WF_U);
+  const double* v = bt_fld(c, bt, WF_V);
+  const double* w = bt_fld(c, bt, WF_W);
+  const double* vis = bt_fld(c, bt, WF_VIS);
   const double dx = c.dx, dy = c.dy, dz = c.dz;
   const double inv2 = 1.0 / (dx * dx) + 1.0 / (dy * dy) + 1.0 / (dz * dz);
   double mu = 0.0, mv = 0.0, mw = 0.0, mdt = 1.0e10;
   const int k = NPL + blockIdx.x * 32 + (threadIdx.x & 31);
   const int j = NPL + blockIdx.y * 8 + (threadIdx.x >> 5);
   const bool in = k < NPL + g.n && j < NPL + g.n;
-  for (int i = NPL + blockIdx.z; in && i < NPL + g.n; i += gridDim.z) {
+  for (int i = NPL + bt_z(bt); in && i < NPL + g.n; i += bt_gz(bt)) {
     const long id = g.at(i, j, k);
     const double uu = LD(u, id), vv = LD(v, id), ww = LD(w, id);
     mu = fmax(mu, fabs(uu));
@@ -182,14 +183,14 @@ __global__ void __launch_bounds__(TPB) k_checkdt(const wf_case c, Geo g, const D
   mv = block_max(mv, sm);
   mw = block_max(mw, sm);
   mdt = block_min(mdt, sm, 1.0e10);
-  wf_scalars* sc = c.sc;
+  wf_scalars* sc = bt_sc(c, bt);
   if (threadIdx.x == 0) {
     atomicMax(&sc->red[0], okey(mu));
     atomicMax(&sc->red[1], okey(mv));
     atomicMax(&sc->red[2], okey(mw));
     atomicMin(&sc->red[3], okey(mdt));
   }
-  if (!last_block(&sc->ticket)) return;
+  if (!last_block(&sc->ticket, gridDim.x * gridDim.y * bt_gz(bt))) return;
   if (threadIdx.x != 0) return;
   const double umax = okey_inv(atomicAdd(&sc->red[0], 0ull));
   const double vmax = okey_inv(atomicAdd(&sc->red[1], 0ull));
@@ -211,6 +212,7 @@ __global__ void __launch_bounds__(TPB) k_checkdt(const wf_case c, Geo g, const D
   sc->itime += 1;
   sc->iters = 0;
   sc->nmg = 0;
+  sc->loop = 1;   // the case takes part in this step's projection loop
   if (dtmax <= 0.0 || !(dtmax < big)) sc->status = WF_ST_DT_COLLAPSE;
   const double dt_old = sc->dt;
   sc->cfl = dt_old / dtmax;
@@ -233,8 +235,17 @@ int launch_checkdt(const wf_case& c, cudaStream_t s) {
 __global__ void k_copy3(const double2* a0, double2* b0,
                         const double2* a1, double2* b1,
                         const double2* a2, double2* b2,
-                        long n2) {
+                        long n2, const Batch bt) {
   pdl_entry();
+  if (bt.tab) {
+    const CasePtrs& cp = bt.tab[bt_case(bt)];
+    a0 = (const double2*)cp.fld[WF_U];
+    b0 = (double2*)cp.fld[WF_UOO];
+    a1 = (const double2*)cp.fld[WF_V];
+    b1 = (double2*)cp.fld[WF_VOO];
+    a2 = (const double2*)cp.fld[WF_W];
+    b2 = (double2*)cp.fld[WF_WOO];
+  }
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n2;
        t += (long)gridDim.x * blockDim.x) {
     b0[t] = a0[t];
@@ -272,19 +283,21 @@ int launch_copy_oo(const wf_case& c, cudaStream_t s) {
 // it in every thread; one host pow gives the same value without a device
 // pow per cell)
 __global__ void __launch_bounds__(TPB) k_wale(const wf_case c, Geo g, const Divs dv,
-                                             const double ls, const double* rrey_dev) {
+                                             const double ls, const double* rrey_dev,
+                                             const Batch bt) {
   pdl_entry();
-  const double* u = c.fld[WF_U];
-  const double* v = c.fld[WF_V];
-  const double* w = c.fld[WF_W];
-  double* vis = c.fld[WF_VIS];
+  const double* u = bt_fld(c, bt, WF_U);
+  const double* v = bt_fld(c, bt, WF_V);
+  const double* w = bt_fld(c, bt, WF_W);
+  double* vis = bt_fld(c, bt, WF_VIS);
+  if (bt.tab) rrey_dev = &bt_sc(c, bt)->rrey;
   const long sI = g.sI, sJ = g.sJ;
   {  // one thread per cell: x = k (runs of 32), y = j (groups of 8), z = i
     const int kx_ = blockIdx.x * 32 + threadIdx.x, jy_ = blockIdx.y * 8 + threadIdx.y;
     if (kx_ >= g.n || jy_ >= g.n) return;
     const int k = NPL + kx_;
     const int j = NPL + jy_;
-    const int i = NPL + (int)blockIdx.z;
+    const int i = NPL + bt_z(bt);
     const long id = g.at(i, j, k);
 #define U_(a) LD(u, id + (a))
 #define V_(a) LD(v, id + (a))
@@ -337,8 +350,12 @@ __global__ void __launch_bounds__(TPB) k_wale(const wf_case c, Geo g, const Divs
 }
 
 // vis = 1/Re on real cells (kernels.py:442-449)
-__global__ void k_fill_real(double* f, Geo g, double val, const double* valp) {
+__global__ void k_fill_real(double* f, Geo g, double val, const double* valp, const Batch bt) {
   pdl_entry();
+  if (bt.tab) {
+    f = bt.tab[bt_case(bt)].fld[WF_VIS];
+    valp = &bt.tab[bt_case(bt)].sc->rrey;
+  }
   if (valp) val = *valp;
   const long tot = (long)g.n * g.n * g.n;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
@@ -358,7 +375,7 @@ int launch_wale(const wf_case& c, cudaStream_t s, const double* rrey_dev) {
     WF_CK(launch_k(k_wale, cells3(c.n, c.n, c.n), cell_block(), 0, s, c, g, divs_of(c), ls,
                    rrey_dev));
     WF_CKL("k_wale");
-    FillReq r{c.fld[WF_VIS], FILL_VIS, c.rrey, rrey_dev};
+    FillReq r{c.fld[WF_VIS], FILL_VIS, c.rrey, rrey_dev, WF_VIS, rrey_dev ? 2 : 0};
     return launch_fills(&r, 1, c.n, s);
   }
   WF_CK(launch_k(k_fill_real, nblocks(tot), TPB, 0, s, c.fld[WF_VIS], g, c.rrey, rrey_dev));
@@ -395,15 +412,15 @@ __device__ __forceinline__ double diff_add(double star, double dt, double alpha,
   return star + dt * alpha * diff;
 }
 
-// vis * lap4(f) at cell id of component COMP (kernels.py:189-225)
+// vis * lap4(f) at cell id of component COMP (kernels.py:189-225); f the
+// component, vis the viscosity field
 template <int COMP>
-__device__ __forceinline__ double diff_term(const wf_case& c, const Geo& g, const Divs& dv,
-                                            long id) {
-  const double* f = c.fld[WF_U + COMP];
+__device__ __forceinline__ double diff_term(const double* f, const double* vis, const Geo& g,
+                                            const Divs& dv, long id) {
   const long vofs = COMP == 0 ? 0 : (COMP == 1 ? g.sJ : 1);
   const double l4 = lap1(f, id, g.sI, dv.d12[0], dv.y12[0]) +
                     lap1(f, id, g.sJ, dv.d12[1], dv.y12[1]) + lap1(f, id, 1, dv.d12[2], dv.y12[2]);
-  return LD(c.fld[WF_VIS], id + vofs) * l4;
+  return LD(vis, id + vofs) * l4;
 }
 
 // one cell (i0, j0, k0 from 0 within the op range) of component COMP
@@ -412,7 +429,8 @@ __device__ __forceinline__ void diff_cell(const wf_case& c, const Geo& g, double
                                           double dt, const Divs& dv, int i0, int j0, int k0) {
   double* star = c.fld[WF_USTAR + COMP];
   const long id = g.at(NPL + i0, NPL + j0, NPL + k0);
-  star[id] = diff_add(star[id], dt, alpha, diff_term<COMP>(c, g, dv, id));
+  star[id] = diff_add(star[id], dt, alpha,
+                      diff_term<COMP>(c.fld[WF_U + COMP], c.fld[WF_VIS], g, dv, id));
 }
 
 // DIFF: also add the component's diffusion to star in the same pass.  The
@@ -424,25 +442,28 @@ __device__ __forceinline__ void diff_cell(const wf_case& c, const Geo& g, double
 // the same star.
 template <int COMP, bool DIFF>
 __global__ void __launch_bounds__(TPB) k_conv(const wf_case c, Geo g, double alpha,
-                                             const double* dtp, const Divs dv) {
+                                             const double* dtp, const Divs dv, const Batch bt) {
   pdl_entry();
-  const double* u = c.fld[WF_U];
-  const double* v = c.fld[WF_V];
-  const double* w = c.fld[WF_W];
-  const double* oo = c.fld[WF_UOO + COMP];
-  double* star = c.fld[WF_USTAR + COMP];
+  const double* u = bt_fld(c, bt, WF_U);
+  const double* v = bt_fld(c, bt, WF_V);
+  const double* w = bt_fld(c, bt, WF_W);
+  const double* oo = bt_fld(c, bt, WF_UOO + COMP);
+  double* star = bt_fld(c, bt, WF_USTAR + COMP);
+  if (bt.tab) dtp = &bt_sc(c, bt)->dt;
   const double dx = c.dx, dy = c.dy, dz = c.dz;
   const double dt = *dtp;
   const long X = g.sI, Y = g.sJ, Z = 1;
   int ni, nj, nk;
   op_dims(COMP, g.n, ni, nj, nk);
   const long tot = (long)ni * nj * nk;
-  {  // one thread per cell: x = k (runs of 32), y = j (groups of 8), z = i
-    const int kx_ = blockIdx.x * 32 + threadIdx.x, jy_ = blockIdx.y * 8 + threadIdx.y;
+  {  // one thread per cell: x = k, y = j (the CTA's shape is chosen per
+     // size, 32 x 8 by default), z = i
+    const int kx_ = blockIdx.x * blockDim.x + threadIdx.x;
+    const int jy_ = blockIdx.y * blockDim.y + threadIdx.y;
     if (kx_ >= nk || jy_ >= nj) return;
     const int k = NPL + kx_;
     const int j = NPL + jy_;
-    const int i = NPL + (int)blockIdx.z;
+    const int i = NPL + bt_z(bt);
     const long id = g.at(i, j, k);
     double tot3;
     if (COMP == 0) {
@@ -501,7 +522,10 @@ __global__ void __launch_bounds__(TPB) k_conv(const wf_case c, Geo g, double alp
       tot3 = duwdx + dvwdy + dw2dz;
     }
     const double s1 = LD(oo, id) - dt * alpha * tot3;
-    star[id] = DIFF ? diff_add(s1, dt, alpha, diff_term<COMP>(c, g, dv, id)) : s1;
+    star[id] = DIFF ? diff_add(s1, dt, alpha,
+                               diff_term<COMP>(COMP == 0 ? u : (COMP == 1 ? v : w),
+                                               bt_fld(c, bt, WF_VIS), g, dv, id))
+                    : s1;
   }
 }
 
@@ -518,16 +542,68 @@ __global__ void __launch_bounds__(TPB) k_diff(const wf_case c, Geo g, double alp
 }
 
 
+// ---- launch shapes per size ------------------------------------------------
+// 0 = the default: k_conv 32 x 8 (a warp along k, 8 rows j); k_rbgs_split
+// 2 cells per thread (WF_SPLIT_CPT overrides), 8 rows per CTA
+static constexpr int SHAPE_MAX_N = 1024;
+static int g_shape[2][SHAPE_MAX_N + 1][2];
+
+static int split_cpt_default() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("WF_SPLIT_CPT");
+    v = e ? atoi(e) : 2;
+    if (v != 1 && v != 2 && v != 4) v = 2;
+  }
+  return v;
+}
+
+void launch_shape(int kind, int n, int* a, int* b) {
+  const bool set = kind >= 0 && kind <= 1 && n >= 0 && n <= SHAPE_MAX_N && g_shape[kind][n][0];
+  if (kind == SHAPE_CONV) {
+    *a = set ? g_shape[kind][n][0] : 32;
+    *b = set ? g_shape[kind][n][1] : 8;
+  } else {
+    *a = set ? g_shape[kind][n][0] : split_cpt_default();
+    *b = set ? g_shape[kind][n][1] : 8;
+  }
+}
+
+int set_launch_shape(int kind, int n, int a, int b) {
+  if (n < 4 || n > SHAPE_MAX_N) return fail(WF_EINVAL, "wf_set_launch_shape: n in 4..1024");
+  if (a == 0 && b == 0) {
+    if (kind != SHAPE_CONV && kind != SHAPE_SPLIT)
+      return fail(WF_EINVAL, "wf_set_launch_shape: kind 0 (k_conv) or 1 (k_rbgs_split)");
+    g_shape[kind][n][0] = g_shape[kind][n][1] = 0;
+    return WF_OK;
+  }
+  if (kind == SHAPE_CONV) {
+    // whole warps, at most TPB threads (the kernel's launch bound)
+    if (a < 1 || b < 1 || a > 256 || (a & (a - 1)) || a * b > TPB || (a * b) % 32)
+      return fail(WF_EINVAL, "wf_set_launch_shape(k_conv): a a power of two, a*b a multiple "
+                             "of 32 and at most 256");
+  } else if (kind == SHAPE_SPLIT) {
+    if ((a != 1 && a != 2 && a != 4) || (b != 1 && b != 2 && b != 4 && b != 8))
+      return fail(WF_EINVAL, "wf_set_launch_shape(k_rbgs_split): a in {1,2,4}, b in {1,2,4,8}");
+  } else {
+    return fail(WF_EINVAL, "wf_set_launch_shape: kind 0 (k_conv) or 1 (k_rbgs_split)");
+  }
+  g_shape[kind][n][0] = a;
+  g_shape[kind][n][1] = b;
+  return WF_OK;
+}
+
 int launch_conv(const wf_case& c, int comp, double alpha, const double* dt,
                 cudaStream_t s, bool with_diff) {
   Geo g = geo_of(c.n);
-  const long tot = (long)c.n * c.n * (c.n - 1);
-  const int nb = nblocks(tot);
   int ni, nj, nk;
   op_dims(comp, c.n, ni, nj, nk);
-  const dim3 gr = cells3(ni, nj, nk), bl = cell_block();
+  int bx, by;
+  launch_shape(SHAPE_CONV, c.n, &bx, &by);
+  const dim3 gr((nk + bx - 1) / bx, (nj + by - 1) / by, ni), bl(bx, by);
   if (comp < 0 || comp > 2) return fail(WF_EINVAL, "conv: comp must be 0, 1 or 2");
-  void (*const kern[2][3])(const wf_case, Geo, double, const double*, const Divs) = {
+  void (*const kern[2][3])(const wf_case, Geo, double, const double*, const Divs,
+                           const Batch) = {
       {k_conv<0, false>, k_conv<1, false>, k_conv<2, false>},
       {k_conv<0, true>, k_conv<1, true>, k_conv<2, true>}};
   WF_CK(launch_k(kern[with_diff ? 1 : 0][comp], gr, bl, 0, s, c, g, alpha, dt, divs_of(c)));
@@ -556,28 +632,34 @@ int launch_diff(const wf_case& c, int comp, double alpha, const double* dt,
 // calvel (kernels.py:232-264): the three components in one launch
 // --------------------------------------------------------------------------
 __global__ void __launch_bounds__(TPB) k_calvel(const wf_case c, Geo g, double alpha,
-                                               const double* dtp, const Divs dv) {
+                                               const double* dtp, const Divs dv,
+                                               const Batch bt) {
   pdl_entry();
-  const double* p = c.fld[WF_P];
+  if (bt_skip(bt)) return;
+  const double* p = bt_fld(c, bt, WF_P);
+  if (bt.tab) dtp = &bt_sc(c, bt)->dt;
   const double dt = *dtp;
+  double* fu = bt_fld(c, bt, WF_U);
+  double* fv = bt_fld(c, bt, WF_V);
+  double* fw = bt_fld(c, bt, WF_W);
+  const double* us = bt_fld(c, bt, WF_USTAR);
+  const double* vs = bt_fld(c, bt, WF_VSTAR);
+  const double* ws = bt_fld(c, bt, WF_WSTAR);
   const int hi = NPL + g.n - 1;  // last real index; the component's own axis stops before it
   {  // one thread per cell: x = k (runs of 32), y = j (groups of 8), z = i
     const int kx_ = blockIdx.x * 32 + threadIdx.x, jy_ = blockIdx.y * 8 + threadIdx.y;
     if (kx_ >= g.n || jy_ >= g.n) return;
     const int k = NPL + kx_;
     const int j = NPL + jy_;
-    const int i = NPL + (int)blockIdx.z;
+    const int i = NPL + bt_z(bt);
     const long id = g.at(i, j, k);
     const double p0 = LD(p, id);
     if (i < hi)
-      c.fld[WF_U][id] = LD(c.fld[WF_USTAR], id) -
-                        div_by_recip(dt * alpha * (LD(p, id + g.sI) - p0), dv.dh[0], dv.yh[0]);
+      fu[id] = LD(us, id) - div_by_recip(dt * alpha * (LD(p, id + g.sI) - p0), dv.dh[0], dv.yh[0]);
     if (j < hi)
-      c.fld[WF_V][id] = LD(c.fld[WF_VSTAR], id) -
-                        div_by_recip(dt * alpha * (LD(p, id + g.sJ) - p0), dv.dh[1], dv.yh[1]);
+      fv[id] = LD(vs, id) - div_by_recip(dt * alpha * (LD(p, id + g.sJ) - p0), dv.dh[1], dv.yh[1]);
     if (k < hi)
-      c.fld[WF_W][id] = LD(c.fld[WF_WSTAR], id) -
-                        div_by_recip(dt * alpha * (LD(p, id + 1) - p0), dv.dh[2], dv.yh[2]);
+      fw[id] = LD(ws, id) - div_by_recip(dt * alpha * (LD(p, id + 1) - p0), dv.dh[2], dv.yh[2]);
   }
 }
 
@@ -588,20 +670,49 @@ int launch_calvel(const wf_case& c, double alpha, const double* dt, cudaStream_t
   return WF_OK;
 }
 
+// one case of a bucket reports its loop decision (wf_scalars.loop bits:
+// 1 continue, 2 run the multigrid part); the last case to report sets the
+// bucket loop's graph conditions from the OR of all decisions and resets
+// the count (kept in the first case's scalar block)
+__device__ __forceinline__ void bucket_report(const Batch& bt, int loop,
+                                              unsigned long long h_if,
+                                              unsigned long long h_loop) {
+  wf_scalars* s0 = bt.tab[0].sc;
+  const unsigned ncases = gridDim.z / (unsigned)bt.nz;
+  atomicOr((unsigned*)&s0->bflags, (unsigned)loop);
+  __threadfence();
+  if (atomicAdd(&s0->bticket, 1u) != ncases - 1) return;
+  __threadfence();
+  const unsigned any = atomicExch((unsigned*)&s0->bflags, 0u);
+  s0->bticket = 0u;
+  if (h_if) cudaGraphSetConditional((cudaGraphConditionalHandle)h_if, (any & 2) ? 1u : 0u);
+  if (h_loop) cudaGraphSetConditional((cudaGraphConditionalHandle)h_loop, (any & 1) ? 1u : 0u);
+}
+
 // --------------------------------------------------------------------------
 // calmas (kernels.py:271-289) + one iteration of the projection control
 // (solver.py:185-209), decided by the last block on the device
 // --------------------------------------------------------------------------
+// In a bucket (bt.tab set) a case whose loop has ended does no work: one of
+// its blocks only reports it to the bucket; the conditions of the bucket's
+// loop are set by whichever case reports last, from the OR of all cases'
+// decisions (collected in the first case's scalar block).
 __global__ void __launch_bounds__(TPB) k_calmas(const wf_case c, Geo g,
                                                unsigned long long h_if,
-                                               unsigned long long h_loop, const Divs dv) {
+                                               unsigned long long h_loop, const Divs dv,
+                                               const Batch bt) {
   pdl_entry();
   __shared__ double sm[32];
-  const double* u = c.fld[WF_U];
-  const double* v = c.fld[WF_V];
-  const double* w = c.fld[WF_W];
-  double* su = c.fld[WF_SU];
-  wf_scalars* sc = c.sc;
+  const double* u = bt_fld(c, bt, WF_U);
+  const double* v = bt_fld(c, bt, WF_V);
+  const double* w = bt_fld(c, bt, WF_W);
+  double* su = bt_fld(c, bt, WF_SU);
+  wf_scalars* sc = bt_sc(c, bt);
+  if (bt.tab && !(sc->loop & 1)) {
+    if (blockIdx.x == 0 && blockIdx.y == 0 && bt_z(bt) == 0 && threadIdx.x == 0)
+      bucket_report(bt, 0, h_if, h_loop);
+    return;
+  }
   const double dt = sc->dt;
   const double rdt = 1.0 / dt;   // fact / dt below as div_by_recip(fact, dt, rdt)
   const double dx = c.dx, dy = c.dy, dz = c.dz;
@@ -609,7 +720,7 @@ __global__ void __launch_bounds__(TPB) k_calmas(const wf_case c, Geo g,
   const int k = NPL + blockIdx.x * 32 + (threadIdx.x & 31);
   const int j = NPL + blockIdx.y * 8 + (threadIdx.x >> 5);
   const bool in = k < NPL + g.n && j < NPL + g.n;
-  for (int i = NPL + blockIdx.z; in && i < NPL + g.n; i += gridDim.z) {
+  for (int i = NPL + bt_z(bt); in && i < NPL + g.n; i += bt_gz(bt)) {
     const long id = g.at(i, j, k);
     const long X = g.sI, Y = g.sJ;
     const double dudx = div_by_recip(-LD(u, id + X) + 27.0 * LD(u, id) - 27.0 * LD(u, id - X) +
@@ -624,7 +735,7 @@ __global__ void __launch_bounds__(TPB) k_calmas(const wf_case c, Geo g,
   }
   mloc = block_max(mloc, sm);
   if (threadIdx.x == 0) atomicMax(&sc->red[4], okey(mloc));
-  if (!last_block(&sc->ticket)) return;
+  if (!last_block(&sc->ticket, gridDim.x * gridDim.y * bt_gz(bt))) return;
   if (threadIdx.x != 0) return;
   const double rmax = okey_inv(atomicAdd(&sc->red[4], 0ull));
   sc->red[4] = okey(0.0);
@@ -639,6 +750,10 @@ __global__ void __launch_bounds__(TPB) k_calmas(const wf_case c, Geo g,
   if (run && it >= c.maxcy && sc->status == WF_ST_OK) sc->status = WF_ST_NOT_CONVERGED;
   const int more = (run && it < c.maxcy) ? 1 : 0;
   sc->loop = (run ? 2 : 0) | more;
+  if (bt.tab) {
+    bucket_report(bt, sc->loop, h_if, h_loop);
+    return;
+  }
   if (h_if) cudaGraphSetConditional((cudaGraphConditionalHandle)h_if, run ? 1u : 0u);
   if (h_loop) cudaGraphSetConditional((cudaGraphConditionalHandle)h_loop, (unsigned)more);
 }
@@ -654,15 +769,20 @@ int launch_calmas(const wf_case& c, unsigned long long h_if, unsigned long long 
 // --------------------------------------------------------------------------
 // p += pp over real cells plus one ring (kernels.py:405-414)
 // --------------------------------------------------------------------------
-__global__ void k_add_ring(double* p, const double* pp, Geo g) {
+__global__ void k_add_ring(double* p, const double* pp, Geo g, const Batch bt) {
   pdl_entry();
+  if (bt_skip(bt)) return;
+  if (bt.tab) {
+    p = bt.tab[bt_case(bt)].fld[WF_P];
+    pp = bt.tab[bt_case(bt)].fld[WF_PP];
+  }
   const int m = g.n + 2;
   {  // one thread per cell: x = k (runs of 32), y = j (groups of 8), z = i
     const int kx_ = blockIdx.x * 32 + threadIdx.x, jy_ = blockIdx.y * 8 + threadIdx.y;
     if (kx_ >= m || jy_ >= m) return;
     const int k = NPL - 1 + kx_;
     const int j = NPL - 1 + jy_;
-    const int i = NPL - 1 + (int)blockIdx.z;
+    const int i = NPL - 1 + bt_z(bt);
     const long id = g.at(i, j, k);
     p[id] = p[id] + pp[id];
   }

@@ -12,10 +12,12 @@
 // calmas kernel and a conditional IF node for the multigrid part; the
 // calmas kernel's last block sets both conditions on the device, so a
 // whole step is one graph launch with no host round trip.
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "wf_internal.h"
 
@@ -34,6 +36,23 @@ bool pdl_enabled() {
   }
   return v == 1 && !g_pdl_off;
 }
+
+BatchCtx& batch_ctx() {
+  static thread_local BatchCtx ctx;
+  return ctx;
+}
+
+// Launches of this thread serve the bucket `tab` (ncases cases) for one
+// scope; tab null = one case.
+struct BatchScope {
+  BatchCtx prev;
+  BatchScope(const CasePtrs* tab, int ncases, int skip) : prev(batch_ctx()) {
+    batch_ctx().tab = tab;
+    batch_ctx().ncases = tab ? ncases : 1;
+    batch_ctx().skip = tab ? skip : 0;
+  }
+  ~BatchScope() { batch_ctx() = prev; }
+};
 
 // Turns programmatic dependent launch off on this thread for one scope.
 struct PdlOff {
@@ -76,13 +95,14 @@ int validate_case(const wf_case& c) {
 // of the same size without being rebuilt.
 static int fill_comp(const wf_case& c, int comp, cudaStream_t s) {
   FillReq r{c.fld[WF_U + comp], comp == 0 ? FILL_U : (comp == 1 ? FILL_V : FILL_W), c.ulid,
-            comp == 0 ? &c.sc->ulid : nullptr};
+            comp == 0 ? &c.sc->ulid : nullptr, WF_U + comp, comp == 0 ? 1 : 0};
   return launch_fills(&r, 1, c.n, s);
 }
 
 static int fill_uvw(const wf_case& c, cudaStream_t s) {
-  FillReq r[3] = {{c.fld[WF_U], FILL_U, c.ulid, &c.sc->ulid}, {c.fld[WF_V], FILL_V, 0.0},
-                  {c.fld[WF_W], FILL_W, 0.0}};
+  FillReq r[3] = {{c.fld[WF_U], FILL_U, c.ulid, &c.sc->ulid, WF_U, 1},
+                  {c.fld[WF_V], FILL_V, 0.0, nullptr, WF_V, 0},
+                  {c.fld[WF_W], FILL_W, 0.0, nullptr, WF_W, 0}};
   return launch_fills(r, 3, c.n, s);
 }
 
@@ -110,7 +130,7 @@ static int step_prologue(const wf_case& c, cudaStream_t s) {
 static int step_mg_part(const wf_case& c, cudaStream_t s) {
   WF_TRY(mg_solve(c, s));
   WF_TRY(launch_add_ring(c.fld[WF_P], c.fld[WF_PP], c.n, s));
-  FillReq r{c.fld[WF_P], FILL_PBOUND, 0.0};
+  FillReq r{c.fld[WF_P], FILL_PBOUND, 0.0, nullptr, WF_P, 0};
   WF_TRY(launch_fills(&r, 1, c.n, s));
   return launch_calvel(c, 1.0, &c.sc->dt, s);
 }
@@ -134,8 +154,12 @@ struct wf_stepper {
 // Append one case's step to graph g as an independent branch (its first
 // nodes have no dependencies): the prologue, a WHILE node over calmas and
 // an IF node holding the multigrid part, then the epilogue.  counts gets the
-// launches of each part.
-static int append_step(cudaGraph_t g, const wf_case& c, int32_t counts[4]) {
+// launches of each part.  With `tab` (ncases rows, c = the first case) the
+// branch steps the whole bucket: every launch serves every case, the
+// multigrid part only the cases whose own loop runs it this iteration, and
+// the loop runs while any case's loop does.
+static int append_step(cudaGraph_t g, const wf_case& c, int32_t counts[4],
+                       const CasePtrs* tab = nullptr, int ncases = 1) {
   cudaStream_t cap;
   WF_CK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
   int rc = WF_OK;
@@ -146,7 +170,10 @@ static int append_step(cudaGraph_t g, const wf_case& c, int32_t counts[4]) {
     e = cudaStreamBeginCaptureToGraph(cap, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) { rc = cuda_fail(e, "cudaStreamBeginCaptureToGraph"); break; }
     long l0 = g_launches;
-    rc = step_prologue(c, cap);
+    {
+      BatchScope bs(tab, ncases, 0);
+      rc = step_prologue(c, cap);
+    }
     counts[0] = (int32_t)(g_launches - l0);
     cudaGraphNode_t wnode = nullptr;
     cudaGraph_t wbody = nullptr;
@@ -170,7 +197,10 @@ static int append_step(cudaGraph_t g, const wf_case& c, int32_t counts[4]) {
         if (e != cudaSuccess) rc = cuda_fail(e, "cudaStreamUpdateCaptureDependencies");
       }
       l0 = g_launches;
-      if (rc == WF_OK) rc = step_epilogue(c, cap);
+      if (rc == WF_OK) {
+        BatchScope bs(tab, ncases, 0);
+        rc = step_epilogue(c, cap);
+      }
       counts[3] = (int32_t)(g_launches - l0);
     }
     cudaGraph_t gout = nullptr;
@@ -185,7 +215,10 @@ static int append_step(cudaGraph_t g, const wf_case& c, int32_t counts[4]) {
     e = cudaStreamBeginCaptureToGraph(cap, wbody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) { rc = cuda_fail(e, "cudaStreamBeginCaptureToGraph(while)"); break; }
     l0 = g_launches;
-    rc = launch_calmas(c, (unsigned long long)h_if, (unsigned long long)h_loop, cap);
+    {
+      BatchScope bs(tab, ncases, 0);
+      rc = launch_calmas(c, (unsigned long long)h_if, (unsigned long long)h_loop, cap);
+    }
     counts[1] = (int32_t)(g_launches - l0);
     cudaGraph_t ibody = nullptr;
     if (rc == WF_OK) {
@@ -216,7 +249,10 @@ static int append_step(cudaGraph_t g, const wf_case& c, int32_t counts[4]) {
     e = cudaStreamBeginCaptureToGraph(cap, ibody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) { rc = cuda_fail(e, "cudaStreamBeginCaptureToGraph(if)"); break; }
     l0 = g_launches;
-    rc = step_mg_part(c, cap);
+    {
+      BatchScope bs(tab, ncases, 2);   // only cases whose loop runs the multigrid part
+      rc = step_mg_part(c, cap);
+    }
     counts[2] = (int32_t)(g_launches - l0);
     e = cudaStreamEndCapture(cap, &gout);
     if (rc == WF_OK && e != cudaSuccess) rc = cuda_fail(e, "cudaStreamEndCapture(if)");
@@ -244,7 +280,65 @@ struct wf_ensemble {
   int ncases;
   cudaGraph_t graph;
   cudaGraphExec_t exec;
+  std::vector<void*> tables;            // device pointer tables of the buckets
+  std::vector<int32_t> bucket_of_case;  // -1 without buckets
+  std::vector<int32_t> counts;          // 4 per bucket (or per case)
 };
+
+// Cases that can share a bucket: the same size, numerics and physics flags
+// (1/Re and the lid velocity are read from each case's scalar block), the
+// same shared coarse operator, and the same optional buffers present.
+static bool same_bucket(const wf_case& a, const wf_case& b) {
+  if (a.n != b.n || a.nlev != b.nlev || a.sgs != b.sgs || a.variable_dt != b.variable_dt ||
+      a.maxcy != b.maxcy || a.mg_fp32 != b.mg_fp32 || a.n_pre != b.n_pre ||
+      a.n_post != b.n_post || a.n_coarse != b.n_coarse || a.n_vcycles != b.n_vcycles)
+    return false;
+  if (a.dx != b.dx || a.dy != b.dy || a.dz != b.dz || a.cw != b.cw ||
+      a.dt_growth != b.dt_growth || a.safety != b.safety || a.eps != b.eps)
+    return false;
+  if (a.mg_cop != b.mg_cop || (a.mg_cop_part == nullptr) != (b.mg_cop_part == nullptr))
+    return false;
+  for (int l = 0; l < WF_MAX_LEVELS; ++l)
+    if ((a.mg_tmp[l] == nullptr) != (b.mg_tmp[l] == nullptr)) return false;
+  return true;
+}
+
+// Largest bucket for cases of size n (per precision of their multigrid).
+// 0 in the table means the built-in rule: a bucket's grids stack its cases
+// along z (< 65536), and its cases' finest multigrid level (phi and rhs)
+// should fit in about half the L2 (64 MB), so the half-sweeps, which
+// dominate a step, keep the bucket's level resident across launches.  From
+// n = 64 on, separate branches are the default.  Measured on B200 (16
+// mixed-precision cases per size, ms per ensemble step, bucketed vs one
+// branch per case): 32^3 1.25 vs 1.74, 48^3 2.87 vs 3.13, 64^3 4.67 vs
+// 4.33, 80^3 10.3 vs 8.5, 96^3 14.8 vs 12.1.  The branches of large cases
+// overlap one another's dependent chains of kernels; a bucket waits for its
+// slowest case at every launch.  wf_set_bucket_cap overrides the rule per
+// size (the autotuner's measurement).
+static constexpr int BUCKET_MAX_N = 1024;
+static int g_bucket_cap[2][BUCKET_MAX_N + 1];
+
+static int bucket_cap(const wf_case& c) {
+  const int set = (c.n >= 0 && c.n <= BUCKET_MAX_N) ? g_bucket_cap[c.mg_fp32 ? 1 : 0][c.n] : 0;
+  if (set > 0) return std::min(set, std::max(1, 60000 / (c.n + 2 * NPL)));
+  if (c.n >= 64) return 1;
+  const long m = c.n + 2;
+  const long lvl_bytes = 2 * m * m * m * (c.mg_fp32 ? 4 : 8);
+  return (int)std::max(1L, std::min(60000L / (c.n + 2 * NPL), (64L << 20) / lvl_bytes));
+}
+
+static CasePtrs ptrs_of(const wf_case& c) {
+  CasePtrs p{};
+  for (int f = 0; f < WF_NFIELDS; ++f) p.fld[f] = c.fld[f];
+  p.sc = c.sc;
+  for (int l = 0; l < WF_MAX_LEVELS; ++l) {
+    p.mg_phi[l] = c.mg_phi[l];
+    p.mg_rhs[l] = c.mg_rhs[l];
+    p.mg_tmp[l] = c.mg_tmp[l];
+  }
+  p.mg_cop_part = c.mg_cop_part;
+  return p;
+}
 
 extern "C" {
 
@@ -260,6 +354,36 @@ int wf_struct_sizes(int64_t* scalars, int64_t* casebytes) {
 
 int wf_set_coarse_strategy(int32_t n, int32_t fp32, int32_t strategy) {
   return set_coarse_strategy(n, fp32, strategy);
+}
+
+int wf_set_launch_shape(int32_t kind, int32_t n, int32_t a, int32_t b) {
+  return set_launch_shape(kind, n, a, b);
+}
+
+int wf_launch_shape(int32_t kind, int32_t n, int32_t* a, int32_t* b) {
+  if (!a || !b || (kind != SHAPE_CONV && kind != SHAPE_SPLIT))
+    return fail(WF_EINVAL, "wf_launch_shape: kind 0 or 1, non-null outputs");
+  int x, y;
+  launch_shape(kind, n, &x, &y);
+  *a = x;
+  *b = y;
+  return WF_OK;
+}
+
+int wf_set_bucket_cap(int32_t n, int32_t fp32, int32_t cap) {
+  if (n < 4 || n > BUCKET_MAX_N || cap < 0)
+    return fail(WF_EINVAL, "wf_set_bucket_cap: n in 4..1024, cap >= 0");
+  g_bucket_cap[fp32 ? 1 : 0][n] = cap;
+  return WF_OK;
+}
+
+int wf_bucket_cap(int32_t n, int32_t fp32, int32_t* cap) {
+  if (!cap || n < 4 || n > BUCKET_MAX_N) return fail(WF_EINVAL, "wf_bucket_cap: n in 4..1024");
+  wf_case c{};
+  c.n = n;
+  c.mg_fp32 = fp32 ? 1 : 0;
+  *cap = bucket_cap(c);
+  return WF_OK;
 }
 
 int wf_mg_level_elems(int32_t n, int32_t nlev, int32_t level, int64_t* elems) {
@@ -448,32 +572,105 @@ int wf_stepper_step(wf_stepper* st, void* stream) {
 int wf_ensemble_create(const wf_case* cases, int32_t ncases, int32_t mode, wf_ensemble** out) {
   if (!cases || !out || ncases < 1) return fail(WF_EINVAL, "null argument or no cases");
   *out = nullptr;
-  if (mode & ~WF_STEP_SERIAL) return fail(WF_EINVAL, "ensemble mode: 0 or WF_STEP_SERIAL");
+  if (mode & ~(WF_STEP_SERIAL | WF_ENS_BUCKETS))
+    return fail(WF_EINVAL, "ensemble mode: 0, WF_STEP_SERIAL and/or WF_ENS_BUCKETS");
   for (int i = 0; i < ncases; ++i) WF_TRY(validate_case(cases[i]));
   PdlOff guard((mode & WF_STEP_SERIAL) != 0);
-  cudaGraph_t g = nullptr;
-  WF_CK(cudaGraphCreate(&g, 0));
+  wf_ensemble* en = new wf_ensemble();
+  en->ncases = ncases;
+  en->graph = nullptr;
+  en->exec = nullptr;
+  en->bucket_of_case.assign(ncases, -1);
+  cudaError_t e = cudaGraphCreate(&en->graph, 0);
+  if (e != cudaSuccess) {
+    delete en;
+    return cuda_fail(e, "cudaGraphCreate(ensemble)");
+  }
   int rc = WF_OK;
-  int32_t counts[4];
-  for (int i = 0; i < ncases && rc == WF_OK; ++i) rc = append_step(g, cases[i], counts);
-  wf_ensemble* en = nullptr;
+  if (mode & WF_ENS_BUCKETS) {
+    // group the cases, at most bucket_cap(case) to a bucket
+    std::vector<std::vector<int>> buckets;
+    for (int i = 0; i < ncases; ++i) {
+      const int cap = bucket_cap(cases[i]);
+      bool placed = false;
+      for (auto& b : buckets)
+        if ((int)b.size() < cap && same_bucket(cases[b[0]], cases[i])) {
+          b.push_back(i);
+          placed = true;
+          break;
+        }
+      if (!placed) buckets.push_back({i});
+    }
+    for (size_t bi = 0; bi < buckets.size() && rc == WF_OK; ++bi) {
+      const auto& b = buckets[bi];
+      std::vector<CasePtrs> rows;
+      for (int i : b) {
+        rows.push_back(ptrs_of(cases[i]));
+        en->bucket_of_case[i] = (int32_t)bi;
+      }
+      void* tab = nullptr;
+      e = cudaMalloc(&tab, rows.size() * sizeof(CasePtrs));
+      if (e != cudaSuccess) { rc = cuda_fail(e, "cudaMalloc(bucket table)"); break; }
+      en->tables.push_back(tab);
+      e = cudaMemcpy(tab, rows.data(), rows.size() * sizeof(CasePtrs), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) { rc = cuda_fail(e, "cudaMemcpy(bucket table)"); break; }
+      int32_t counts[4] = {0, 0, 0, 0};
+      rc = append_step(en->graph, cases[b[0]], counts, (const CasePtrs*)tab, (int)b.size());
+      en->counts.insert(en->counts.end(), counts, counts + 4);
+    }
+  } else {
+    for (int i = 0; i < ncases && rc == WF_OK; ++i) {
+      int32_t counts[4] = {0, 0, 0, 0};
+      rc = append_step(en->graph, cases[i], counts);
+      en->counts.insert(en->counts.end(), counts, counts + 4);
+    }
+  }
   if (rc == WF_OK) {
-    en = new wf_ensemble();
-    en->ncases = ncases;
-    en->graph = g;
-    en->exec = nullptr;
-    const cudaError_t e = cudaGraphInstantiate(&en->exec, g, 0);
+    e = cudaGraphInstantiate(&en->exec, en->graph, 0);
     if (e != cudaSuccess) rc = cuda_fail(e, "cudaGraphInstantiate(ensemble)");
   }
   if (rc != WF_OK) {
-    if (en) {
-      wf_ensemble_destroy(en);
-    } else {
-      cudaGraphDestroy(g);
-    }
+    wf_ensemble_destroy(en);
     return rc;
   }
   *out = en;
+  return WF_OK;
+}
+
+int wf_mg_solve_bucket(const wf_case* cases, int32_t ncases, void* table, void* stream) {
+  if (!cases || ncases < 1 || !table) return fail(WF_EINVAL, "null argument or no cases");
+  if (ncases > std::max(1, 60000 / (cases[0].n + 2 * NPL)))
+    return fail(WF_EINVAL, "wf_mg_solve_bucket: too many cases for one launch");
+  for (int i = 0; i < ncases; ++i) {
+    WF_TRY(validate_case(cases[i]));
+    if (!same_bucket(cases[0], cases[i]))
+      return fail(WF_EINVAL, "wf_mg_solve_bucket: the cases differ in size or numerics");
+  }
+  std::vector<CasePtrs> rows;
+  for (int i = 0; i < ncases; ++i) rows.push_back(ptrs_of(cases[i]));
+  cudaStream_t s = (cudaStream_t)stream;
+  WF_CK(cudaMemcpyAsync(table, rows.data(), rows.size() * sizeof(CasePtrs),
+                        cudaMemcpyHostToDevice, s));
+  WF_CK(cudaStreamSynchronize(s));   // the rows live on this thread's stack
+  BatchScope bs((const CasePtrs*)table, ncases, 0);
+  return mg_solve(cases[0], s);
+}
+
+int wf_mg_bucket_table_bytes(int32_t ncases, int64_t* bytes) {
+  if (!bytes || ncases < 1) return fail(WF_EINVAL, "null argument or no cases");
+  *bytes = (int64_t)ncases * (int64_t)sizeof(CasePtrs);
+  return WF_OK;
+}
+
+int wf_ensemble_layout(const wf_ensemble* en, int32_t* nbuckets, int32_t* bucket_of_case,
+                       int32_t* counts) {
+  if (!en || !nbuckets) return fail(WF_EINVAL, "null argument");
+  const int nb = en->tables.empty() ? en->ncases : (int)en->tables.size();
+  *nbuckets = nb;
+  if (bucket_of_case)
+    for (int i = 0; i < en->ncases; ++i) bucket_of_case[i] = en->bucket_of_case[i];
+  if (counts)
+    for (size_t i = 0; i < en->counts.size(); ++i) counts[i] = en->counts[i];
   return WF_OK;
 }
 
@@ -487,6 +684,7 @@ int wf_ensemble_destroy(wf_ensemble* en) {
   if (!en) return WF_OK;
   if (en->exec) cudaGraphExecDestroy(en->exec);
   if (en->graph) cudaGraphDestroy(en->graph);
+  for (void* t : en->tables) cudaFree(t);
   delete en;
   return WF_OK;
 }

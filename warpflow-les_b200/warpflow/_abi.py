@@ -41,6 +41,8 @@ class WfScalars(ctypes.Structure):
         ("ticket", ctypes.c_uint32),
         ("nmg", ctypes.c_int32),
         ("gbar", ctypes.c_uint32 * 2),
+        ("bticket", ctypes.c_uint32),
+        ("bflags", ctypes.c_int32),
     ]
 
 
@@ -87,6 +89,10 @@ SIGNATURES = {
     "wf_struct_sizes": (_I32, [ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
     "wf_scalars_init": (_I32, [_VP, _D, _D, _D, _VP]),
     "wf_set_coarse_strategy": (_I32, [_I32, _I32, _I32]),
+    "wf_set_launch_shape": (_I32, [_I32, _I32, _I32, _I32]),
+    "wf_launch_shape": (_I32, [_I32, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_I32)]),
+    "wf_set_bucket_cap": (_I32, [_I32, _I32, _I32]),
+    "wf_bucket_cap": (_I32, [_I32, _I32, ctypes.POINTER(_I32)]),
     "wf_mg_level_elems": (_I32, [_I32, _I32, _I32, ctypes.POINTER(ctypes.c_int64)]),
     "wf_mg_coarse_op_elems": (_I32, [_CP, ctypes.POINTER(ctypes.c_int64),
                                      ctypes.POINTER(ctypes.c_int64)]),
@@ -111,6 +117,8 @@ SIGNATURES = {
     "wf_mg_solve_noalloc": (_I32, [_VP, _VP, _I32, _I32, _D, _D, _D, _VP]),
     "wf_mg_noalloc_status": (_I32, [_VP, ctypes.POINTER(_I32)]),
     "wf_wait_probe": (_I32, [_VP, _VP, _I32, _I32, _VP]),
+    "wf_mg_solve_bucket": (_I32, [_CP, _I32, _VP, _VP]),
+    "wf_mg_bucket_table_bytes": (_I32, [_I32, ctypes.POINTER(ctypes.c_int64)]),
     "wf_mg_vcycle": (_I32, [_CP, _VP, _VP, _VP]),
     "wf_mg_relax": (_I32, [_CP, _VP, _VP, _I32, _VP]),
     "wf_mg_dc_cycle": (_I32, [_CP, _VP, _VP, _VP]),
@@ -122,6 +130,8 @@ SIGNATURES = {
     "wf_ensemble_create": (_I32, [_CP, _I32, _I32, ctypes.POINTER(_VP)]),
     "wf_ensemble_step": (_I32, [_VP, _VP]),
     "wf_ensemble_destroy": (_I32, [_VP]),
+    "wf_ensemble_layout": (_I32, [_VP, ctypes.POINTER(_I32), ctypes.POINTER(_I32),
+                                  ctypes.POINTER(_I32)]),
     "wf_stepper_launch_counts": (_I32, [_VP, ctypes.POINTER(_I32)]),
 }
 

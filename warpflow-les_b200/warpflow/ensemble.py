@@ -1,13 +1,14 @@
 """Many independent cavity cases advanced together on one GPU.
 
-Each case keeps its fields and multigrid hierarchy resident on the device
-and owns one captured CUDA graph for its whole step (the projection loop
-inside it is device-driven, so cases that need more outer iterations do not
-hold the others back on the host).  A step of the ensemble launches every
-active case's graph on a pool of streams so that their kernels run
-concurrently -- a small case's latency-bound coarse solve overlaps with a
-large case's bandwidth-bound sweeps -- then gathers all scalar blocks with
-one device-to-host copy.
+Each case keeps its fields and multigrid hierarchy resident on the device.
+A step of the ensemble is one launch of one CUDA graph holding every case's
+step (the projection loops inside it are device-driven, so cases that need
+more outer iterations do not hold the others back on the host): small cases
+of one size share every kernel launch as a bucket, large cases run as
+concurrent branches -- a small case's latency-bound coarse solve overlaps
+with a large case's bandwidth-bound sweeps.  All scalar blocks come back
+with one device-to-host copy.  Once a case retires, the remaining cases'
+own graphs are launched on a pool of streams instead.
 
 The 64-case benchmark ensemble (N in {32, 48, 64, 80, 96}, Re in
 [100, 1000], lid velocity in [0.5, 1.5], seeded) is built by
@@ -25,6 +26,8 @@ from . import _abi
 from .config import case_from_dict
 from .fields import cuda_device
 from .solver import STEP_SERIAL, FlowSolver
+
+ENS_BUCKETS = 4   # WF_ENS_BUCKETS
 from .topology import build_topology
 
 
@@ -65,13 +68,15 @@ class Ensemble:
     info dict per case (or the exception a case raised, which retires it).
 
     With ``single_graph`` (default) all cases' steps also form ONE CUDA graph
-    (``wf_ensemble_create``: every case an independent branch), and a step
-    of the whole ensemble is one graph launch; once a case has retired, or
-    for a subset, the cases' own graphs are launched on a pool of
-    ``nstreams`` streams instead.
+    (``wf_ensemble_create``), and a step of the whole ensemble is one graph
+    launch.  With ``buckets`` (default) cases of the same size and numerics
+    share their launches: each bucket is one branch of the graph whose every
+    kernel serves all its cases (``WF_ENS_BUCKETS``); without it every case
+    is a branch of its own.  Once a case has retired, or for a subset, the
+    cases' own graphs are launched on a pool of ``nstreams`` streams instead.
     """
 
-    def __init__(self, cfgs, device="cuda:0", nstreams=32, single_graph=True):
+    def __init__(self, cfgs, device="cuda:0", nstreams=32, single_graph=True, buckets=True):
         self.device = cuda_device(device)
         # Concurrent cases: kernels that wait for their predecessor while
         # resident would hold SMs other streams could use.
@@ -80,10 +85,12 @@ class Ensemble:
                                    serial=concurrent) for cfg in cfgs]
         self.active = [True] * len(self.solvers)
         self._graph = None
+        self.buckets = bool(buckets and single_graph)
         if single_graph and len(self.solvers) > 1:
             arr = (_abi.WfCase * len(self.solvers))(*[sv.case for sv in self.solvers])
             self._graph = ctypes.c_void_p()
-            _abi.call("wf_ensemble_create", arr, len(self.solvers), STEP_SERIAL,
+            mode = STEP_SERIAL | (ENS_BUCKETS if self.buckets else 0)
+            _abi.call("wf_ensemble_create", arr, len(self.solvers), mode,
                       ctypes.byref(self._graph))
         ns = max(1, min(nstreams, len(self.solvers)))
         self.streams = [torch.cuda.Stream(self.device) for _ in range(ns)]
@@ -94,6 +101,33 @@ class Ensemble:
 
     def __len__(self):
         return len(self.solvers)
+
+    def layout(self):
+        """(bucket of each case, launch counts per bucket: prologue, calmas
+        pass, multigrid part, epilogue) of the one-graph step; without
+        buckets every case is its own."""
+        if self._graph is None:
+            return list(range(len(self))), [s.launch_counts() for s in self.solvers]
+        n = len(self.solvers)
+        nb = ctypes.c_int32()
+        of = (ctypes.c_int32 * n)()
+        counts = (ctypes.c_int32 * (4 * n))()
+        _abi.call("wf_ensemble_layout", self._graph, ctypes.byref(nb), of, counts)
+        bucket = list(of) if self.buckets else list(range(n))
+        return bucket, [tuple(counts[4 * b:4 * b + 4]) for b in range(nb.value)]
+
+    def launches_per_step(self):
+        """Kernel launches of the last one-graph step: per bucket (or case),
+        the prologue and epilogue once, the calmas pass per outer iteration
+        and the multigrid part per solve of its busiest case."""
+        bucket, counts = self.layout()
+        total = 0
+        for b, (c0, c1, c2, c3) in enumerate(counts):
+            members = [self.solvers[i] for i in range(len(self)) if bucket[i] == b]
+            it = max(s.outer_iters for s in members)
+            nmg = max(s.last_nmg for s in members)
+            total += c0 + c3 + it * c1 + nmg * c2
+        return total
 
     def cells(self, which=None):
         idx = self._which(which)

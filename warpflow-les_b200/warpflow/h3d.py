@@ -149,8 +149,11 @@ def export(sol, outdir):
 
 def import_restart(sol, path):
     """Load a tecbin dump's real cells of u, v, w, p and vis into `sol` and
-    rebuild this package's ghost layers on the device (the initial fills of
-    the velocities and pressure, the vis fill)."""
+    rebuild this package's ghost layers on the device as a fresh solver's
+    are built: ghosts zeroed, then the initial fills of the velocities and
+    pressure and the vis fill.  (The fills are ordered face sequences whose
+    edge and corner values depend on what the ghosts held before, so the
+    ghosts are rebuilt from zero rather than from whatever `sol` held.)"""
     import ctypes
 
     from . import _abi
@@ -158,7 +161,7 @@ def import_restart(sol, path):
     got = read_tecbin(path, n)
     core = slice(NPL, NPL + n)
     for name in ("u", "v", "w", "p", "vis"):
-        a = sol.f[name].numpy()
+        a = np.zeros(sol.f[name].shape)
         a[core, core, core] = got[name]
         sol.f[name].assign(a)
     s = sol._stream()
