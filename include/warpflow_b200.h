@@ -131,15 +131,16 @@ WF_API int wf_scalars_init(wf_scalars* sc, double dt0, double rrey, double ulid,
 WF_API int wf_set_coarse_strategy(int32_t n, int32_t fp32, int32_t strategy);
 /* Tuning knob (no reference counterpart): the launch shape of a kernel for
  * size n.  kind 0 = the convection pass (k_conv): a x b threads per CTA, a
- * along k (a power of two), b along j, a*b a multiple of 32 and <= 256;
- * default 32 x 8.  kind 1 = the split red-black half-sweep of an n^3 level
- * (k_rbgs_split): a = cells per thread (1, 2, 4), b = rows per CTA (1, 2,
- * 4, 8); default 2 x 8.  a = b = 0 restores the default.  Results do not
+ * along k (a power of two), b along j, a*b a multiple of 32 and <= 256,
+ * and c consecutive planes i per thread (1..16); default 32 x 8 x 1.
+ * kind 1 = the split red-black half-sweep of an n^3 level (k_rbgs_split):
+ * a = cells per thread (1, 2, 4), b = rows per CTA (1, 2, 4, 8), c = 1;
+ * default 2 x 8 x 1.  a = b = c = 0 restores the default.  Results do not
  * depend on the shape (each cell's arithmetic is the same).  Process-wide;
  * read when a launch is issued, so set it before steppers are built.
  * wf_launch_shape reads the shape in force. */
-WF_API int wf_set_launch_shape(int32_t kind, int32_t n, int32_t a, int32_t b);
-WF_API int wf_launch_shape(int32_t kind, int32_t n, int32_t* a, int32_t* b);
+WF_API int wf_set_launch_shape(int32_t kind, int32_t n, int32_t a, int32_t b, int32_t c);
+WF_API int wf_launch_shape(int32_t kind, int32_t n, int32_t* a, int32_t* b, int32_t* c);
 /* bytes of MG workspace a case needs at each level (caller allocates) */
 WF_API int wf_mg_level_elems(int32_t n, int32_t nlev, int32_t level, int64_t* elems);
 /* No counterpart in the reference.  The coarsest-level relax of a V-cycle
@@ -305,9 +306,11 @@ WF_API int wf_stepper_destroy(wf_stepper* s);
  * per bucket or case (prologue, calmas pass, multigrid part, epilogue).
  * A bucket holds at most wf_bucket_cap(n, mg_fp32) cases of its size: by
  * default as many as keep their finest multigrid level within half the L2
- * below n = 64, and 1 (a branch per case, measured faster there) from 64
- * on; wf_set_bucket_cap(n, fp32, cap) overrides it per size (cap 0
- * restores the default; process-wide, read when an ensemble is created). */
+ * (and the stacked grid within the z limit); wf_set_bucket_cap(n, fp32,
+ * cap) overrides it per size (1 = a branch per case, 0 restores the
+ * default; process-wide, read when an ensemble is created).  Buckets pay
+ * for ensembles of one size; for a mix of sizes a branch per case (mode
+ * without WF_ENS_BUCKETS) measured faster on B200. */
 #define WF_ENS_BUCKETS 4
 WF_API int wf_set_bucket_cap(int32_t n, int32_t fp32, int32_t cap);
 WF_API int wf_bucket_cap(int32_t n, int32_t fp32, int32_t* cap);

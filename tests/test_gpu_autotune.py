@@ -44,23 +44,23 @@ def test_tune_buckets_installs_faster_form(tmp_path):
 def test_tune_shapes_and_bit_identical_step():
     """The shape tuner times k_conv and k_rbgs_split shapes at 80^3 (each
     checked bit-identical to the default), installs the fastest, and a
-    solver built with non-default shapes steps exactly like one built with
-    the defaults."""
+    solver built with non-default shapes (several planes per thread) steps
+    exactly like one built with the defaults, alone and in a bucket."""
     from warpflow import FlowSolver, autotune, build_topology
     from warpflow.ensemble import cavity_case
     try:
-        table = autotune.tune_shapes(sizes=(80,), conv=((32, 8), (16, 16), (64, 4)),
-                                     split=((2, 8), (1, 4), (4, 2)), reps=3)
+        table = autotune.tune_shapes(sizes=(80,), conv=((32, 8, 1), (16, 16, 3), (64, 4, 8)),
+                                     split=((2, 8, 1), (1, 4, 1), (4, 2, 1)), reps=3)
         for kind in ("conv", "split"):
             rec = table[kind][80]
             assert tuple(autotune.shape(kind, 80)) == tuple(rec["best"])
-            assert min(rec["us"].values()) == rec["us"]["%dx%d" % tuple(rec["best"])]
+            assert min(rec["us"].values()) == rec["us"]["%dx%dx%d" % tuple(rec["best"])]
         cfg = cavity_case(80, precision="fp64")
-        autotune.set_shape("conv", 80, 16, 16)
+        autotune.set_shape("conv", 80, 16, 16, 3)
         autotune.set_shape("split", 80, 4, 2)
         a = FlowSolver(cfg, build_topology(cfg), "cuda:0")
-        autotune.set_shape("conv", 80, 0, 0)
-        autotune.set_shape("split", 80, 0, 0)
+        autotune.set_shape("conv", 80, 0, 0, 0)
+        autotune.set_shape("split", 80, 0, 0, 0)
         b = FlowSolver(cfg, build_topology(cfg), "cuda:0")
         for _ in range(2):
             assert a.step() == b.step()
@@ -69,8 +69,30 @@ def test_tune_shapes_and_bit_identical_step():
         a.close()
         b.close()
     finally:
-        autotune.set_shape("conv", 80, 0, 0)
-        autotune.set_shape("split", 80, 0, 0)
+        autotune.set_shape("conv", 80, 0, 0, 0)
+        autotune.set_shape("split", 80, 0, 0, 0)
+
+
+def test_conv_planes_in_a_bucket():
+    """Several planes per thread in a bucket launch (grid z = cases x plane
+    groups, the last group short): each case as alone."""
+    from warpflow import FlowSolver, autotune, build_topology
+    from warpflow.ensemble import Ensemble, cavity_case
+    cfgs = [cavity_case(24, re, 1.0, precision="fp64") for re in (200.0, 700.0)]
+    try:
+        autotune.set_shape("conv", 24, 32, 4, 5)
+        ens = Ensemble(cfgs, nstreams=1)
+        assert ens.layout()[0] == [0, 0]
+        autotune.set_shape("conv", 24, 0, 0, 0)
+        alone = [FlowSolver(c, build_topology(c), "cuda:0") for c in cfgs]
+        for _ in range(2):
+            assert ens.step() == [s.step() for s in alone]
+        for sol, ref in zip(ens.solvers, alone):
+            for name in ("u", "v", "w", "p"):
+                np.testing.assert_array_equal(sol.f[name].numpy(), ref.f[name].numpy())
+        ens.close()
+    finally:
+        autotune.set_shape("conv", 24, 0, 0, 0)
 
 
 @pytest.mark.parametrize("n", [8, 12, 16, 20, 24])

@@ -73,7 +73,10 @@ def test_bucketed_ensemble_matches_alone(precision):
     from warpflow import FlowSolver, build_topology
     from warpflow.ensemble import Ensemble, cavity_case
     cfgs = [cavity_case(n, re, u, precision=precision, noise=nz) for n, re, u, nz in BUCKET_SPECS]
-    ens = Ensemble(cfgs, nstreams=2)
+    mixed = Ensemble(cfgs[:2], nstreams=1)      # two sizes: a branch per case by default
+    assert not mixed.buckets and mixed.layout()[0] == [0, 1]
+    mixed.close()
+    ens = Ensemble(cfgs, nstreams=2, buckets=True)
     bucket, counts = ens.layout()
     assert len(counts) == 3 and bucket[0] == bucket[2] == bucket[4] != bucket[1]
     alone = [FlowSolver(c, build_topology(c), "cuda:0") for c in cfgs]
@@ -145,7 +148,8 @@ def test_bucket_with_cluster_coarse_sweeps():
         c = cavity_case(48, re, 1.0, levels=2, precision="fp64")
         c.numerics.mg_coarse = "sweeps"
         cfgs.append(c)
-    ens = Ensemble(cfgs, nstreams=1)
+    ens = Ensemble(cfgs, nstreams=1)          # one size: bucketed by default
+    assert ens.buckets
     bucket, counts = ens.layout()
     assert len(counts) == 1 and bucket == [0, 0, 0]
     alone = [FlowSolver(c, build_topology(c), "cuda:0") for c in cfgs]

@@ -1,8 +1,8 @@
 """The ensemble's bucket-size rule (host logic only, no GPU call): cases
-below 64^3 share launches up to what keeps their finest multigrid level
-within half the L2 and the stacked grid within the z limit; from 64^3 on
-each case is its own branch; a cap set per size overrides the rule and is
-clipped to the grid limit; the autotuner's JSON cache re-installs it."""
+of one size share launches up to what keeps their finest multigrid level
+within half the L2 and the stacked grid within the z limit; a cap set per
+size overrides the rule and is clipped to the grid limit; the autotuner's
+JSON cache re-installs it."""
 import json
 
 import pytest
@@ -20,17 +20,16 @@ def _rule(n, fp32):
 
 @pytest.mark.parametrize("fp32", [True, False])
 def test_default_rule(fp32):
-    for n in (8, 16, 32, 48, 56):
+    for n in (8, 16, 32, 48, 56, 64, 80, 96, 128, 256):
         assert _cap(n, fp32) == _rule(n, fp32), n
-    for n in (64, 80, 96, 128, 256):
-        assert _cap(n, fp32) == 1, n
+    assert _cap(256, fp32) == 1 and _cap(96, True) == 8 and _cap(80, True) == 15
 
 
 def test_override_and_clip():
     from warpflow import _abi, autotune
     try:
         autotune.set_bucket_cap(80, 6)
-        assert _cap(80) == 6 and _cap(80, fp32=False) == 1
+        assert _cap(80) == 6 and _cap(80, fp32=False) == _rule(80, False)
         autotune.set_bucket_cap(32, 10 ** 6)
         assert _cap(32) == 60000 // (32 + 6)
         autotune.set_bucket_cap(32, 1)
@@ -38,7 +37,7 @@ def test_override_and_clip():
     finally:
         autotune.set_bucket_cap(80, 0)
         autotune.set_bucket_cap(32, 0)
-    assert _cap(80) == 1 and _cap(32) == _rule(32, True)
+    assert _cap(80) == _rule(80, True) and _cap(32) == _rule(32, True)
     with pytest.raises(RuntimeError):
         autotune.set_bucket_cap(2, 4)
     with pytest.raises(RuntimeError):
@@ -68,25 +67,26 @@ def test_launch_shapes_set_validate_and_cache(tmp_path):
     """Launch-shape table (host only): defaults, accepted and rejected
     shapes, reset, and the JSON cache."""
     from warpflow import autotune
-    assert autotune.shape("conv", 80) == (32, 8)
-    assert autotune.shape("split", 80) == (2, 8)
+    assert autotune.shape("conv", 80) == (32, 8, 1)
+    assert autotune.shape("split", 80) == (2, 8, 1)
     try:
-        autotune.set_shape("conv", 80, 16, 16)
+        autotune.set_shape("conv", 80, 16, 16, 4)
         autotune.set_shape("split", 80, 4, 2)
-        assert autotune.shape("conv", 80) == (16, 16)
-        assert autotune.shape("split", 80) == (4, 2)
-        assert autotune.shape("conv", 96) == (32, 8)      # per size
-        for kind, a, b in (("conv", 24, 8), ("conv", 32, 16), ("conv", 16, 1),
-                           ("split", 3, 8), ("split", 2, 16)):
+        assert autotune.shape("conv", 80) == (16, 16, 4)
+        assert autotune.shape("split", 80) == (4, 2, 1)
+        assert autotune.shape("conv", 96) == (32, 8, 1)      # per size
+        for kind, a, b, c in (("conv", 24, 8, 1), ("conv", 32, 16, 1), ("conv", 16, 1, 1),
+                              ("conv", 32, 8, 0), ("conv", 32, 8, 17),
+                              ("split", 3, 8, 1), ("split", 2, 16, 1), ("split", 2, 8, 2)):
             with pytest.raises(RuntimeError):
-                autotune.set_shape(kind, 80, a, b)
+                autotune.set_shape(kind, 80, a, b, c)
         p = tmp_path / "tune.json"
-        autotune.save({}, p, shapes={"conv": {80: {"best": [64, 4], "us": {}}},
-                                     "split": {80: {"best": [1, 4], "us": {}}}})
+        autotune.save({}, p, shapes={"conv": {80: {"best": [64, 4, 2], "us": {}}},
+                                     "split": {80: {"best": [1, 4, 1], "us": {}}}})
         autotune.load_and_apply(p)
-        assert autotune.shape("conv", 80) == (64, 4)
-        assert autotune.shape("split", 80) == (1, 4)
+        assert autotune.shape("conv", 80) == (64, 4, 2)
+        assert autotune.shape("split", 80) == (1, 4, 1)
     finally:
-        autotune.set_shape("conv", 80, 0, 0)
-        autotune.set_shape("split", 80, 0, 0)
-    assert autotune.shape("conv", 80) == (32, 8)
+        autotune.set_shape("conv", 80, 0, 0, 0)
+        autotune.set_shape("split", 80, 0, 0, 0)
+    assert autotune.shape("conv", 80) == (32, 8, 1)

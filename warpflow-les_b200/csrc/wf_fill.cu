@@ -23,10 +23,13 @@ struct FaceOp {
 constexpr int MAX_OPS_PER_PHASE = 4;
 constexpr int MAX_JOBS = 3;
 
+constexpr int MAX_LAYERS = NPL;
+
 struct PhaseJob {
   double* fld;
   int fid, vsrc;   // bucket launches: the field's slot, the source of valp (1 ulid, 2 rrey)
   int nops;
+  int indep;       // no op reads a cell that an op of this job writes: loads may go first
   FaceOp ops[MAX_OPS_PER_PHASE];
 };
 
@@ -53,6 +56,45 @@ __global__ void k_fill_phase(const PhaseArgs args, const Batch bt) {
     const CasePtrs& cp = bt.tab[bt_case(bt)];
     f = cp.fld[J.fid];
     valp = J.vsrc == 1 ? &cp.sc->ulid : (J.vsrc == 2 ? &cp.sc->rrey : nullptr);
+  }
+  if (J.indep) {
+    // every source of the job is read before any ghost is written (the host
+    // checked that no source is a cell the job writes), so a thread's loads
+    // are independent and in flight together instead of one per layer
+    double val[MAX_OPS_PER_PHASE][MAX_LAYERS];
+    long gidx[MAX_OPS_PER_PHASE][MAX_LAYERS];
+#pragma unroll
+    for (int o = 0; o < MAX_OPS_PER_PHASE; ++o) {
+#pragma unroll
+      for (int m = 0; m < MAX_LAYERS; ++m) gidx[o][m] = -1;
+      if (o >= J.nops) continue;
+      const FaceOp& op = J.ops[o];
+      if (a >= op.na || b >= op.nb) continue;
+      const int pa = op.a0 + a, pb = op.b0 + b;
+#pragma unroll
+      for (int m = 0; m < MAX_LAYERS; ++m) {
+        if (m >= op.nlay) continue;
+        const int g = op.high ? op.g0 + m : op.g0 - m;
+        gidx[o][m] = op.axis == 0 ? ((long)g * P + pa) * P + pb
+                                  : (op.axis == 1 ? ((long)pa * P + g) * P + pb
+                                                  : ((long)pa * P + pb) * P + g);
+        if (op.lin) {
+          const int sidx = op.high ? op.s0 - m : op.s0 + m;
+          const long si = op.axis == 0 ? ((long)sidx * P + pa) * P + pb
+                                       : (op.axis == 1 ? ((long)pa * P + sidx) * P + pb
+                                                       : ((long)pa * P + pb) * P + sidx);
+          val[o][m] = op.val * f[si];
+        } else {
+          val[o][m] = op.valp ? *(valp ? valp : op.valp) : op.val;
+        }
+      }
+    }
+#pragma unroll
+    for (int o = 0; o < MAX_OPS_PER_PHASE; ++o)
+#pragma unroll
+      for (int m = 0; m < MAX_LAYERS; ++m)
+        if (gidx[o][m] >= 0) f[gidx[o][m]] = val[o][m];
+    return;
   }
   for (int o = 0; o < J.nops; ++o) {
     const FaceOp& op = J.ops[o];
@@ -93,6 +135,32 @@ static FaceOp lin(int axis, int high, int g0, int s0, double sign, int a0, int n
 static FaceOp cst(int axis, int high, int g0, double val, int a0, int na, int b0,
                   int nb, int nlay, const double* valp = nullptr) {
   return FaceOp{axis, high, 0, nlay, g0, 0, val, a0, na, b0, nb, valp};
+}
+
+// true when no op of the list reads a cell that an op of the list writes
+// (the ops of one phase share its axis, so it suffices to compare the layer
+// indices along the axis and the (a, b) rectangles): then every load may
+// precede every store and the result is the same as in program order
+static bool ops_independent(const FaceOp* ops, int nops) {
+  for (int w = 0; w < nops; ++w)
+    if (ops[w].nlay > MAX_LAYERS) return false;   // the kernel's hoisted form holds MAX_LAYERS
+  for (int r = 0; r < nops; ++r) {
+    if (!ops[r].lin) continue;
+    for (int w = 0; w < nops; ++w) {
+      if (ops[w].axis != ops[r].axis) return false;
+      const bool overlap_ab = ops[r].a0 < ops[w].a0 + ops[w].na && ops[w].a0 < ops[r].a0 + ops[r].na &&
+                              ops[r].b0 < ops[w].b0 + ops[w].nb && ops[w].b0 < ops[r].b0 + ops[r].nb;
+      if (!overlap_ab) continue;
+      for (int mr = 0; mr < ops[r].nlay; ++mr) {
+        const int src = ops[r].high ? ops[r].s0 - mr : ops[r].s0 + mr;
+        for (int mw = 0; mw < ops[w].nlay; ++mw) {
+          const int dst = ops[w].high ? ops[w].g0 + mw : ops[w].g0 - mw;
+          if (src == dst) return false;
+        }
+      }
+    }
+  }
+  return true;
 }
 
 // phase ops of one fill kind; returns op count for `phase` (0 = x, 1 = y, 2 = z)
@@ -179,6 +247,7 @@ int launch_fills(const FillReq* reqs, int nreq, int n, cudaStream_t s) {
       a.job[r].fid = reqs[r].fid;
       a.job[r].vsrc = reqs[r].vsrc;
       a.job[r].nops = program(reqs[r].kind, n, reqs[r].val, reqs[r].valp, phase, a.job[r].ops);
+      a.job[r].indep = ops_independent(a.job[r].ops, a.job[r].nops) ? 1 : 0;
       for (int o = 0; o < a.job[r].nops; ++o) {
         a.amax = a.job[r].ops[o].na > a.amax ? a.job[r].ops[o].na : a.amax;
         a.bmax = a.job[r].ops[o].nb > a.bmax ? a.job[r].ops[o].nb : a.bmax;

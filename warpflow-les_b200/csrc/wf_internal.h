@@ -157,13 +157,14 @@ int launch_add_ring(double* p, const double* pp, int n, cudaStream_t s);
 int launch_scalars_init(wf_scalars* sc, double dt0, double rrey, double ulid, cudaStream_t s);
 
 // ---- launch shapes chosen per size --------------------------------------
-// kind SHAPE_CONV: k_conv's CTA, a = extent along k (x), b = along j (y);
-// kind SHAPE_SPLIT: k_rbgs_split, a = cells per thread, b = rows per CTA.
-// Process-wide, read when a launch is issued (a graph keeps the shapes it
-// was captured with); set by wf_set_launch_shape (the autotuner).
+// kind SHAPE_CONV: k_conv's CTA, a = extent along k (x), b = along j (y),
+// c = planes i per thread; kind SHAPE_SPLIT: k_rbgs_split, a = cells per
+// thread, b = rows per CTA (c = 1).  Process-wide, read when a launch is
+// issued (a graph keeps the shapes it was captured with); set by
+// wf_set_launch_shape (the autotuner).
 constexpr int SHAPE_CONV = 0, SHAPE_SPLIT = 1;
-void launch_shape(int kind, int n, int* a, int* b);
-int set_launch_shape(int kind, int n, int a, int b);
+void launch_shape(int kind, int n, int* a, int* b, int* c);
+int set_launch_shape(int kind, int n, int a, int b, int c);
 
 // ---- multigrid -----------------------------------------------------------
 int mg_solve(const wf_case& c, cudaStream_t s);

@@ -1274,6 +1274,7 @@ static int try_coarse_tb(const Lvl<T>& L, int nsweeps, cudaStream_t s, int* rc) 
 // equal the mathematical S to rounding, so the relax agrees with the
 // sweeps to rounding.
 constexpr int COP_GMAX = 24;
+static_assert(COP_GMAX <= 32, "k_cop_gemm writes symmetry q from lane q");
 
 static bool cop_size_ok(int nc) {
   return nc == 4 || nc == 8 || nc == 12 || nc == 16 || nc == 20 || nc == 24;
@@ -1304,7 +1305,7 @@ struct CopPlan {
   }
 };
 
-constexpr int COP_RB = 4;   // representatives per CTA of k_cop_gemm
+constexpr int COP_RB = 16;  // representatives per CTA of k_cop_gemm (2 per warp)
 constexpr int COP_KS = 8;   // slices of the B cells (the product's sum) per output
 
 // per-case scratch of the operator product: the permuted copies of v_B
@@ -1473,10 +1474,13 @@ template <> struct Vec2<double> { using type = double2; };
 template <> struct Vec2<float> { using type = float2; };
 
 // Y_s[x][g] = sum over the s-th slice of B cells u of C[x][u] * V[g][u]:
-// a CTA takes COP_RB representatives x and one slice; warp w the symmetries
-// 3w .. 3w+2; lanes step through the slice two cells at a time (2-vector
-// loads, two steps in flight), each summing its cells in ascending order,
-// then the lanes are added by a butterfly (fixed order)
+// a CTA takes COP_RB representatives x and one slice, and first copies the
+// slice of every permuted copy V[g] into shared memory (each CTA reads it
+// once from L2; the operator rows are read once in all); warp w takes the
+// representatives x0 + 2w, x0 + 2w + 1 and every symmetry; lanes step
+// through the slice two cells at a time (2-vector loads), each summing its
+// cells in ascending order, then the lanes are added by a butterfly (fixed
+// order)
 template <class T>
 __global__ void __launch_bounds__(256) k_cop_gemm(const T* C, const T* V, T* Y, int nrep,
                                                   int M, int ng, const Batch bt) {
@@ -1487,57 +1491,69 @@ __global__ void __launch_bounds__(256) k_cop_gemm(const T* C, const T* V, T* Y, 
     Y = (T*)bt.tab[bt_case(bt)].mg_cop_part + (long)COP_GMAX * M;
   }
   using V2 = typename Vec2<T>::type;
+  extern __shared__ __align__(16) unsigned char cop_smem[];
+  V2* sv = reinterpret_cast<V2*>(cop_smem);   // [ng][nh]: this slice of every V[g]
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int x0 = blockIdx.x * COP_RB, s = blockIdx.y;
   const int per = (((M + COP_KS - 1) / COP_KS) + 1) & ~1;   // even: 2-vector aligned
   const int h0 = s * per / 2, h1 = min(M, s * per + per) / 2;   // 2-vector range
-  const int g0 = 3 * w;
-  T acc[COP_RB][3];
+  const int nh = max(0, h1 - h0);
+  for (int t = threadIdx.x; t < ng * nh; t += blockDim.x) {
+    const int g = t / nh, h = t - g * nh;
+    sv[t] = reinterpret_cast<const V2*>(V + (long)g * M)[h0 + h];
+  }
+  __syncthreads();
+  const int r0 = x0 + 2 * w;
+  T acc[2][COP_GMAX];
 #pragma unroll
-  for (int r = 0; r < COP_RB; ++r)
-#pragma unroll
-    for (int q = 0; q < 3; ++q) acc[r][q] = T(0);
-  if (g0 < ng) {
-    const V2* cr[COP_RB];
-#pragma unroll
-    for (int r = 0; r < COP_RB; ++r)
-      cr[r] = reinterpret_cast<const V2*>(C + (long)min(x0 + r, nrep - 1) * M);
-    const V2* vg[3];
-#pragma unroll
-    for (int q = 0; q < 3; ++q) vg[q] = reinterpret_cast<const V2*>(V + (long)min(g0 + q, ng - 1) * M);
-#pragma unroll 2
+  for (int q = 0; q < COP_GMAX; ++q) acc[0][q] = acc[1][q] = T(0);
+  if (r0 < nrep) {
+    const V2* c0p = reinterpret_cast<const V2*>(C + (long)r0 * M);
+    const V2* c1p = reinterpret_cast<const V2*>(C + (long)min(r0 + 1, nrep - 1) * M);
+#pragma unroll 1
     for (int h = h0 + lane; h < h1; h += 32) {
-      V2 c[COP_RB], v[3];
+      const V2 c0 = c0p[h], c1 = c1p[h];
+      const V2* vh = sv + (h - h0);
 #pragma unroll
-      for (int r = 0; r < COP_RB; ++r) c[r] = cr[r][h];
-#pragma unroll
-      for (int q = 0; q < 3; ++q) v[q] = vg[q][h];
-#pragma unroll
-      for (int r = 0; r < COP_RB; ++r)
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-          acc[r][q] = fma(c[r].x, v[q].x, acc[r][q]);
-          acc[r][q] = fma(c[r].y, v[q].y, acc[r][q]);
+      for (int q = 0; q < COP_GMAX; ++q) {
+        if (q < ng) {
+          const V2 v = vh[q * nh];
+          acc[0][q] = fma(c0.x, v.x, acc[0][q]);
+          acc[0][q] = fma(c0.y, v.y, acc[0][q]);
+          acc[1][q] = fma(c1.x, v.x, acc[1][q]);
+          acc[1][q] = fma(c1.y, v.y, acc[1][q]);
         }
+      }
     }
   }
 #pragma unroll
-  for (int r = 0; r < COP_RB; ++r)
+  for (int r = 0; r < 2; ++r)
 #pragma unroll
-    for (int q = 0; q < 3; ++q) {
+    for (int q = 0; q < COP_GMAX; ++q) {
       T y = acc[r][q];
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
       acc[r][q] = y;
     }
-  if (lane == 0 && g0 < ng) {
+  // lane q writes symmetry q of both representatives
+  T y0 = T(0), y1 = T(0);
 #pragma unroll
-    for (int r = 0; r < COP_RB; ++r)
-#pragma unroll
-      for (int q = 0; q < 3; ++q)
-        if (x0 + r < nrep && g0 + q < ng)
-          Y[((long)s * nrep + x0 + r) * COP_GMAX + g0 + q] = acc[r][q];
+  for (int q = 0; q < COP_GMAX; ++q)
+    if (lane == q) {
+      y0 = acc[0][q];
+      y1 = acc[1][q];
+    }
+  if (lane < ng) {
+    if (r0 < nrep) Y[((long)s * nrep + r0) * COP_GMAX + lane] = y0;
+    if (r0 + 1 < nrep) Y[((long)s * nrep + r0 + 1) * COP_GMAX + lane] = y1;
   }
+}
+
+// shared memory of k_cop_gemm: the slice of every permuted copy
+template <class T>
+static size_t cop_gemm_smem(int M, int ng) {
+  const int per = (((M + COP_KS - 1) / COP_KS) + 1) & ~1;
+  return (size_t)ng * (per / 2) * 2 * sizeof(T);
 }
 
 // x_B[o] = the slices of Y[x][g] added in ascending order, (x, g) the pair
@@ -1578,7 +1594,9 @@ static int apply_coarse_op(const Lvl<T>& L, const T* op, T* part, cudaStream_t s
   const int* prod = reinterpret_cast<const int*>(op + (long)P.nrep * P.M) + P.nrep;
   WF_CK(launch_k(k_cop_vg<T>, (P.M + 31) / 32, 256, 0, s, L, V, P.G));
   WF_CKL("k_cop_vg");
-  WF_CK(launch_k(k_cop_gemm<T>, dim3((P.nrep + COP_RB - 1) / COP_RB, COP_KS), 256, 0, s, op,
+  const size_t sm = cop_gemm_smem<T>(P.M, P.G.ng);
+  WF_CK(cudaFuncSetAttribute(k_cop_gemm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  WF_CK(launch_k(k_cop_gemm<T>, dim3((P.nrep + COP_RB - 1) / COP_RB, COP_KS), 256, sm, s, op,
                  (const T*)V, Y, P.nrep, P.M, P.G.ng));
   WF_CKL("k_cop_gemm");
   WF_CK(launch_k(k_cop_out<T>, (P.M + 255) / 256, 256, 0, s, (const T*)Y, prod, P.nrep, L));
@@ -1812,8 +1830,8 @@ static int split_sweeps(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
   const int m = L.n + 2;
   T* sp = L.tmp;
   const T* sr = L.tmp + (long)m * m * m;
-  int cpt, rows;
-  launch_shape(SHAPE_SPLIT, L.n, &cpt, &rows);   // cpt in {1, 2, 4}, rows <= SPLIT_ROWS
+  int cpt, rows, one;
+  launch_shape(SHAPE_SPLIT, L.n, &cpt, &rows, &one);   // cpt in {1, 2, 4}, rows <= SPLIT_ROWS
   const dim3 grid((L.n / 2 + 32 * cpt - 1) / (32 * cpt), (L.n + rows - 1) / rows, L.n);
   const ApRecip<T> rt = ap_recip(L);
   auto kern = cpt == 4 ? k_rbgs_split<T, 4> : cpt == 2 ? k_rbgs_split<T, 2> : k_rbgs_split<T, 1>;

@@ -442,7 +442,8 @@ __device__ __forceinline__ void diff_cell(const wf_case& c, const Geo& g, double
 // the same star.
 template <int COMP, bool DIFF>
 __global__ void __launch_bounds__(TPB) k_conv(const wf_case c, Geo g, double alpha,
-                                             const double* dtp, const Divs dv, const Batch bt) {
+                                             const double* dtp, const Divs dv, int planes,
+                                             const Batch bt) {
   pdl_entry();
   const double* u = bt_fld(c, bt, WF_U);
   const double* v = bt_fld(c, bt, WF_V);
@@ -456,14 +457,19 @@ __global__ void __launch_bounds__(TPB) k_conv(const wf_case c, Geo g, double alp
   int ni, nj, nk;
   op_dims(COMP, g.n, ni, nj, nk);
   const long tot = (long)ni * nj * nk;
-  {  // one thread per cell: x = k, y = j (the CTA's shape is chosen per
-     // size, 32 x 8 by default), z = i
-    const int kx_ = blockIdx.x * blockDim.x + threadIdx.x;
-    const int jy_ = blockIdx.y * blockDim.y + threadIdx.y;
-    if (kx_ >= nk || jy_ >= nj) return;
-    const int k = NPL + kx_;
-    const int j = NPL + jy_;
-    const int i = NPL + bt_z(bt);
+  // one thread per (j, k) column and `planes` consecutive planes i: x = k,
+  // y = j (the CTA's shape and the planes are chosen per size, 32 x 8 x 1 by
+  // default), z = group of planes.  A CTA that walks through several planes
+  // finds a cell's neighbours across i in L1, loaded for the planes before.
+  const int kx_ = blockIdx.x * blockDim.x + threadIdx.x;
+  const int jy_ = blockIdx.y * blockDim.y + threadIdx.y;
+  if (kx_ >= nk || jy_ >= nj) return;
+  const int k = NPL + kx_;
+  const int j = NPL + jy_;
+  const int i_end = min(ni, (bt_z(bt) + 1) * planes);
+#pragma unroll 1
+  for (int ii = bt_z(bt) * planes; ii < i_end; ++ii) {
+    const int i = NPL + ii;
     const long id = g.at(i, j, k);
     double tot3;
     if (COMP == 0) {
@@ -543,10 +549,11 @@ __global__ void __launch_bounds__(TPB) k_diff(const wf_case c, Geo g, double alp
 
 
 // ---- launch shapes per size ------------------------------------------------
-// 0 = the default: k_conv 32 x 8 (a warp along k, 8 rows j); k_rbgs_split
-// 2 cells per thread (WF_SPLIT_CPT overrides), 8 rows per CTA
+// 0 = the default: k_conv 32 x 8 threads (a warp along k, 8 rows j), one
+// plane i per thread; k_rbgs_split 2 cells per thread (WF_SPLIT_CPT
+// overrides), 8 rows per CTA
 static constexpr int SHAPE_MAX_N = 1024;
-static int g_shape[2][SHAPE_MAX_N + 1][2];
+static int g_shape[2][SHAPE_MAX_N + 1][3];
 
 static int split_cpt_default() {
   static int v = -1;
@@ -558,38 +565,39 @@ static int split_cpt_default() {
   return v;
 }
 
-void launch_shape(int kind, int n, int* a, int* b) {
+void launch_shape(int kind, int n, int* a, int* b, int* c) {
   const bool set = kind >= 0 && kind <= 1 && n >= 0 && n <= SHAPE_MAX_N && g_shape[kind][n][0];
   if (kind == SHAPE_CONV) {
     *a = set ? g_shape[kind][n][0] : 32;
     *b = set ? g_shape[kind][n][1] : 8;
+    *c = set ? g_shape[kind][n][2] : 1;
   } else {
     *a = set ? g_shape[kind][n][0] : split_cpt_default();
     *b = set ? g_shape[kind][n][1] : 8;
+    *c = 1;
   }
 }
 
-int set_launch_shape(int kind, int n, int a, int b) {
+int set_launch_shape(int kind, int n, int a, int b, int c) {
   if (n < 4 || n > SHAPE_MAX_N) return fail(WF_EINVAL, "wf_set_launch_shape: n in 4..1024");
-  if (a == 0 && b == 0) {
-    if (kind != SHAPE_CONV && kind != SHAPE_SPLIT)
-      return fail(WF_EINVAL, "wf_set_launch_shape: kind 0 (k_conv) or 1 (k_rbgs_split)");
-    g_shape[kind][n][0] = g_shape[kind][n][1] = 0;
+  if (kind != SHAPE_CONV && kind != SHAPE_SPLIT)
+    return fail(WF_EINVAL, "wf_set_launch_shape: kind 0 (k_conv) or 1 (k_rbgs_split)");
+  if (a == 0 && b == 0 && c == 0) {
+    g_shape[kind][n][0] = g_shape[kind][n][1] = g_shape[kind][n][2] = 0;
     return WF_OK;
   }
   if (kind == SHAPE_CONV) {
     // whole warps, at most TPB threads (the kernel's launch bound)
-    if (a < 1 || b < 1 || a > 256 || (a & (a - 1)) || a * b > TPB || (a * b) % 32)
+    if (a < 1 || b < 1 || a > 256 || (a & (a - 1)) || a * b > TPB || (a * b) % 32 || c < 1 ||
+        c > 16)
       return fail(WF_EINVAL, "wf_set_launch_shape(k_conv): a a power of two, a*b a multiple "
-                             "of 32 and at most 256");
-  } else if (kind == SHAPE_SPLIT) {
-    if ((a != 1 && a != 2 && a != 4) || (b != 1 && b != 2 && b != 4 && b != 8))
-      return fail(WF_EINVAL, "wf_set_launch_shape(k_rbgs_split): a in {1,2,4}, b in {1,2,4,8}");
-  } else {
-    return fail(WF_EINVAL, "wf_set_launch_shape: kind 0 (k_conv) or 1 (k_rbgs_split)");
+                             "of 32 and at most 256, c in 1..16");
+  } else if ((a != 1 && a != 2 && a != 4) || (b != 1 && b != 2 && b != 4 && b != 8) || c != 1) {
+    return fail(WF_EINVAL, "wf_set_launch_shape(k_rbgs_split): a in {1,2,4}, b in {1,2,4,8}, c = 1");
   }
   g_shape[kind][n][0] = a;
   g_shape[kind][n][1] = b;
+  g_shape[kind][n][2] = c;
   return WF_OK;
 }
 
@@ -598,15 +606,16 @@ int launch_conv(const wf_case& c, int comp, double alpha, const double* dt,
   Geo g = geo_of(c.n);
   int ni, nj, nk;
   op_dims(comp, c.n, ni, nj, nk);
-  int bx, by;
-  launch_shape(SHAPE_CONV, c.n, &bx, &by);
-  const dim3 gr((nk + bx - 1) / bx, (nj + by - 1) / by, ni), bl(bx, by);
+  int bx, by, planes;
+  launch_shape(SHAPE_CONV, c.n, &bx, &by, &planes);
+  const dim3 gr((nk + bx - 1) / bx, (nj + by - 1) / by, (ni + planes - 1) / planes), bl(bx, by);
   if (comp < 0 || comp > 2) return fail(WF_EINVAL, "conv: comp must be 0, 1 or 2");
-  void (*const kern[2][3])(const wf_case, Geo, double, const double*, const Divs,
+  void (*const kern[2][3])(const wf_case, Geo, double, const double*, const Divs, int,
                            const Batch) = {
       {k_conv<0, false>, k_conv<1, false>, k_conv<2, false>},
       {k_conv<0, true>, k_conv<1, true>, k_conv<2, true>}};
-  WF_CK(launch_k(kern[with_diff ? 1 : 0][comp], gr, bl, 0, s, c, g, alpha, dt, divs_of(c)));
+  WF_CK(launch_k(kern[with_diff ? 1 : 0][comp], gr, bl, 0, s, c, g, alpha, dt, divs_of(c),
+                 planes));
   WF_CKL("k_conv");
   return WF_OK;
 }

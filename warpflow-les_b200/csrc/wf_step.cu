@@ -307,21 +307,18 @@ static bool same_bucket(const wf_case& a, const wf_case& b) {
 // 0 in the table means the built-in rule: a bucket's grids stack its cases
 // along z (< 65536), and its cases' finest multigrid level (phi and rhs)
 // should fit in about half the L2 (64 MB), so the half-sweeps, which
-// dominate a step, keep the bucket's level resident across launches.  From
-// n = 64 on, separate branches are the default.  Measured on B200 (16
-// mixed-precision cases per size, ms per ensemble step, bucketed vs one
-// branch per case): 32^3 1.25 vs 1.74, 48^3 2.87 vs 3.13, 64^3 4.67 vs
-// 4.33, 80^3 10.3 vs 8.5, 96^3 14.8 vs 12.1.  The branches of large cases
-// overlap one another's dependent chains of kernels; a bucket waits for its
-// slowest case at every launch.  wf_set_bucket_cap overrides the rule per
-// size (the autotuner's measurement).
+// dominate a step, keep the bucket's level resident across launches.
+// Measured on B200 with 13 equal mixed-precision cases per size, one bucket
+// against a branch per case (ms per ensemble step): 32^3 1.07 vs 1.84,
+// 48^3 2.45 vs 3.29, 64^3 3.88 vs 4.44, 80^3 8.49 vs 8.94, 96^3 12.49 vs
+// 12.61.  wf_set_bucket_cap overrides the rule per size (the autotuner's
+// measurement).
 static constexpr int BUCKET_MAX_N = 1024;
 static int g_bucket_cap[2][BUCKET_MAX_N + 1];
 
 static int bucket_cap(const wf_case& c) {
   const int set = (c.n >= 0 && c.n <= BUCKET_MAX_N) ? g_bucket_cap[c.mg_fp32 ? 1 : 0][c.n] : 0;
   if (set > 0) return std::min(set, std::max(1, 60000 / (c.n + 2 * NPL)));
-  if (c.n >= 64) return 1;
   const long m = c.n + 2;
   const long lvl_bytes = 2 * m * m * m * (c.mg_fp32 ? 4 : 8);
   return (int)std::max(1L, std::min(60000L / (c.n + 2 * NPL), (64L << 20) / lvl_bytes));
@@ -356,17 +353,18 @@ int wf_set_coarse_strategy(int32_t n, int32_t fp32, int32_t strategy) {
   return set_coarse_strategy(n, fp32, strategy);
 }
 
-int wf_set_launch_shape(int32_t kind, int32_t n, int32_t a, int32_t b) {
-  return set_launch_shape(kind, n, a, b);
+int wf_set_launch_shape(int32_t kind, int32_t n, int32_t a, int32_t b, int32_t c) {
+  return set_launch_shape(kind, n, a, b, c);
 }
 
-int wf_launch_shape(int32_t kind, int32_t n, int32_t* a, int32_t* b) {
-  if (!a || !b || (kind != SHAPE_CONV && kind != SHAPE_SPLIT))
+int wf_launch_shape(int32_t kind, int32_t n, int32_t* a, int32_t* b, int32_t* c) {
+  if (!a || !b || !c || (kind != SHAPE_CONV && kind != SHAPE_SPLIT))
     return fail(WF_EINVAL, "wf_launch_shape: kind 0 or 1, non-null outputs");
-  int x, y;
-  launch_shape(kind, n, &x, &y);
+  int x, y, z;
+  launch_shape(kind, n, &x, &y, &z);
   *a = x;
   *b = y;
+  *c = z;
   return WF_OK;
 }
 

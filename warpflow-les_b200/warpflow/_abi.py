@@ -89,8 +89,9 @@ SIGNATURES = {
     "wf_struct_sizes": (_I32, [ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
     "wf_scalars_init": (_I32, [_VP, _D, _D, _D, _VP]),
     "wf_set_coarse_strategy": (_I32, [_I32, _I32, _I32]),
-    "wf_set_launch_shape": (_I32, [_I32, _I32, _I32, _I32]),
-    "wf_launch_shape": (_I32, [_I32, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_I32)]),
+    "wf_set_launch_shape": (_I32, [_I32, _I32, _I32, _I32, _I32]),
+    "wf_launch_shape": (_I32, [_I32, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_I32),
+                               ctypes.POINTER(_I32)]),
     "wf_set_bucket_cap": (_I32, [_I32, _I32, _I32]),
     "wf_bucket_cap": (_I32, [_I32, _I32, ctypes.POINTER(_I32)]),
     "wf_mg_level_elems": (_I32, [_I32, _I32, _I32, ctypes.POINTER(ctypes.c_int64)]),

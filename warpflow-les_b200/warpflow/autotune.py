@@ -144,22 +144,26 @@ def tune_buckets(sizes=(32, 48, 64, 80, 96), ncases=8, precision="mixed", reps=5
 
 
 SHAPE_CONV, SHAPE_SPLIT = 0, 1
-CONV_SHAPES = ((32, 8), (16, 16), (64, 4), (32, 4), (16, 8), (128, 2), (64, 2), (32, 2),
-               (16, 4), (8, 16), (8, 32))
-SPLIT_SHAPES = tuple((c, r) for c in (1, 2, 4) for r in (2, 4, 8))
+# k_conv: threads along k, along j, planes i per thread
+CONV_SHAPES = tuple((a, b, c) for a, b in ((32, 8), (16, 16), (64, 4), (32, 4), (16, 8),
+                                           (128, 2), (32, 2), (8, 32))
+                    for c in (1, 2, 4, 8))
+# k_rbgs_split: cells per thread, rows per CTA
+SPLIT_SHAPES = tuple((c, r, 1) for c in (1, 2, 4) for r in (2, 4, 8))
 _KIND = {"conv": SHAPE_CONV, "split": SHAPE_SPLIT}
 
 
-def set_shape(kind, n, a, b):
-    """Launch shape of `kind` ("conv" or "split") for size n; (0, 0) restores
-    the default."""
-    _abi.call("wf_set_launch_shape", _KIND[kind], int(n), int(a), int(b))
+def set_shape(kind, n, a, b, c=1):
+    """Launch shape of `kind` ("conv" or "split") for size n; (0, 0, 0)
+    restores the default."""
+    _abi.call("wf_set_launch_shape", _KIND[kind], int(n), int(a), int(b), int(c))
 
 
 def shape(kind, n):
-    a, b = ctypes.c_int32(), ctypes.c_int32()
-    _abi.call("wf_launch_shape", _KIND[kind], int(n), ctypes.byref(a), ctypes.byref(b))
-    return a.value, b.value
+    a, b, c = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+    _abi.call("wf_launch_shape", _KIND[kind], int(n), ctypes.byref(a), ctypes.byref(b),
+              ctypes.byref(c))
+    return a.value, b.value, c.value
 
 
 def _time_fn(fn, reps):
@@ -181,8 +185,8 @@ def tune_shapes(sizes=(80,), conv=CONV_SHAPES, split=SPLIT_SHAPES, reps=10, devi
     on the split copy (FP64, n >= 80, even), of the split half-sweep (12
     half-sweeps: a 12-sweep relax less a 6-sweep one).  Install the fastest
     per size and return {"conv": {n: rec}, "split": {n: rec}}, rec =
-    {"best": [a, b], "us": {"axb": time}}.  Raises if a shape changes a
-    result."""
+    {"best": [a, b, c], "us": {"axbxc": time}}.  Raises if a shape changes
+    a result."""
     from .ensemble import cavity_case
     from .solver import FlowSolver
     out = {"conv": {}, "split": {}}
@@ -192,25 +196,26 @@ def tune_shapes(sizes=(80,), conv=CONV_SHAPES, split=SPLIT_SHAPES, reps=10, devi
         stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
         dtp = ctypes.c_void_p(sol._sc.data_ptr())   # wf_scalars.dt is the first member
 
-        def conv():
+        def conv_pass():
             for comp in range(3):
                 _abi.call("wf_conv", ctypes.byref(sol.case), comp, 0.5, dtp, stream)
 
         times, ref = {}, None
-        for a, b in conv:
-            set_shape("conv", n, a, b)
-            t = _time_fn(conv, reps)
+        for a, b, c in conv:
+            set_shape("conv", n, a, b, c)
+            t = _time_fn(conv_pass, reps)
             got = [sol.f[k].numpy() for k in ("ustar", "vstar", "wstar")]
             if ref is None:
                 ref = got
             elif any(not np.array_equal(x, y) for x, y in zip(got, ref)):
-                set_shape("conv", n, 0, 0)
-                raise RuntimeError("k_conv shape %dx%d changed the result at n=%d" % (a, b, n))
-            times["%dx%d" % (a, b)] = t
+                set_shape("conv", n, 0, 0, 0)
+                raise RuntimeError("k_conv shape %dx%dx%d changed the result at n=%d"
+                                   % (a, b, c, n))
+            times["%dx%dx%d" % (a, b, c)] = t
         best = min(times, key=times.get)
-        a, b = (int(x) for x in best.split("x"))
-        set_shape("conv", n, a, b)
-        out["conv"][n] = {"best": [a, b], "us": {k: round(v, 2) for k, v in times.items()}}
+        a, b, c = (int(x) for x in best.split("x"))
+        set_shape("conv", n, a, b, c)
+        out["conv"][n] = {"best": [a, b, c], "us": {k: round(v, 2) for k, v in times.items()}}
 
         mg = sol.mg
         lev = mg.levels[0]
@@ -218,7 +223,7 @@ def tune_shapes(sizes=(80,), conv=CONV_SHAPES, split=SPLIT_SHAPES, reps=10, devi
             rhs = np.random.default_rng(n).standard_normal(lev.shape)
             lev.rhs.assign(rhs)
             times, ref = {}, None
-            for c, r in split:
+            for c, r, _ in split:
                 set_shape("split", n, c, r)
                 lev.phi.zero_()
                 mg._relax(0, 6)
@@ -226,16 +231,17 @@ def tune_shapes(sizes=(80,), conv=CONV_SHAPES, split=SPLIT_SHAPES, reps=10, devi
                 if ref is None:
                     ref = got
                 elif not np.array_equal(got, ref):
-                    set_shape("split", n, 0, 0)
+                    set_shape("split", n, 0, 0, 0)
                     raise RuntimeError("k_rbgs_split shape %dx%d changed the result at n=%d"
                                        % (c, r, n))
                 t12 = _time_fn(lambda: mg._relax(0, 12), reps)
                 t6 = _time_fn(lambda: mg._relax(0, 6), reps)
-                times["%dx%d" % (c, r)] = (t12 - t6) / 12
+                times["%dx%dx1" % (c, r)] = (t12 - t6) / 12
             best = min(times, key=times.get)
-            c, r = (int(x) for x in best.split("x"))
+            c, r, _ = (int(x) for x in best.split("x"))
             set_shape("split", n, c, r)
-            out["split"][n] = {"best": [c, r], "us": {k: round(v, 3) for k, v in times.items()}}
+            out["split"][n] = {"best": [c, r, 1],
+                               "us": {k: round(v, 3) for k, v in times.items()}}
         sol.close()
     return out
 
