@@ -1,11 +1,11 @@
 """The alternative relax paths of the fine and mid-size levels, each forced on
 or off in child processes -- sweeps on row-parity-split copies (default for
-levels >= 128), cluster-resident relaxes of 28..48^3 levels (default), and
-one-launch red-black sweeps (off by default): multigrid solves must match
-the FP64 oracle and the mixed form must stay within its tolerance.  The
-split and one-launch paths divide exactly like the in-place one-colour path
-and must equal it bit for bit; the cluster kernels multiply by the
-reciprocal of the diagonal (one rounding away) and must agree to 1e-12."""
+levels >= 80 in FP64), cluster-resident relaxes of 28..48^3 levels, and
+one-launch red-black sweeps: multigrid solves must match the FP64 oracle
+and the mixed form must stay within its tolerance.  The split and
+one-launch paths divide exactly like the in-place one-colour path and must
+equal it bit for bit; the cluster kernels multiply by the reciprocal of the
+diagonal (one rounding away) and must agree to 1e-12."""
 import hashlib
 import json
 import os
@@ -19,8 +19,9 @@ from conftest import PKG, ROOT
 pytestmark = pytest.mark.gpu
 
 SCRIPT = r"""
-import hashlib, json, sys
+import hashlib, json, os, sys
 sys.path[:0] = [%r, %r]
+check = os.environ.get("WF_TEST_ORACLE") == "1"   # else only the hashes
 import numpy as np
 from oracle import wf_oracle as O
 from warpflow import Multigrid, build_topology
@@ -28,7 +29,8 @@ from warpflow.config import case_from_dict
 from warpflow.fields import DeviceField
 out = {}
 for n, L, prec in ((20, 2, "fp64"), (24, 3, "fp64"), (40, 3, "fp64"), (40, 3, "mixed"),
-                   (70, 2, "fp64"), (64, 3, "fp64"), (96, 3, "fp64"), (96, 3, "mixed")):
+                   (70, 2, "fp64"), (64, 3, "fp64"), (80, 3, "fp64"), (80, 3, "mixed"),
+                   (96, 3, "fp64"), (96, 3, "mixed")):
     cfg = case_from_dict({"grid": {"nx": n, "ny": n, "nz": n},
                           "numerics": {"mg_levels": L, "mg_precision": prec}})
     h = 1.0 / n
@@ -38,9 +40,10 @@ for n, L, prec in ((20, 2, "fp64"), (24, 3, "fp64"), (40, 3, "fp64"), (40, 3, "m
     su = DeviceField.zeros(shape, "cuda:0"); pp = DeviceField.zeros(shape, "cuda:0")
     su.assign(rhs)
     mg.solve(su, pp, 3)
-    ref = np.zeros(shape)
-    O.Multigrid(n, L, h, h, h).solve(rhs, ref, n)
-    out["%%d_%%d_%%s" %% (n, L, prec)] = float(np.abs(pp.numpy() - ref).max() / np.abs(ref).max())
+    if check:
+        ref = np.zeros(shape)
+        O.Multigrid(n, L, h, h, h).solve(rhs, ref, n)
+        out["%%d_%%d_%%s" %% (n, L, prec)] = float(np.abs(pp.numpy() - ref).max() / np.abs(ref).max())
     out["hash_%%d_%%d_%%s" %% (n, L, prec)] = hashlib.sha1(pp.numpy().tobytes()).hexdigest()
     # harness relax with an odd sweep count on level 0 (fp64 only)
     if prec == "fp64":
@@ -48,11 +51,12 @@ for n, L, prec in ((20, 2, "fp64"), (24, 3, "fp64"), (40, 3, "fp64"), (40, 3, "m
         lev.rhs.assign(np.random.default_rng(1).standard_normal(lev.shape))
         lev.phi.zero_()
         mg._relax(0, 5)
-        ol = O.Level(n, h, h, h)
-        ol.rhs[...] = lev.rhs.numpy()
-        for _ in range(5):
-            O.rbgs(ol, 0); O.rbgs(ol, 1); O.mg_refill(ol.phi, n)
-        out["relax_%%d" %% n] = float(np.abs(lev.phi.numpy() - ol.phi).max() / np.abs(ol.phi).max())
+        if check:
+            ol = O.Level(n, h, h, h)
+            ol.rhs[...] = lev.rhs.numpy()
+            for _ in range(5):
+                O.rbgs(ol, 0); O.rbgs(ol, 1); O.mg_refill(ol.phi, n)
+            out["relax_%%d" %% n] = float(np.abs(lev.phi.numpy() - ol.phi).max() / np.abs(ol.phi).max())
         out["hash_relax_%%d" %% n] = hashlib.sha1(lev.phi.numpy().tobytes()).hexdigest()
 print(json.dumps(out))
 """ % (ROOT, PKG)
@@ -61,8 +65,9 @@ print(json.dumps(out))
 OFF = str(1 << 30)
 
 
-def _run(env_extra):
+def _run(env_extra, oracle):
     env = dict(os.environ, **env_extra)
+    env["WF_TEST_ORACLE"] = "1" if oracle else "0"
     r = subprocess.run([sys.executable, "-c", SCRIPT], capture_output=True, text=True,
                        env=env, timeout=600)
     assert r.returncode == 0, r.stderr[-3000:]
@@ -71,7 +76,7 @@ def _run(env_extra):
 
 @pytest.fixture(scope="module")
 def in_place():
-    return _run({"WF_SPLIT_MIN": OFF, "WF_SWEEP2_MIN": OFF, "WF_MID": "0"})
+    return _run({"WF_SPLIT_MIN": OFF, "WF_SWEEP2_MIN": OFF, "WF_MID": "0"}, True)
 
 
 @pytest.mark.parametrize("env,exact", [
@@ -80,7 +85,14 @@ def in_place():
     ({"WF_SPLIT_MIN": OFF, "WF_SWEEP2_MIN": OFF, "WF_MID": "1"}, False)],
     ids=["split", "one_launch", "mid_cluster"])
 def test_relax_paths_match_oracle_and_in_place(env, exact, in_place):
-    res = _run(env)
+    """Bit-exact paths must reproduce the in-place path's hashes (which is
+    itself checked against the oracle); the cluster path is checked against
+    the oracle directly."""
+    res = _run(env, not exact)
+    for key, val in in_place.items():
+        if not key.startswith("hash_"):
+            tol = 1e-5 if key.endswith("mixed") else 1e-11
+            assert val <= tol, (key, val)
     for key, val in res.items():
         if key.startswith("hash_"):
             if exact:
