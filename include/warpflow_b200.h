@@ -258,6 +258,40 @@ WF_API int wf_mg_residual_max(const wf_case* c, const double* phi0, const double
 /* bcs.py:326-360 _mk_neumann on all six faces of a level-0 pair. */
 WF_API int wf_mg_refill(const wf_case* c, double* phi0, void* stream);
 
+/* ---- sub-domains (more than one rank per case) --------------------------
+ * The reference decomposes a case over MPI ranks (topology.py:30-53): each
+ * rank steps its own cube of cells, and halo.py:59-130 HaloExchanger.exchange
+ * copies ghost slabs between neighbours along x, then y, then z, each slab
+ * the full extent of the other two axes (so edge and corner ghosts follow
+ * without diagonal messages).  These entries are the device side of that:
+ * the host moves the buffers between ranks (NCCL or gloo). */
+/* halo.py:16-55 _gather_{x,y,z} (unpack = 0) and _scatter_{x,y,z}
+ * (unpack = 1): the box [i0,i0+ni) x [j0,j0+nj) x [k0,k0+nk) of a 3-D
+ * array with strides (sI, sJ, 1) to / from a dense buffer ordered
+ * [i][j][k]. */
+WF_API int wf_box_copy(double* arr, int64_t sI, int64_t sJ, int32_t i0, int32_t j0, int32_t k0,
+                       int32_t ni, int32_t nj, int32_t nk, double* buf, int32_t unpack,
+                       void* stream);
+/* solver.py:222-225: uoo/voo/woo = u/v/w over the whole padded arrays. */
+WF_API int wf_copy_oo(const wf_case* c, void* stream);
+/* One pass of the reference multigrid at a sub-domain, on level `level` of
+ * the case (level 0 = the one-ring core of pp and su, as wf_mg_solve):
+ * op 0 one colour half-sweep (multigrid.py:70-90) with the face
+ * coefficients of multigrid.py:23-67, zero only across a physical face;
+ * op 1 the Neumann mirror of the physical faces (bcs.py:326-360, the
+ * mgbound half of multigrid.py:264-287; the seams are the host's exchange);
+ * op 2 restriction from level-1 (multigrid.py:93-119) and the coarse phi
+ * zeroed (multigrid.py:310-312); op 3 prolongation from level+1 onto the
+ * real cells (multigrid.py:122-146); op 4 pp zeroed (multigrid.py:332-333).
+ * `phys`: bit f set when face f is physical (0 west, 1 east, 2 south,
+ * 3 north, 4 bottom, 5 top). */
+WF_API int wf_rk_mg_op(const wf_case* c, int32_t op, int32_t level, int32_t phys,
+                       int32_t color, void* stream);
+/* Where level `level` of the case lives: the ring cell (0,0,0) of its phi,
+ * its strides (k stride 1) and its edge m = n_l + 2. */
+WF_API int wf_rk_level_view(const wf_case* c, int32_t level, double** phi, int64_t* sI,
+                            int64_t* sJ, int32_t* m);
+
 /* No counterpart in the reference: a check of the library's bounded
  * device-side waits.  One CTA runs one wait that can never complete and
  * must give up after `tries` tries (1 .. 2^22): kind 0 the grid barrier of

@@ -129,16 +129,26 @@ def apply_initial(f, n, ulid):
     apply_p_mirror(f["p"], n)
 
 
-def mg_refill(phi, n):
-    """bcs.py:326-360 ``_mk_neumann`` with npl=1 on all six faces
-    (face interiors only; edges and corners untouched)."""
+ALL_PHYS = (True,) * 6
+
+
+def mg_refill(phi, n, phys=ALL_PHYS):
+    """bcs.py:326-360 ``_mk_neumann`` with npl=1 on the physical faces
+    (multigrid.py:264-287; face interiors only, edges and corners
+    untouched).  ``phys``: west, east, south, north, bottom, top."""
     s = slice(1, n + 1)
-    phi[0, s, s] = phi[1, s, s]
-    phi[n + 1, s, s] = phi[n, s, s]
-    phi[s, 0, s] = phi[s, 1, s]
-    phi[s, n + 1, s] = phi[s, n, s]
-    phi[s, s, 0] = phi[s, s, 1]
-    phi[s, s, n + 1] = phi[s, s, n]
+    if phys[0]:
+        phi[0, s, s] = phi[1, s, s]
+    if phys[1]:
+        phi[n + 1, s, s] = phi[n, s, s]
+    if phys[2]:
+        phi[s, 0, s] = phi[s, 1, s]
+    if phys[3]:
+        phi[s, n + 1, s] = phi[s, n, s]
+    if phys[4]:
+        phi[s, s, 0] = phi[s, s, 1]
+    if phys[5]:
+        phi[s, s, n + 1] = phi[s, s, n]
 
 
 # --------------------------------------------------------------------------
@@ -390,8 +400,9 @@ class Level:
     """multigrid.py:207-220 plus the coefficient arrays of ``_mgcoeff``
     (multigrid.py:23-67): 1/d^2 faces, zeroed across physical boundaries."""
 
-    def __init__(self, n, dxl, dyl, dzl, dtype=np.float64):
+    def __init__(self, n, dxl, dyl, dzl, dtype=np.float64, phys=ALL_PHYS):
         self.n = n
+        self.phys = tuple(phys)
         shp = (n + 2,) * 3
         self.phi = np.zeros(shp, dtype=dtype)
         self.rhs = np.zeros(shp, dtype=dtype)
@@ -403,12 +414,20 @@ class Level:
         cn = cs.copy()
         cb = np.full((n,) * 3, 1.0 / (dzl * dzl))
         ct = cb.copy()
-        cw[0, :, :] = 0.0
-        ce[n - 1, :, :] = 0.0
-        cs[:, 0, :] = 0.0
-        cn[:, n - 1, :] = 0.0
-        cb[:, :, 0] = 0.0
-        ct[:, :, n - 1] = 0.0
+        # multigrid.py:38-55: zeroed only across a physical face (a seam
+        # between ranks keeps its coefficient)
+        if phys[0]:
+            cw[0, :, :] = 0.0
+        if phys[1]:
+            ce[n - 1, :, :] = 0.0
+        if phys[2]:
+            cs[:, 0, :] = 0.0
+        if phys[3]:
+            cn[:, n - 1, :] = 0.0
+        if phys[4]:
+            cb[:, :, 0] = 0.0
+        if phys[5]:
+            ct[:, :, n - 1] = 0.0
         self.aw, self.ae, self.as_, self.an, self.ab, self.at = (
             cw, ce, cs, cn, cb, ct)
         self.ap = -(cw + ce + cs + cn + cb + ct)
@@ -478,13 +497,25 @@ def prolong(c, f):
 
 
 class Multigrid:
-    """multigrid.py:223-337 (single rank, all six faces physical)."""
+    """multigrid.py:223-337.  One rank by default (all six faces physical);
+    at a sub-domain, ``phys`` marks the physical faces and ``comm`` (see
+    RankComm) exchanges the one-cell rings at the seams."""
 
-    def __init__(self, n, nlev, dx, dy, dz):
-        self.levels = [Level(n >> l, dx * 2.0 ** l, dy * 2.0 ** l, dz * 2.0 ** l)
+    def __init__(self, n, nlev, dx, dy, dz, phys=ALL_PHYS, comm=None):
+        self.phys = tuple(phys)
+        self.comm = comm
+        self.levels = [Level(n >> l, dx * 2.0 ** l, dy * 2.0 ** l, dz * 2.0 ** l,
+                             phys=self.phys)
                        for l in range(nlev)]
         self.n_pre, self.n_post = N_PRE, N_POST
         self.n_coarse, self.n_vcycles = N_COARSE, N_VCYCLES
+
+    def refill(self, lev):
+        """multigrid.py:264-287: mirror at the physical faces, then the halo
+        exchange of the ring (NPL_MG = 1)."""
+        mg_refill(lev.phi, lev.n, self.phys)
+        if self.comm is not None:
+            self.comm.exchange(lev.phi, 1)
 
     def relax(self, l, nsweeps):
         """multigrid.py:289-299: red, black, then ONE ring refill per sweep."""
@@ -492,7 +523,7 @@ class Multigrid:
         for _ in range(nsweeps):
             rbgs(lev, 0)
             rbgs(lev, 1)
-            mg_refill(lev.phi, lev.n)
+            self.refill(lev)
 
     def vcycle(self):
         """multigrid.py:301-322."""
@@ -503,7 +534,7 @@ class Multigrid:
             self.relax(l, self.n_pre if l < L - 1 else self.n_coarse)
         for l in range(L - 2, -1, -1):
             prolong(self.levels[l + 1], self.levels[l])
-            mg_refill(self.levels[l].phi, self.levels[l].n)
+            self.refill(self.levels[l])
             self.relax(l, self.n_post)
 
     def solve(self, su, pp, n):
@@ -520,6 +551,89 @@ class Multigrid:
 
 
 # --------------------------------------------------------------------------
+# sub-domains (topology.py, halo.py)
+# --------------------------------------------------------------------------
+def cart_neighbors(rank, sd):
+    """topology.py:40-45: ``Create_cart(sd, periods=False, reorder=False)``
+    then ``Shift(axis, 1)`` for each axis.  MPI numbers a cartesian
+    communicator's ranks in row-major order of their coordinates (the last
+    axis fastest), so these neighbours follow that order -- not the x-fastest
+    ``_rank_to_coords`` that places the sub-domain (topology.py:56-61).
+    -1 marks a physical face."""
+    c = [rank // (sd[1] * sd[2]), (rank // sd[2]) % sd[1], rank % sd[2]]
+    out = {}
+    for axis, name in enumerate("xyz"):
+        pair = []
+        for step in (-1, 1):
+            cc = list(c)
+            cc[axis] += step
+            if 0 <= cc[axis] < sd[axis]:
+                pair.append((cc[0] * sd[1] + cc[1]) * sd[2] + cc[2])
+            else:
+                pair.append(-1)
+        out[name] = tuple(pair)
+    return out
+
+
+def phys_faces(neighbors):
+    """multigrid.py:229-231: a face is physical where it has no neighbour
+    (the cavity has no periodic face).  Order west, east, south, north,
+    bottom, top."""
+    return tuple(neighbors["xyz"[f // 2]][f % 2] < 0 for f in range(6))
+
+
+class RankComm:
+    """The reference's communicator calls at one rank of a decomposed run,
+    over a torch.distributed group (gloo): ``allreduce`` (solver.py:120,
+    134, 150, 176) and the HaloExchanger (halo.py:81-130)."""
+
+    def __init__(self, neighbors):
+        self.neighbors = neighbors
+
+    def allreduce(self, x, op):
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([float(x)], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.MIN)
+        return float(t.item())
+
+    def _sendrecv(self, snd, peer, stag, rcv, rtag):
+        import torch
+        import torch.distributed as dist
+        st = torch.from_numpy(np.ascontiguousarray(snd))
+        rt = torch.empty(rcv.shape, dtype=torch.float64)
+        req = dist.isend(st, dst=peer, tag=stag)
+        dist.recv(rt, src=peer, tag=rtag)
+        req.wait()
+        rcv[...] = rt.numpy()
+
+    def exchange(self, arr, npl, nl=None):
+        """halo.py:81-130: per axis x, y, z, the ``nl`` real layers next to
+        each seam go to the neighbour and its layers land in this side's
+        ghosts; a slab spans the whole array in the other two axes, ghosts
+        included (tags 21 / 22 paired by data flow)."""
+        nl = npl if nl is None else nl
+        for axis in range(3):
+            lo, hi = self.neighbors["xyz"[axis]]
+            if lo < 0 and hi < 0:
+                continue
+            n = arr.shape[axis] - 2 * npl
+            send_lo, send_hi = npl, npl + n - nl
+            recv_lo, recv_hi = npl - nl, npl + n
+            pairs = []
+            if lo >= 0:
+                pairs.append((lo, send_lo, recv_lo, 21, 22))
+            if hi >= 0:
+                pairs.append((hi, send_hi, recv_hi, 22, 21))
+            for peer, so, ro, stag, rtag in pairs:
+                sl = [slice(None)] * 3
+                sl[axis] = slice(so, so + nl)
+                rl = [slice(None)] * 3
+                rl[axis] = slice(ro, ro + nl)
+                self._sendrecv(arr[tuple(sl)], peer, stag, arr[tuple(rl)], rtag)
+
+
+# --------------------------------------------------------------------------
 # solver (solver.py)
 # --------------------------------------------------------------------------
 FIELDS = ("u", "v", "w", "p", "ustar", "vstar", "wstar", "uoo", "voo", "woo",
@@ -527,14 +641,19 @@ FIELDS = ("u", "v", "w", "p", "ustar", "vstar", "wstar", "uoo", "voo", "woo",
 
 
 class OracleSolver:
-    """solver.py:29-271 at one rank; ``cfg`` is the reference-shaped
-    CaseConfig (config.py:88-98)."""
+    """solver.py:29-271; ``cfg`` is the reference-shaped CaseConfig
+    (config.py:88-98).  One rank by default; with ``rank``/``comm`` (a
+    RankComm over a gloo group of sd_x * sd_y * sd_z processes) this is one
+    sub-domain of the decomposed run (topology.py:30-53)."""
 
-    def __init__(self, cfg):
+    def __init__(self, cfg, comm=None):
         self.cfg = cfg
-        n = cfg.grid.nx
+        self.comm = comm
+        sd = tuple(int(m) for m in cfg.mpi.domains)
+        gn = (cfg.grid.nx, cfg.grid.ny, cfg.grid.nz)
+        self.ncells = tuple(g // d for g, d in zip(gn, sd))
+        n = self.ncells[0]
         self.n = n
-        self.ncells = (cfg.grid.nx, cfg.grid.ny, cfg.grid.nz)
         self.dx = cfg.domain.lx / cfg.grid.nx
         self.dy = cfg.domain.ly / cfg.grid.ny
         self.dz = cfg.domain.lz / cfg.grid.nz
@@ -542,7 +661,9 @@ class OracleSolver:
         shp = (n + 2 * NPL,) * 3
         self.f = {k: np.zeros(shp) for k in FIELDS}
         self.ulid = cfg.boundaries.lid_velocity
-        self.mg = Multigrid(n, cfg.numerics.mg_levels, self.dx, self.dy, self.dz)
+        phys = phys_faces(comm.neighbors) if comm is not None else ALL_PHYS
+        self.mg = Multigrid(n, cfg.numerics.mg_levels, self.dx, self.dy, self.dz,
+                            phys=phys, comm=comm)
         self.dt = cfg.time.dt_init
         self.ctime = 0.0
         self.itime = 0
@@ -555,8 +676,17 @@ class OracleSolver:
         self.f["vis"][...] = self.rey
         apply_initial(self.f, n, self.ulid)
 
+    def _exchange(self, name):
+        if self.comm is not None:
+            self.comm.exchange(self.f[name], NPL)
+
+    def _allreduce(self, x, op):
+        return x if self.comm is None else self.comm.allreduce(x, op)
+
     def fill_bc(self, name):
-        """solver.py:88-97."""
+        """solver.py:88-97: halo exchange, then the ghost fills (which the
+        reference applies on all six faces at every rank)."""
+        self._exchange(name)
         if name == "u":
             apply_u(self.f["u"], self.n, self.ulid)
         elif name == "v":
@@ -567,8 +697,11 @@ class OracleSolver:
     def compute_dt(self):
         """solver.py:122-150."""
         f, n = self.f, self.n
-        umax, vmax, wmax = maxabs(f["u"], n), maxabs(f["v"], n), maxabs(f["w"], n)
-        dtv = dtvisc(f["u"], f["v"], f["w"], f["vis"], self.dx, self.dy, self.dz, n)
+        umax = self._allreduce(maxabs(f["u"], n), "max")
+        vmax = self._allreduce(maxabs(f["v"], n), "max")
+        wmax = self._allreduce(maxabs(f["w"], n), "max")
+        dtv = self._allreduce(
+            dtvisc(f["u"], f["v"], f["w"], f["vis"], self.dx, self.dy, self.dz, n), "min")
         big = 1.0e10
         dtcfl = big
         for d, um in zip((self.dx, self.dy, self.dz), (umax, vmax, wmax)):
@@ -579,20 +712,22 @@ class OracleSolver:
             raise RuntimeError("time step collapsed (dtmax = %.3e)" % dtmax)
         self.cfl = self.dt / dtmax
         if self.cfg.time.variable_dt:
-            self.dt = min(self.dt * self.cfg.time.dt_growth,
-                          self.cfg.time.safety_factor * dtmax)
+            self.dt = self._allreduce(min(self.dt * self.cfg.time.dt_growth,
+                                          self.cfg.time.safety_factor * dtmax), "min")
 
     def _calvel(self, alpha):
-        """solver.py:155-166."""
+        """solver.py:155-166 (the halo exchange of u, v, w closes it)."""
         f = self.f
         for comp, star, d in (("u", "ustar", self.dx), ("v", "vstar", self.dy),
                               ("w", "wstar", self.dz)):
             calvel(comp, f[star], f["p"], f[comp], d, self.dt, alpha, self.n)
+        for name in ("u", "v", "w"):
+            self._exchange(name)
 
     def _calmas(self):
         f = self.f
-        self.rmax = calmas(f["u"], f["v"], f["w"], f["su"], self.dx, self.dy,
-                           self.dz, self.dt, self.n)
+        self.rmax = self._allreduce(calmas(f["u"], f["v"], f["w"], f["su"], self.dx,
+                                           self.dy, self.dz, self.dt, self.n), "max")
 
     def _project(self):
         """solver.py:178-212."""
@@ -613,6 +748,7 @@ class OracleSolver:
                                    % (self.rmax, self.itime))
             self.mg.solve(f["su"], f["pp"], self.n)
             add_ring(f["p"], f["pp"], self.n)
+            self._exchange("p")
             apply_pbound(f["p"], self.n)
             self._calvel(1.0)
         self.outer_iters = iters

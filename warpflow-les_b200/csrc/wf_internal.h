@@ -181,6 +181,12 @@ int mg_solve_noalloc(const double* su, double* pp, int n, int nlev, double dx, d
                      double dz, cudaStream_t s);
 int mg_noalloc_status(void* stream, int32_t* status);
 int wait_probe(unsigned* gbar, int* err, int kind, int tries, cudaStream_t s);
+// sub-domains (more than one rank per case)
+int launch_box(double* arr, long sI, long sJ, int i0, int j0, int k0, int ni, int nj, int nk,
+               double* buf, int unpack, cudaStream_t s);
+int rk_mg_op(const wf_case& c, int op, int level, int phys, int color, cudaStream_t s);
+int rk_level_view(const wf_case& c, int level, double** phi, int64_t* sI, int64_t* sJ,
+                  int32_t* m);
 int mg_residual_max_pair(const wf_case& c, const double* phi0, const double* rhs0,
                          double* out, cudaStream_t s);
 

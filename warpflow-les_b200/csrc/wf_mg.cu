@@ -2958,4 +2958,191 @@ int mg_noalloc_status(void* stream, int32_t* status) {
   return WF_OK;
 }
 
+
+// ---------------------------------------------------------------------------
+// Sub-domains (the reference's multigrid.py and halo.py at more than one
+// rank).  At a seam between ranks the reference keeps the face coefficient
+// (multigrid.py:23-67 zeroes it only across a physical face) and refreshes
+// the one-cell ring by a halo exchange once per full sweep, after the
+// Neumann mirror of the physical faces (multigrid.py:264-299).  These
+// kernels do one reference pass each, on a level of a case whose level 0 is
+// the core of pp and su (as mg_solve); the ring at the seams is the host's:
+//   op 0  one colour half-sweep (multigrid.py:70-90), no ring writes
+//   op 1  Neumann mirror of the physical faces' interiors (bcs.py:326-360)
+//   op 2  restriction from level-1 to level (multigrid.py:93-119), the
+//         coarse phi zeroed, ring included (multigrid.py:310-312)
+//   op 3  prolongation from level+1 to level, real cells only (122-146)
+//   op 4  pp zeroed over the whole padded array (multigrid.py:332-333)
+// `phys` holds one bit per face, set when the face is physical: bit 0 west,
+// 1 east, 2 south, 3 north, 4 bottom, 5 top.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double seam_coef(bool edge, int phys, int bit, double a) {
+  return (edge && ((phys >> bit) & 1)) ? 0.0 : a;
+}
+
+__global__ void __launch_bounds__(MG_TPB) k_rk_rbgs(const Lvl<double> L, int phys, int color) {
+  pdl_entry();
+  const int n = L.n;
+  const int kx = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
+  const int i = blockIdx.z;
+  if (kx >= (n + 1) / 2 || j >= n) return;
+  const int k = 2 * kx + ((1 + i + j + color) & 1);
+  if (k >= n) return;
+  const long c = lid(L, i + 1, j + 1, k + 1);
+  const double aw = seam_coef(i == 0, phys, 0, L.ax), ae = seam_coef(i == n - 1, phys, 1, L.ax);
+  const double as = seam_coef(j == 0, phys, 2, L.ay), an = seam_coef(j == n - 1, phys, 3, L.ay);
+  const double ab = seam_coef(k == 0, phys, 4, L.az), at = seam_coef(k == n - 1, phys, 5, L.az);
+  const double ap = -(aw + ae + as + an + ab + at);
+  const double* p = L.phi;
+  const double s = aw * p[c - L.sI] + ae * p[c + L.sI] + as * p[c - L.sJ] + an * p[c + L.sJ] +
+                   ab * p[c - 1] + at * p[c + 1];
+  L.phi[c] = (L.rhs[c] - s) / ap;
+}
+
+__global__ void k_rk_mirror(const Lvl<double> L, int phys) {
+  pdl_entry();
+  const int n = L.n;
+  const long tot = (long)n * n;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
+       t += (long)gridDim.x * blockDim.x) {
+    const int a = 1 + (int)(t / n), b = 1 + (int)(t % n);
+    double* p = L.phi;
+    if (phys & 1) p[lid(L, 0, a, b)] = p[lid(L, 1, a, b)];
+    if (phys & 2) p[lid(L, n + 1, a, b)] = p[lid(L, n, a, b)];
+    if (phys & 4) p[lid(L, a, 0, b)] = p[lid(L, a, 1, b)];
+    if (phys & 8) p[lid(L, a, n + 1, b)] = p[lid(L, a, n, b)];
+    if (phys & 16) p[lid(L, a, b, 0)] = p[lid(L, a, b, 1)];
+    if (phys & 32) p[lid(L, a, b, n + 1)] = p[lid(L, a, b, n)];
+  }
+}
+
+__global__ void __launch_bounds__(MG_TPB) k_rk_restrict(const Lvl<double> F, Lvl<double> C,
+                                                        int phys) {
+  pdl_entry();
+  const int nc = C.n, n = F.n;
+  const int ck = blockIdx.x * 32 + threadIdx.x, cj = blockIdx.y * 8 + threadIdx.y;
+  const int ci = blockIdx.z;
+  if (ck >= nc || cj >= nc) return;
+  const double* p = F.phi;
+  double acc = 0.0;
+  for (int di = 0; di < 2; ++di)
+    for (int dj = 0; dj < 2; ++dj)
+      for (int dk = 0; dk < 2; ++dk) {
+        const int i = 2 * ci + di, j = 2 * cj + dj, k = 2 * ck + dk;
+        const long c = lid(F, i + 1, j + 1, k + 1);
+        const double aw = seam_coef(i == 0, phys, 0, F.ax), ae = seam_coef(i == n - 1, phys, 1, F.ax);
+        const double as = seam_coef(j == 0, phys, 2, F.ay), an = seam_coef(j == n - 1, phys, 3, F.ay);
+        const double ab = seam_coef(k == 0, phys, 4, F.az), at = seam_coef(k == n - 1, phys, 5, F.az);
+        const double ap = -(aw + ae + as + an + ab + at);
+        const double res = F.rhs[c] - (aw * p[c - F.sI] + ae * p[c + F.sI] + as * p[c - F.sJ] +
+                                       an * p[c + F.sJ] + ab * p[c - 1] + at * p[c + 1] +
+                                       ap * p[c]);
+        acc = acc + res;
+      }
+  const_cast<double*>(C.rhs)[lid(C, ci + 1, cj + 1, ck + 1)] = acc * 0.125;
+  // every cell of the (nc+2)^3 coarse phi zeroed once: this cell and the
+  // ring cells nearest to it
+  const int zi0 = ci == 0 ? -1 : 0, zi1 = ci == nc - 1 ? 1 : 0;
+  const int zj0 = cj == 0 ? -1 : 0, zj1 = cj == nc - 1 ? 1 : 0;
+  const int zk0 = ck == 0 ? -1 : 0, zk1 = ck == nc - 1 ? 1 : 0;
+  for (int oi = zi0; oi <= zi1; ++oi)
+    for (int oj = zj0; oj <= zj1; ++oj)
+      for (int ok = zk0; ok <= zk1; ++ok)
+        C.phi[lid(C, ci + 1 + oi, cj + 1 + oj, ck + 1 + ok)] = 0.0;
+}
+
+__global__ void __launch_bounds__(MG_TPB) k_rk_prolong(const Lvl<double> C, Lvl<double> F) {
+  pdl_entry();
+  const int n = F.n;
+  const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
+  const int i = blockIdx.z;
+  if (k >= n || j >= n) return;
+  const int c0x = (i % 2 == 0) ? i / 2 - 1 : i / 2;
+  const double wx0 = (i % 2 == 0) ? 0.25 : 0.75;
+  const int c0y = (j % 2 == 0) ? j / 2 - 1 : j / 2;
+  const double wy0 = (j % 2 == 0) ? 0.25 : 0.75;
+  const int c0z = (k % 2 == 0) ? k / 2 - 1 : k / 2;
+  const double wz0 = (k % 2 == 0) ? 0.25 : 0.75;
+  double acc = 0.0;
+  for (int di = 0; di < 2; ++di) {
+    const double wxi = di == 0 ? wx0 : 1.0 - wx0;
+    for (int dj = 0; dj < 2; ++dj) {
+      const double wyj = dj == 0 ? wy0 : 1.0 - wy0;
+      for (int dk = 0; dk < 2; ++dk) {
+        const double wzk = dk == 0 ? wz0 : 1.0 - wz0;
+        acc = acc + wxi * wyj * wzk * C.phi[lid(C, c0x + di + 1, c0y + dj + 1, c0z + dk + 1)];
+      }
+    }
+  }
+  const long c = lid(F, i + 1, j + 1, k + 1);
+  F.phi[c] = F.phi[c] + acc;
+}
+
+// the levels of a case, level 0 the one-ring core of pp (phi) and su (rhs)
+static int rank_levels(const wf_case& c, std::vector<Lvl<double>>& lv) {
+  const long P = padded(c.n);
+  const long off = (long)(NPL - 1) * (P * P + P + 1);
+  WF_TRY(build_levels<double>(c, c.fld[WF_PP] + off, c.fld[WF_SU] + off, P * P, P, lv));
+  for (auto& L : lv) {
+    L.tmp = nullptr;
+    L.split = 0;
+  }
+  return WF_OK;
+}
+
+int rk_mg_op(const wf_case& c, int op, int level, int phys, int color, cudaStream_t s) {
+  if (c.mg_fp32) return fail(WF_EUNSUPPORTED, "sub-domain multigrid runs in FP64");
+  if (!c.fld[WF_PP] || !c.fld[WF_SU]) return fail(WF_EINVAL, "null pp or su");
+  if (phys < 0 || phys > 63) return fail(WF_EINVAL, "face mask out of range");
+  std::vector<Lvl<double>> lv;
+  WF_TRY(rank_levels(c, lv));
+  const int L = (int)lv.size();
+  if (level < 0 || level >= L) return fail(WF_EINVAL, "level out of range");
+  const Lvl<double>& V = lv[level];
+  switch (op) {
+    case 0:
+      if (color != 0 && color != 1) return fail(WF_EINVAL, "colour must be 0 or 1");
+      WF_CK(launch_k(k_rk_rbgs, cells3(V.n, V.n, (V.n + 1) / 2), cell_block(), 0, s, V, phys,
+                     color));
+      WF_CKL("k_rk_rbgs");
+      return WF_OK;
+    case 1:
+      WF_CK(launch_k(k_rk_mirror, mg_blocks((long)V.n * V.n), MG_TPB, 0, s, V, phys));
+      WF_CKL("k_rk_mirror");
+      return WF_OK;
+    case 2:
+      if (level < 1) return fail(WF_EINVAL, "restriction needs level >= 1");
+      WF_CK(launch_k(k_rk_restrict, cells3(V.n, V.n, V.n), cell_block(), 0, s, lv[level - 1],
+                     V, phys));
+      WF_CKL("k_rk_restrict");
+      return WF_OK;
+    case 3:
+      if (level > L - 2) return fail(WF_EINVAL, "prolongation needs a coarser level");
+      WF_CK(launch_k(k_rk_prolong, cells3(V.n, V.n, V.n), cell_block(), 0, s, lv[level + 1], V));
+      WF_CKL("k_rk_prolong");
+      return WF_OK;
+    case 4: {
+      const long P = padded(c.n);
+      WF_CK(launch_k(k_zero<double>, mg_blocks(P * P * P), MG_TPB, 0, s, c.fld[WF_PP], P * P * P,
+                     (int)WF_PP));
+      WF_CKL("k_zero pp");
+      return WF_OK;
+    }
+    default:
+      return fail(WF_EINVAL, "unknown sub-domain multigrid op");
+  }
+}
+
+int rk_level_view(const wf_case& c, int level, double** phi, int64_t* sI, int64_t* sJ,
+                  int32_t* m) {
+  std::vector<Lvl<double>> lv;
+  WF_TRY(rank_levels(c, lv));
+  if (level < 0 || level >= (int)lv.size()) return fail(WF_EINVAL, "level out of range");
+  *phi = lv[level].phi;
+  *sI = lv[level].sI;
+  *sJ = lv[level].sJ;
+  *m = lv[level].n + 2;
+  return WF_OK;
+}
+
 }  // namespace wf

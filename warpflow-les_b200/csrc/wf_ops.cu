@@ -804,4 +804,40 @@ int launch_add_ring(double* p, const double* pp, int n, cudaStream_t s) {
   return WF_OK;
 }
 
+
+// --------------------------------------------------------------------------
+// halo slabs of a sub-domain (reference halo.py:16-55 gather/scatter): a box
+// of a strided 3-D array (k contiguous) to and from a dense buffer ordered
+// [i][j][k], so a slab along any axis is one contiguous message
+// --------------------------------------------------------------------------
+__global__ void k_box(double* arr, long sI, long sJ, int i0, int j0, int k0, int ni, int nj,
+                      int nk, double* buf, int unpack) {
+  pdl_entry();
+  const long tot = (long)ni * nj * nk;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
+       t += (long)gridDim.x * blockDim.x) {
+    const int k = (int)(t % nk);
+    const long r = t / nk;
+    const int j = (int)(r % nj), i = (int)(r / nj);
+    const long a = (long)(i0 + i) * sI + (long)(j0 + j) * sJ + (k0 + k);
+    if (unpack)
+      arr[a] = buf[t];
+    else
+      buf[t] = arr[a];
+  }
+}
+
+int launch_box(double* arr, long sI, long sJ, int i0, int j0, int k0, int ni, int nj, int nk,
+               double* buf, int unpack, cudaStream_t s) {
+  if (!arr || !buf) return fail(WF_EINVAL, "null array or buffer");
+  if (ni < 0 || nj < 0 || nk < 0 || i0 < 0 || j0 < 0 || k0 < 0 || sJ < nk + k0 || sI < sJ)
+    return fail(WF_EINVAL, "box out of range");
+  const long tot = (long)ni * nj * nk;
+  if (tot == 0) return WF_OK;
+  WF_CK(launch_k(k_box, nblocks(tot), TPB, 0, s, arr, sI, sJ, i0, j0, k0, ni, nj, nk, buf,
+                 unpack));
+  WF_CKL("k_box");
+  return WF_OK;
+}
+
 }  // namespace wf

@@ -500,6 +500,27 @@ int wf_mg_build_coarse_op(const wf_case* c, void* s) {
   return build_coarse_op_case(*c, (cudaStream_t)s);
 }
 
+int wf_box_copy(double* arr, int64_t sI, int64_t sJ, int32_t i0, int32_t j0, int32_t k0,
+                int32_t ni, int32_t nj, int32_t nk, double* buf, int32_t unpack, void* s) {
+  return launch_box(arr, sI, sJ, i0, j0, k0, ni, nj, nk, buf, unpack ? 1 : 0, (cudaStream_t)s);
+}
+int wf_copy_oo(const wf_case* c, void* s) {
+  if (!c) return fail(WF_EINVAL, "null case");
+  for (int f : {WF_U, WF_V, WF_W, WF_UOO, WF_VOO, WF_WOO})
+    if (!c->fld[f]) return fail(WF_EINVAL, "null field pointer");
+  return launch_copy_oo(*c, (cudaStream_t)s);
+}
+int wf_rk_mg_op(const wf_case* c, int32_t op, int32_t level, int32_t phys, int32_t color,
+                void* s) {
+  if (!c) return fail(WF_EINVAL, "null case");
+  return rk_mg_op(*c, op, level, phys, color, (cudaStream_t)s);
+}
+int wf_rk_level_view(const wf_case* c, int32_t level, double** phi, int64_t* sI, int64_t* sJ,
+                     int32_t* m) {
+  if (!c || !phi || !sI || !sJ || !m) return fail(WF_EINVAL, "null argument");
+  return rk_level_view(*c, level, phi, sI, sJ, m);
+}
+
 int wf_mg_refill(const wf_case* c, double* phi0, void* s) {
   if (!c || !phi0) return fail(WF_EINVAL, "null argument");
   return mg_refill_pair(*c, phi0, (cudaStream_t)s);
