@@ -79,6 +79,7 @@ class WfCase(ctypes.Structure):
 
 _VP = ctypes.c_void_p
 _I32 = ctypes.c_int32
+_I64 = ctypes.c_int64
 _D = ctypes.c_double
 _CP = ctypes.POINTER(WfCase)
 
@@ -125,6 +126,12 @@ SIGNATURES = {
     "wf_mg_dc_cycle": (_I32, [_CP, _VP, _VP, _VP]),
     "wf_mg_residual_max": (_I32, [_CP, _VP, _VP, _VP, _VP]),
     "wf_mg_refill": (_I32, [_CP, _VP, _VP]),
+    "wf_box_copy": (_I32, [_VP, _I64, _I64, _I32, _I32, _I32, _I32, _I32, _I32, _VP, _I32,
+                           _VP]),
+    "wf_copy_oo": (_I32, [_CP, _VP]),
+    "wf_rk_mg_op": (_I32, [_CP, _I32, _I32, _I32, _I32, _VP]),
+    "wf_rk_level_view": (_I32, [_CP, _I32, ctypes.POINTER(_VP), ctypes.POINTER(_I64),
+                                ctypes.POINTER(_I64), ctypes.POINTER(_I32)]),
     "wf_stepper_create": (_I32, [_CP, _I32, ctypes.POINTER(_VP)]),
     "wf_stepper_step": (_I32, [_VP, _VP]),
     "wf_stepper_destroy": (_I32, [_VP]),
