@@ -7,6 +7,14 @@ Runs `time.n_steps` (or --steps) FlowSolver steps, prints the reference's
 log line every `output.log_interval` steps and writes a snapshot every
 `output.n_out` steps and at the end.  --resume continues from a snapshot
 written by this build.
+
+A case whose `mpi.domains` has more than one sub-domain runs one process
+per rank under torchrun, where the reference runs under mpirun:
+
+    torchrun --nproc-per-node 8 warpflow-les_b200/run.py --case case.yaml
+
+Each rank joins the process group (NCCL between GPUs) on GPU LOCAL_RANK
+and writes its own snapshot files (snap_<itime>_r<rank>.npz).
 """
 import argparse
 import os
@@ -17,6 +25,25 @@ sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 
 from warpflow import FlowSolver, __version__, build_topology, load_case  # noqa: E402
 from warpflow.io import SnapshotWriter, read_snapshot, restore  # noqa: E402
+
+
+def _join_ranks(cfg):
+    """Join the torch.distributed group for a decomposed case; returns the
+    rank's GPU, or None for a single-domain case (or when torchrun did not
+    start several processes: build_topology then reports the mismatch)."""
+    sd = cfg.mpi.domains
+    if sd[0] * sd[1] * sd[2] == 1 or int(os.environ.get("WORLD_SIZE", "1")) == 1:
+        return None
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if not dist.is_initialized():
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return "cuda:%d" % local
 
 
 def main(argv=None):
@@ -33,8 +60,11 @@ def main(argv=None):
     if args.outdir:
         cfg.output.outdir = args.outdir
     nsteps = args.steps if args.steps is not None else cfg.time.n_steps
+    rank_dev = _join_ranks(cfg)
     topo = build_topology(cfg)
-    device = "cuda:0" if args.device == "auto" else args.device
+    device = args.device
+    if device == "auto":
+        device = rank_dev or "cuda:0"
     if topo.rank == 0:
         print("warpflow-les %s: case=%s grid=%dx%dx%d domains=%s device=%s"
               % (__version__, cfg.name, cfg.grid.nx, cfg.grid.ny, cfg.grid.nz,
@@ -62,6 +92,9 @@ def main(argv=None):
         print("done: itime=%d ctime=%.6f wall=%.1fs" % (last, sol.ctime, time.time() - t0),
               flush=True)
     sol.close()
+    if rank_dev is not None:
+        import torch.distributed as dist
+        dist.destroy_process_group()
 
 
 if __name__ == "__main__":

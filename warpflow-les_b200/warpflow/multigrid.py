@@ -16,6 +16,13 @@ The level-0 ``phi``/``rhs`` arrays serve the standalone harness form
 in FP32 as a correction of an FP64 defect correction: the residual, the
 accumulation of the solution and everything outside the multigrid stay FP64.
 
+At a sub-domain of a decomposed case (``topo.nranks`` > 1) the solve runs
+the reference's own sequence (multigrid.py:264-337) from the host, one
+device pass at a time (``wf_rk_mg_op``): face coefficients kept across the
+seams between ranks, the Neumann mirror on the physical faces only, and a
+halo exchange of the one-cell ring after every full sweep and every
+prolongation; FP64, coarsest level by sweeps.
+
 ``coarse="operator"`` (config ``numerics.mg_coarse``, the default) runs
 the coarsest level's n_coarse sweeps from zero -- a fixed linear map of its
 rhs -- through one precomputed dense operator on the even-parity half of
@@ -61,12 +68,19 @@ class _CoeffView:
         for name, c in (("aw", cx), ("ae", cx), ("as_", cy), ("an", cy),
                         ("ab", cz), ("at", cz)):
             core[name] = np.full((n, n, n), c)
-        core["aw"][0] = 0.0
-        core["ae"][n - 1] = 0.0
-        core["as_"][:, 0] = 0.0
-        core["an"][:, n - 1] = 0.0
-        core["ab"][:, :, 0] = 0.0
-        core["at"][:, :, n - 1] = 0.0
+        phys = getattr(self.lev, "phys", (True,) * 6)
+        if phys[0]:
+            core["aw"][0] = 0.0
+        if phys[1]:
+            core["ae"][n - 1] = 0.0
+        if phys[2]:
+            core["as_"][:, 0] = 0.0
+        if phys[3]:
+            core["an"][:, n - 1] = 0.0
+        if phys[4]:
+            core["ab"][:, :, 0] = 0.0
+        if phys[5]:
+            core["at"][:, :, n - 1] = 0.0
         if self.which == "ap":
             val = -(core["aw"] + core["ae"] + core["as_"] + core["an"]
                     + core["ab"] + core["at"])
@@ -77,7 +91,8 @@ class _CoeffView:
 
 
 class _Level:
-    def __init__(self, n3, h, device, dtype=torch.float64):
+    def __init__(self, n3, h, device, dtype=torch.float64, phys=(True,) * 6):
+        self.phys = tuple(phys)
         self.n3 = tuple(n3)
         self.shape = tuple(x + 2 for x in n3)
         self.h = tuple(h)
@@ -96,6 +111,16 @@ class Multigrid:
         self.coarse = coarse or getattr(cfg.numerics, "mg_coarse", "operator")
         if self.coarse not in ("operator", "sweeps"):
             raise ValueError("coarse must be 'operator' or 'sweeps'")
+        # a sub-domain: physical faces are those without a neighbour rank
+        # (multigrid.py:229-231); its solve is the reference's sequence
+        self.ranks = topo.nranks > 1
+        self.phys = tuple(topo.neighbors["xyz"[f // 2]][f % 2] < 0 for f in range(6))
+        self.phys_mask = sum(1 << f for f in range(6) if self.phys[f])
+        self.halo = None
+        if self.ranks:
+            if self.precision != "fp64":
+                raise ValueError("mg_precision 'mixed' runs at one rank per case")
+            self.coarse = "sweeps"
         self._cop_part = None
         self.topo = topo
         self.device = cuda_device(device)
@@ -107,7 +132,7 @@ class Multigrid:
         for l in range(cfg.numerics.mg_levels):
             s = 2.0 ** l
             self.levels.append(_Level(tuple(x >> l for x in nb),
-                                      (dx * s, dy * s, dz * s), self.device))
+                                      (dx * s, dy * s, dz * s), self.device, phys=self.phys))
         self._f32 = []
         if self.precision == "mixed":
             for lev in self.levels:
@@ -238,4 +263,51 @@ class Multigrid:
         for i, name in enumerate(_abi.FIELD_NAMES):
             if not c.fld[i]:
                 c.fld[i] = su3.ptr  # unused slots must be non-null for validation
+        if self.ranks:
+            self._solve_ranks(c)
+            return
         _abi.call("wf_mg_solve", ctypes.byref(c), self._stream())
+
+    # -- sub-domain form: the reference's sequence, one pass at a time -- #
+    def _rk(self, c, op, level, color=0):
+        _abi.call("wf_rk_mg_op", ctypes.byref(c), op, level, self.phys_mask, color,
+                  self._stream())
+
+    def _rk_refill(self, c, views, l):
+        """multigrid.py:264-287: mirror at the physical faces, then the halo
+        exchange of the ring."""
+        self._rk(c, 1, l)
+        ptr, sI, sJ, m = views[l]
+        self.halo.exchange_view(ptr, sI, sJ, (m, m, m))
+
+    def _rk_relax(self, c, views, l, nsweeps):
+        """multigrid.py:289-299: red, black, one refill per sweep."""
+        for _ in range(nsweeps):
+            self._rk(c, 0, l, 0)
+            self._rk(c, 0, l, 1)
+            self._rk_refill(c, views, l)
+
+    def _solve_ranks(self, c):
+        """multigrid.py:301-337 at a sub-domain: pp zeroed, n_vcycles
+        V-cycles on level 0 = the core of pp (phi) and su (rhs)."""
+        if self.halo is None:
+            from .halo import HaloExchanger
+            self.halo = HaloExchanger(self.topo, self.device, NPL_MG)
+        L = c.nlev
+        views = []
+        for l in range(L):
+            ptr, sI, sJ, m = ctypes.c_void_p(), ctypes.c_int64(), ctypes.c_int64(), \
+                ctypes.c_int32()
+            _abi.call("wf_rk_level_view", ctypes.byref(c), l, ctypes.byref(ptr),
+                      ctypes.byref(sI), ctypes.byref(sJ), ctypes.byref(m))
+            views.append((ptr.value, sI.value, sJ.value, m.value))
+        self._rk(c, 4, 0)
+        for _ in range(self.n_vcycles):
+            for l in range(L):
+                if l > 0:
+                    self._rk(c, 2, l)
+                self._rk_relax(c, views, l, self.n_pre if l < L - 1 else self.n_coarse)
+            for l in range(L - 2, -1, -1):
+                self._rk(c, 3, l)
+                self._rk_refill(c, views, l)
+                self._rk_relax(c, views, l, self.n_post)

@@ -12,6 +12,13 @@ Public interface as the reference (solver.py:29-271): constructor
 cfl}``, the field dict ``f`` (13 names), ``ncells``, ``dx/dy/dz``, ``rey``,
 ``dt``, ``ctime``, ``itime``, ``rmax``, ``cfl``, ``outer_iters``, ``bnd``,
 ``ulid``, ``mg``, ``cfg``, ``topo``; same exception messages.
+
+At a sub-domain of a decomposed case (``topo.nranks`` > 1, one process per
+GPU) ``step()`` runs the reference's own sequence from the host instead of
+the graph: each device pass through its C-ABI entry, the halo exchange
+before every ghost fill and after every velocity correction, and the
+reference's allreduces of the dt reductions and of the divergence maximum
+(solver.py:88-212).
 """
 from __future__ import annotations
 
@@ -24,7 +31,7 @@ from . import _abi
 from .bcs import BoundaryKernels
 from .fields import DeviceField, cuda_device
 from .multigrid import Multigrid
-from .topology import NPL
+from .topology import MAX, MIN, NPL
 
 ALFARK = (0.5, 1.0)  # Heun RK2 stage coefficients (reference solver.py:26)
 
@@ -79,12 +86,19 @@ class FlowSolver:
         self.case = self._make_case()
         self._init_state()
 
+        self.ranks = topo.nranks > 1
+        self._stepper = None
+        self.serial = bool(serial)
+        if self.ranks:
+            from .halo import HaloExchanger
+            self.halo = HaloExchanger(topo, dev, NPL)
+            self.step_mode = "ranks"
+            return
         mode = step_mode or os.environ.get("WF_STEP_MODE", "graph")
         if mode not in STEP_MODES:
             raise ValueError("step_mode must be one of %s" % sorted(STEP_MODES))
         self.step_mode = mode
         self._stepper = ctypes.c_void_p()
-        self.serial = bool(serial)
         _abi.call("wf_stepper_create", ctypes.byref(self.case),
                   STEP_MODES[mode] | (STEP_SERIAL if serial else 0),
                   ctypes.byref(self._stepper))
@@ -210,11 +224,110 @@ class FlowSolver:
 
     def step(self):
         """One time step (reference solver.py:217-271)."""
+        if self.ranks:
+            return self._step_ranks()
         self.launch_step()
         return self.finish_step()
 
+    # -- sub-domain form (solver.py:88-271 at one of several ranks) ------ #
+    def _fill_bc_ranks(self, name):
+        """solver.py:88-97: halo exchange, then the ghost fills (the
+        reference fills all six faces at every rank)."""
+        self.halo.exchange(self.f[name])
+        self.fill_bc(name)
+
+    def _calvel_ranks(self, alpha):
+        """solver.py:155-166: the correction, then the halo exchange of u,
+        v, w (no ghost fill)."""
+        _abi.call("wf_calvel", ctypes.byref(self.case), float(alpha), self._dt_dev,
+                  self._stream())
+        for name in ("u", "v", "w"):
+            self.halo.exchange(self.f[name])
+
+    def _step_ranks(self):
+        c, s, comm = ctypes.byref(self.case), self._stream(), self.topo.comm
+        cfg = self.cfg
+        self._dt_dev = ctypes.c_void_p(self._sc.data_ptr() + _abi.WfScalars.dt.offset)
+        self.itime += 1
+        # solver.py:122-150: this rank's reductions on the device, the
+        # global ones and the dt update on the host
+        _abi.call("wf_checkdt", c, s)
+        sc = self._pull_scalars()
+        umax = comm.allreduce(float(sc.umax), op=MAX)
+        vmax = comm.allreduce(float(sc.vmax), op=MAX)
+        wmax = comm.allreduce(float(sc.wmax), op=MAX)
+        dtvisc = comm.allreduce(float(sc.dtvisc), op=MIN)
+        big = 1.0e10
+        dtcfl = big
+        for d, um in zip((self.dx, self.dy, self.dz), (umax, vmax, wmax)):
+            if um > 0.0:
+                dtcfl = min(dtcfl, d / um)
+        dtmax = min(dtvisc, dtcfl)
+        if dtmax <= 0.0 or not (dtmax < big):
+            raise RuntimeError("time step collapsed (dtmax = %.3e)" % dtmax)
+        self.cfl = self._dt / dtmax
+        if cfg.time.variable_dt:
+            self._dt = comm.allreduce(min(self._dt * cfg.time.dt_growth,
+                                          cfg.time.safety_factor * dtmax), op=MIN)
+        self._ctime += self._dt
+        sc.dt, sc.ctime, sc.itime, sc.cfl, sc.dtmax = (self._dt, self._ctime, self.itime,
+                                                       self.cfl, dtmax)
+        sc.status = _abi.ST_OK
+        self._sc.copy_(self._sc_host, non_blocking=True)
+        torch.cuda.current_stream(self.device).synchronize()
+
+        _abi.call("wf_copy_oo", c, s)
+        _abi.call("wf_wale_vis", c, s)
+        for stage, alpha in enumerate(ALFARK):
+            for comp in range(3):
+                self._fill_bc_ranks("uvw"[comp])
+                _abi.call("wf_conv", c, comp, float(alpha), self._dt_dev, s)
+            for comp in range(3):
+                self._fill_bc_ranks("uvw"[comp])
+                _abi.call("wf_diff", c, comp, float(alpha), self._dt_dev, s)
+            if stage + 1 < len(ALFARK):
+                self._calvel_ranks(alpha)
+
+        # solver.py:178-212
+        eps = cfg.numerics.div_tolerance
+        maxcy = cfg.numerics.max_outer_iters
+        self._calvel_ranks(1.0)
+        iters = 0
+        self.rmax_trace = []
+        for it in range(1, maxcy + 1):
+            iters = it
+            _abi.call("wf_calmas", c, s)
+            self.rmax = comm.allreduce(float(self._pull_scalars().rmax), op=MAX)
+            self.rmax_trace.append(self.rmax)
+            if self.rmax < eps and it > 1:
+                break
+            if self.rmax > 10.0:
+                raise RuntimeError("projection diverged: rmax = %.6e at itime %d"
+                                   % (self.rmax, self.itime))
+            self.mg.solve(self.f["su"], self.f["pp"], NPL)
+            _abi.call("wf_add_ring", self.f["p"].ptr, self.f["pp"].ptr, self.n, s)
+            self.halo.exchange(self.f["p"])
+            self.bcs.apply_pbound(self.f["p"], self.n)
+            self._calvel_ranks(1.0)
+        else:
+            if self.topo.rank == 0:
+                print("warning: projection did not converge, rmax = %.6e after %d "
+                      "iterations" % (self.rmax, maxcy), flush=True)
+        self.outer_iters = iters
+        for name in ("u", "v", "w"):
+            self._fill_bc_ranks(name)
+        sc = self._pull_scalars()
+        sc.rmax, sc.iters, sc.status = self.rmax, iters, _abi.ST_OK
+        self._sc.copy_(self._sc_host, non_blocking=True)
+        torch.cuda.current_stream(self.device).synchronize()
+        return {"ctime": self._ctime, "dt": self._dt, "rmax": self.rmax,
+                "iters": self.outer_iters, "cfl": self.cfl}
+
     def launch_step(self):
         """Enqueue one step on the current stream without waiting."""
+        if self.ranks:
+            raise RuntimeError("a sub-domain steps through step() (its halo exchanges "
+                               "and allreduces need the host)")
         _abi.call("wf_stepper_step", self._stepper, self._stream())
 
     def launch_counts(self):
