@@ -48,11 +48,11 @@ def test_step_matches_reference_golden(tag, mode):
 
 
 def test_serial_stepper_bit_identical():
-    """A stepper built without programmatic dependent launch (the form
-    ensembles and the server use) computes exactly the same step."""
+    """A stepper built without programmatic dependent launch (the default)
+    and one built with it compute exactly the same step."""
     from warpflow import FlowSolver, build_topology
     cfg = make_cfg(24, levels=3)
-    a = _solver(cfg)
+    a = FlowSolver(cfg, build_topology(cfg), "cuda:0", serial=False)
     b = FlowSolver(cfg, build_topology(cfg), "cuda:0", serial=True)
     for _ in range(3):
         ra, rb = a.step(), b.step()

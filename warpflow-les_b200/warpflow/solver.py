@@ -40,11 +40,16 @@ STEP_SERIAL = 2   # WF_STEP_SERIAL: no programmatic dependent launch
 
 
 class FlowSolver:
-    def __init__(self, cfg, topo, device, step_mode=None, serial=False):
-        """`serial=True` builds the step without programmatic dependent
-        launch (each kernel's CTAs wait for the previous kernel to finish
-        before becoming resident); use it when many solvers step
-        concurrently on one GPU."""
+    def __init__(self, cfg, topo, device, step_mode=None, serial=True):
+        """`serial` (the default) builds the step without programmatic
+        dependent launch: each kernel's CTAs become resident only after the
+        previous kernel finished.  Measured on B200 the single-case step
+        graph is about 1.3 % faster that way at 80^3 (1.008 against 1.024 ms
+        and 1.019 against 1.031 ms in two runs; 256^3 and 512^3 unchanged),
+        and many solvers stepping concurrently need it (waiting CTAs would
+        hold SMs other streams could use).  `serial=False` launches the
+        step's kernels with programmatic dependent launch; the results are
+        the same bits."""
         self.cfg = cfg
         self.topo = topo
         dev = cuda_device(device)
