@@ -58,3 +58,38 @@ def test_decomposed_solver_matches_reference(tag):
             worst = max(worst, d)
             assert d <= 1e-10, (tag, r, key, d)
     print("%s: %d ranks, max |gpu - reference| = %.3e" % (tag, nr, worst))
+
+
+def test_cli_decomposed_under_torchrun(tmp_path):
+    """run.py under torchrun at 2 ranks (halos through gloo, both ranks on
+    cuda:0): the reference's log lines from rank 0, one snapshot per rank,
+    and each rank's final fields equal to the reference's decomposed run."""
+    import socket
+    import subprocess
+    import sys
+
+    from conftest import PKG
+    g = np.load(os.path.join(GOLDEN, "golden_r2x_16x8x8_l3.npz"))
+    raw = yaml.safe_load(str(g["case_yaml"]))
+    raw["output"]["outdir"] = str(tmp_path / "out")
+    case = tmp_path / "case.yaml"
+    case.write_text(yaml.safe_dump(raw))
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    env = dict(os.environ, WF_DIST_BACKEND="gloo")
+    r = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+                        "--nproc-per-node", "2", "--master-addr", "127.0.0.1",
+                        "--master-port", str(port), os.path.join(PKG, "run.py"),
+                        "--case", str(case)],
+                       capture_output=True, text=True, timeout=600, env=env)
+    assert r.returncode == 0, r.stderr[-3000:]
+    its = [l for l in r.stdout.splitlines() if l.startswith("it ")]
+    assert len(its) == 2, r.stdout
+    assert "domains=[2, 1, 1]" in r.stdout
+    for rank in range(2):
+        z = np.load(tmp_path / "out" / ("snap_000002_r%03d.npz" % rank))
+        for name in ("u", "v", "w", "p"):
+            d = float(np.abs(z[name] - g["r%d_s2_%s" % (rank, name)]).max())
+            assert d <= 1e-10, (rank, name, d)
+        assert tuple(z["offsets"]) == (8 * rank, 0, 0)

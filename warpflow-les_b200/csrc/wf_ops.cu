@@ -451,12 +451,10 @@ __global__ void __launch_bounds__(TPB) k_conv(const wf_case c, Geo g, double alp
   const double* oo = bt_fld(c, bt, WF_UOO + COMP);
   double* star = bt_fld(c, bt, WF_USTAR + COMP);
   if (bt.tab) dtp = &bt_sc(c, bt)->dt;
-  const double dx = c.dx, dy = c.dy, dz = c.dz;
   const double dt = *dtp;
   const long X = g.sI, Y = g.sJ, Z = 1;
   int ni, nj, nk;
   op_dims(COMP, g.n, ni, nj, nk);
-  const long tot = (long)ni * nj * nk;
   // one thread per (j, k) column and `planes` consecutive planes i: x = k,
   // y = j (the CTA's shape and the planes are chosen per size, 32 x 8 x 1 by
   // default), z = group of planes.  A CTA that walks through several planes

@@ -15,6 +15,8 @@ per rank under torchrun, where the reference runs under mpirun:
 
 Each rank joins the process group (NCCL between GPUs) on GPU LOCAL_RANK
 and writes its own snapshot files (snap_<itime>_r<rank>.npz).
+WF_DIST_BACKEND=gloo moves the halos through host memory instead, and
+then ranks may share a GPU (LOCAL_RANK modulo the GPU count).
 """
 import argparse
 import os
@@ -39,10 +41,15 @@ def _join_ranks(cfg):
     import torch
     import torch.distributed as dist
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    backend = os.environ.get("WF_DIST_BACKEND", "nccl")
+    if backend not in ("nccl", "gloo"):
+        raise ValueError("WF_DIST_BACKEND must be nccl or gloo")
+    if backend == "gloo":
+        local %= max(1, torch.cuda.device_count())
     if not dist.is_initialized():
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+        kw = {"device_id": torch.device("cuda", local)} if backend == "nccl" else {}
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300), **kw)
     return "cuda:%d" % local
 
 
