@@ -258,6 +258,20 @@ WF_API int wf_mg_residual_max(const wf_case* c, const double* phi0, const double
 /* bcs.py:326-360 _mk_neumann on all six faces of a level-0 pair. */
 WF_API int wf_mg_refill(const wf_case* c, double* phi0, void* stream);
 
+/* No counterpart in the reference (its fills are ordered face launches,
+ * bcs.py:201-323).  The composed one-launch program of a ghost fill, for
+ * checking on the host: kind 0 u, 1 v, 2 w, 3 vis, 4 pbound, 5 the initial p
+ * mirror; 4 <= n <= 256.  Entries are (dst, code) pairs of offsets into the
+ * padded (n+6)^3 field: code bit 0 set = a constant (bits 2.. : 0 for 0.0,
+ * 1 for the fill's value), else bits 2.. = the source offset; bit 1 set =
+ * negated.  The first nsimple entries are independent gathers; the rest are
+ * ngroup groups (entries gstart[g] .. gstart[g+1]-1 after the simple ones),
+ * each applied by one thread that reads every source before it writes.
+ * Sources always hold the values from before the fill.  Call with null ent
+ * and gstart to get the counts (2 * nent ints, ngroup + 1 ints). */
+WF_API int wf_fill_program(int32_t kind, int32_t n, int32_t* nsimple, int32_t* ngroup,
+                           int64_t* nent, int32_t* ent, int32_t* gstart);
+
 /* ---- sub-domains (more than one rank per case) --------------------------
  * The reference decomposes a case over MPI ranks (topology.py:30-53): each
  * rank steps its own cube of cells, and halo.py:59-130 HaloExchanger.exchange

@@ -7,6 +7,15 @@
 // ordered phases -- x faces, y faces, z faces -- and each phase runs as one
 // launch in which a thread owns one (a, b) line of every face op of that
 // phase and walks its layers in order.  Up to three fields share a launch.
+#include <algorithm>
+#include <cstdlib>
+#include <functional>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <unordered_map>
+#include <vector>
+
 #include "wf_dev.cuh"
 #include "wf_internal.h"
 
@@ -231,9 +240,285 @@ static int program(int kind, int n, double val, const double* valp, int phase, F
   return k;
 }
 
+
+// ---- one-launch fills -------------------------------------------------------
+// The ordered face ops of a fill only copy (times +-1) and set constants, so
+// every cell a fill writes ends as s * old(x) -- the value some cell x held
+// before the fill -- or s * K, K = 0 or the fill's value, s = +-1.  The host
+// composes the ops in the reference's order once per (fill kind, n) and the
+// fill then runs as ONE launch of independent gathers instead of three
+// ordered phases whose threads walk their layers load by load.  Where a
+// written cell's final value needs the old value of a cell that the same
+// fill also overwrites, both cells (and any others chained to them) go to
+// one thread, which loads every value it needs before it stores any: a
+// "group".  Every other written cell is one thread's single gather.  The
+// products by +-1 are exact, so the result is the phases' bit for bit.
+//
+// Table entries are (dst, code): dst the cell's offset in the field; code
+// bit 0 set: a constant (bits 2.. = 0 for 0.0, 1 for the fill's value),
+// else bits 2.. = the source offset; bit 1 set: negate.
+constexpr int ONE_GMAX = 16;        // cells of one group
+constexpr int ONE_NMAX = 256;       // largest n served by one-launch fills
+
+struct OneProg {
+  const int2* ent = nullptr;   // nsimple entries, then the groups' entries
+  const int* gstart = nullptr; // ngroup + 1 offsets into ent (from nsimple)
+  int nsimple = 0, ngroup = 0;
+};
+
+struct OneJob {
+  double* fld;
+  int fid, vsrc;
+  double val;
+  const double* valp;
+  OneProg prog;
+};
+
+struct OneArgs {
+  OneJob job[MAX_JOBS];
+  int njob;
+};
+
+__device__ __forceinline__ double one_value(const double* f, int code, double K) {
+  const double v = (code & 1) ? ((code >> 2) ? K : 0.0) : f[code >> 2];
+  return (code & 2) ? -v : v;
+}
+
+__global__ void k_fill_one(const OneArgs args, const Batch bt) {
+  pdl_entry();
+  if (bt_skip(bt)) return;
+  const int jb = bt_z(bt);
+  if (jb >= args.njob) return;
+  const OneJob& J = args.job[jb];
+  double* f = J.fld;
+  const double* valp = J.valp;
+  if (bt.tab) {
+    const CasePtrs& cp = bt.tab[bt_case(bt)];
+    f = cp.fld[J.fid];
+    if (J.vsrc) valp = J.vsrc == 1 ? &cp.sc->ulid : &cp.sc->rrey;
+  }
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const double K = valp ? *valp : J.val;
+  if (t < J.prog.nsimple) {
+    const int2 e = J.prog.ent[t];
+    f[e.x] = one_value(f, e.y, K);
+    return;
+  }
+  const int g = t - J.prog.nsimple;
+  if (g >= J.prog.ngroup) return;
+  const int a = J.prog.nsimple + J.prog.gstart[g], b = J.prog.nsimple + J.prog.gstart[g + 1];
+  double v[ONE_GMAX];
+#pragma unroll
+  for (int q = 0; q < ONE_GMAX; ++q)
+    if (a + q < b) v[q] = one_value(f, J.prog.ent[a + q].y, K);
+#pragma unroll
+  for (int q = 0; q < ONE_GMAX; ++q)
+    if (a + q < b) f[J.prog.ent[a + q].x] = v[q];
+}
+
+// compose the fill's ops (reference order) into its one-launch program;
+// false when a group would exceed ONE_GMAX cells
+static bool one_build(int kind, int n, std::vector<int2>& ent, std::vector<int>& gstart,
+                      int& nsimple) {
+  const long P = n + 2 * NPL;
+  // expression of every written cell: (source offset or constant id, const, negate)
+  struct Ex { long ref; bool cst, neg; };
+  std::unordered_map<long, Ex> ex;
+  ex.reserve((size_t)6 * NPL * P * P);
+  auto cur = [&](long c) -> Ex {
+    auto it = ex.find(c);
+    return it == ex.end() ? Ex{c, false, false} : it->second;
+  };
+  std::vector<long> order;   // written cells, first write order
+  for (int phase = 0; phase < 3; ++phase) {
+    FaceOp ops[MAX_OPS_PER_PHASE];
+    const int nops = program(kind, n, 1.0, nullptr, phase, ops);
+    for (int o = 0; o < nops; ++o) {
+      const FaceOp& op = ops[o];
+      for (int a = 0; a < op.na; ++a)
+        for (int b = 0; b < op.nb; ++b)
+          for (int m = 0; m < op.nlay; ++m) {
+            const long pa = op.a0 + a, pb = op.b0 + b;
+            const long gidx = op.high ? op.g0 + m : op.g0 - m;
+            auto at = [&](long x) {
+              return op.axis == 0 ? (x * P + pa) * P + pb
+                                  : (op.axis == 1 ? (pa * P + x) * P + pb : (pa * P + pb) * P + x);
+            };
+            const long dst = at(gidx);
+            Ex e;
+            if (op.lin) {
+              e = cur(at(op.high ? op.s0 - m : op.s0 + m));
+              if (op.val < 0) e.neg = !e.neg;
+            } else {
+              // a constant op writes 0.0 or the fill's value (ulid, 1/Re),
+              // which program() was given as 1.0 here
+              e = Ex{op.val == 0.0 ? 0 : 1, true, false};
+            }
+            if (!ex.count(dst)) order.push_back(dst);
+            ex[dst] = e;
+          }
+    }
+  }
+  // union-find over written cells: a cell whose value is the old value of
+  // another written cell goes with it
+  std::unordered_map<long, long> parent;
+  parent.reserve(order.size());
+  std::function<long(long)> find = [&](long x) {
+    long r = x;
+    while (parent[r] != r) r = parent[r];
+    while (parent[x] != r) {
+      const long nx = parent[x];
+      parent[x] = r;
+      x = nx;
+    }
+    return r;
+  };
+  for (long c : order) parent[c] = c;
+  for (long c : order) {
+    const Ex& e = ex[c];
+    if (!e.cst && e.ref != c && ex.count(e.ref)) {
+      const long ra = find(c), rb = find(e.ref);
+      if (ra != rb) parent[ra] = rb;
+    }
+  }
+  std::unordered_map<long, std::vector<long>> comp;
+  for (long c : order) {
+    const Ex& e = ex[c];
+    if (!e.cst && e.ref == c && !e.neg) continue;   // unchanged: nothing to write
+    comp[find(c)].push_back(c);
+  }
+  auto code = [&](const Ex& e) {
+    return (int)((e.ref << 2) | (e.neg ? 2 : 0) | (e.cst ? 1 : 0));
+  };
+  std::vector<int2> simple;
+  std::vector<std::vector<long>> groups;
+  for (auto& kv : comp) {
+    if (kv.second.size() == 1) {
+      const long c = kv.second[0];
+      simple.push_back(make_int2((int)c, code(ex[c])));
+    } else {
+      if (kv.second.size() > (size_t)ONE_GMAX) return false;
+      groups.push_back(kv.second);
+    }
+  }
+  std::sort(simple.begin(), simple.end(), [](const int2& p, const int2& q) { return p.x < q.x; });
+  std::sort(groups.begin(), groups.end());
+  ent = simple;
+  nsimple = (int)simple.size();
+  gstart.assign(1, 0);
+  for (auto& gr : groups) {
+    std::sort(gr.begin(), gr.end());
+    for (long c : gr) ent.push_back(make_int2((int)c, code(ex[c])));
+    gstart.push_back((int)(ent.size() - nsimple));
+  }
+  return true;
+}
+
+// the device program of (kind, n) on the current device, built on first use;
+// null while the stream is being captured and it does not exist yet (the
+// phased fill then runs), or for sizes above ONE_NMAX
+static const OneProg* one_prog(int kind, int n, cudaStream_t s) {
+  static int on = -1;
+  if (on < 0) {
+    const char* e = getenv("WF_FILL1");
+    on = (e && e[0] == '0') ? 0 : 1;
+  }
+  if (n > ONE_NMAX || !on) return nullptr;
+  static std::mutex mu;
+  static std::map<std::tuple<int, int, int>, OneProg*> progs;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  const auto key = std::make_tuple(dev, kind, n);
+  auto it = progs.find(key);
+  if (it != progs.end()) return it->second;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (s && cudaStreamIsCapturing(s, &cs) != cudaSuccess) return nullptr;
+  if (cs != cudaStreamCaptureStatusNone) return nullptr;
+  std::vector<int2> ent;
+  std::vector<int> gstart;
+  int nsimple = 0;
+  OneProg* p = new OneProg();
+  if (one_build(kind, n, ent, gstart, nsimple)) {
+    int2* de = nullptr;
+    int* dg = nullptr;
+    if (cudaMalloc(&de, ent.size() * sizeof(int2)) != cudaSuccess ||
+        cudaMalloc(&dg, gstart.size() * sizeof(int)) != cudaSuccess ||
+        cudaMemcpy(de, ent.data(), ent.size() * sizeof(int2), cudaMemcpyHostToDevice) !=
+            cudaSuccess ||
+        cudaMemcpy(dg, gstart.data(), gstart.size() * sizeof(int), cudaMemcpyHostToDevice) !=
+            cudaSuccess) {
+      cudaGetLastError();
+      delete p;
+      return nullptr;
+    }
+    p->ent = de;
+    p->gstart = dg;
+    p->nsimple = nsimple;
+    p->ngroup = (int)gstart.size() - 1;
+  }
+  progs[key] = p->ent ? p : nullptr;
+  if (!p->ent) delete p;
+  return progs[key];
+}
+
+int fill_program(int kind, int n, int32_t* nsimple, int32_t* ngroup, int64_t* nent,
+                 int32_t* ent, int32_t* gstart) {
+  if (kind < FILL_U || kind > FILL_PMIRROR) return fail(WF_EINVAL, "fill kind out of range");
+  if (n < 4 || n > ONE_NMAX) return fail(WF_EINVAL, "fill program: n in 4..256");
+  std::vector<int2> e;
+  std::vector<int> g;
+  int ns = 0;
+  if (!one_build(kind, n, e, g, ns)) return fail(WF_EUNSUPPORTED, "fill program: group too large");
+  *nsimple = ns;
+  *ngroup = (int32_t)g.size() - 1;
+  *nent = (int64_t)e.size();
+  if (ent)
+    for (size_t q = 0; q < e.size(); ++q) {
+      ent[2 * q] = e[q].x;
+      ent[2 * q + 1] = e[q].y;
+    }
+  if (gstart)
+    for (size_t q = 0; q < g.size(); ++q) gstart[q] = g[q];
+  return WF_OK;
+}
+
+int prepare_fills(int n) {
+  for (int kind = FILL_U; kind <= FILL_PMIRROR; ++kind) one_prog(kind, n, nullptr);
+  return WF_OK;
+}
+
+// the one-launch form of launch_fills; false when a job has no program
+static bool launch_fills_one(const FillReq* reqs, int nreq, int n, cudaStream_t s, int* rc) {
+  OneArgs a{};
+  a.njob = nreq;
+  int maxthreads = 0;
+  for (int r = 0; r < nreq; ++r) {
+    const OneProg* p = one_prog(reqs[r].kind, n, s);
+    if (!p) return false;
+    a.job[r] = OneJob{reqs[r].fld, reqs[r].fid, reqs[r].vsrc, reqs[r].val, reqs[r].valp, *p};
+    maxthreads = std::max(maxthreads, p->nsimple + p->ngroup);
+  }
+  *rc = WF_OK;
+  cudaError_t e = launch_k(k_fill_one, dim3((maxthreads + 255) / 256, 1, nreq), dim3(256), 0, s, a);
+  ++g_launches;
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) *rc = cuda_fail(e, "k_fill_one");
+  return true;
+}
+
 int launch_fills(const FillReq* reqs, int nreq, int n, cudaStream_t s) {
   if (nreq < 1 || nreq > MAX_JOBS) return fail(WF_EINVAL, "launch_fills: 1..3 fields");
   if (n < 4) return fail(WF_EINVAL, "ghost fills need n >= 4");
+  for (int r = 0; r < nreq; ++r) {
+    if (!reqs[r].fld) return fail(WF_EINVAL, "launch_fills: null field");
+    if (batch_ctx().tab && reqs[r].fid < 0)
+      return fail(WF_EUNSUPPORTED, "launch_fills: a bucket fill needs field slots");
+  }
+  {
+    int rc = WF_OK;
+    if (launch_fills_one(reqs, nreq, n, s, &rc)) return rc;
+  }
   for (int phase = 0; phase < 3; ++phase) {
     PhaseArgs a{};
     a.njob = nreq;

@@ -136,8 +136,13 @@ struct FillReq {
   int fid = -1;             // the field's slot (enum wf_field), for bucket launches
   int vsrc = 0;             // valp in the scalar block: 1 ulid, 2 rrey (bucket launches)
 };
-// up to 3 independent field fills, executed as 3 ordered axis phases
+// up to 3 independent field fills: one launch of the composed fill program
+// (sizes up to 256), else 3 ordered axis phases
 int launch_fills(const FillReq* reqs, int nreq, int n, cudaStream_t s);
+// build the composed fill programs of size n now (outside any stream capture)
+int prepare_fills(int n);
+int fill_program(int kind, int n, int32_t* nsimple, int32_t* ngroup, int64_t* nent,
+                 int32_t* ent, int32_t* gstart);
 
 // ---- operators -----------------------------------------------------------
 int launch_init_noise(double* u, double* v, double* w, int n, double amp,

@@ -500,6 +500,11 @@ int wf_mg_build_coarse_op(const wf_case* c, void* s) {
   return build_coarse_op_case(*c, (cudaStream_t)s);
 }
 
+int wf_fill_program(int32_t kind, int32_t n, int32_t* nsimple, int32_t* ngroup, int64_t* nent,
+                    int32_t* ent, int32_t* gstart) {
+  if (!nsimple || !ngroup || !nent) return fail(WF_EINVAL, "null argument");
+  return fill_program(kind, n, nsimple, ngroup, nent, ent, gstart);
+}
 int wf_box_copy(double* arr, int64_t sI, int64_t sJ, int32_t i0, int32_t j0, int32_t k0,
                 int32_t ni, int32_t nj, int32_t nk, double* buf, int32_t unpack, void* s) {
   return launch_box(arr, sI, sJ, i0, j0, k0, ni, nj, nk, buf, unpack ? 1 : 0, (cudaStream_t)s);
@@ -532,6 +537,7 @@ int wf_stepper_create(const wf_case* c, int32_t mode, wf_stepper** out) {
   WF_TRY(validate_case(*c));
   if (mode & ~(1 | WF_STEP_SERIAL))
     return fail(WF_EINVAL, "mode must be 0 (graph) or 1 (host loop), optionally | WF_STEP_SERIAL");
+  prepare_fills(c->n);   // the fill programs are built outside the capture
   wf_stepper* st = new wf_stepper();
   st->c = *c;
   st->mode = mode & 1;
@@ -594,6 +600,7 @@ int wf_ensemble_create(const wf_case* cases, int32_t ncases, int32_t mode, wf_en
   if (mode & ~(WF_STEP_SERIAL | WF_ENS_BUCKETS))
     return fail(WF_EINVAL, "ensemble mode: 0, WF_STEP_SERIAL and/or WF_ENS_BUCKETS");
   for (int i = 0; i < ncases; ++i) WF_TRY(validate_case(cases[i]));
+  for (int i = 0; i < ncases; ++i) prepare_fills(cases[i].n);
   PdlOff guard((mode & WF_STEP_SERIAL) != 0);
   wf_ensemble* en = new wf_ensemble();
   en->ncases = ncases;

@@ -129,6 +129,8 @@ SIGNATURES = {
     "wf_box_copy": (_I32, [_VP, _I64, _I64, _I32, _I32, _I32, _I32, _I32, _I32, _VP, _I32,
                            _VP]),
     "wf_copy_oo": (_I32, [_CP, _VP]),
+    "wf_fill_program": (_I32, [_I32, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_I32),
+                               ctypes.POINTER(_I64), _VP, _VP]),
     "wf_rk_mg_op": (_I32, [_CP, _I32, _I32, _I32, _I32, _VP]),
     "wf_rk_level_view": (_I32, [_CP, _I32, ctypes.POINTER(_VP), ctypes.POINTER(_I64),
                                 ctypes.POINTER(_I64), ctypes.POINTER(_I32)]),
