@@ -415,11 +415,11 @@ __device__ __forceinline__ double diff_add(double star, double dt, double alpha,
 // vis * lap4(f) at cell id of component COMP (kernels.py:189-225); f the
 // component, vis the viscosity field
 template <int COMP>
-__device__ __forceinline__ double diff_term(const double* f, const double* vis, const Geo& g,
-                                            const Divs& dv, long id) {
-  const long vofs = COMP == 0 ? 0 : (COMP == 1 ? g.sJ : 1);
-  const double l4 = lap1(f, id, g.sI, dv.d12[0], dv.y12[0]) +
-                    lap1(f, id, g.sJ, dv.d12[1], dv.y12[1]) + lap1(f, id, 1, dv.d12[2], dv.y12[2]);
+__device__ __forceinline__ double diff_term(const double* f, const double* vis, long sI,
+                                            long sJ, const Divs& dv, long id) {
+  const long vofs = COMP == 0 ? 0 : (COMP == 1 ? sJ : 1);
+  const double l4 = lap1(f, id, sI, dv.d12[0], dv.y12[0]) +
+                    lap1(f, id, sJ, dv.d12[1], dv.y12[1]) + lap1(f, id, 1, dv.d12[2], dv.y12[2]);
   return LD(vis, id + vofs) * l4;
 }
 
@@ -430,9 +430,13 @@ __device__ __forceinline__ void diff_cell(const wf_case& c, const Geo& g, double
   double* star = c.fld[WF_USTAR + COMP];
   const long id = g.at(NPL + i0, NPL + j0, NPL + k0);
   star[id] = diff_add(star[id], dt, alpha,
-                      diff_term<COMP>(c.fld[WF_U + COMP], c.fld[WF_VIS], g, dv, id));
+                      diff_term<COMP>(c.fld[WF_U + COMP], c.fld[WF_VIS], g.sI, g.sJ, dv, id));
 }
 
+// PC: the padded extent n + 6 as a compile-time constant for the common
+// sizes (0: read from g), so that every neighbour load is one base address
+// plus an immediate offset instead of a runtime 64-bit address sum -- the
+// pass is instruction-bound; the arithmetic is the same.
 // DIFF: also add the component's diffusion to star in the same pass.  The
 // step's fill of the component between its convection and its diffusion
 // (solver.py:253-263) changes only ghost cells that lie outside the grid in
@@ -440,7 +444,7 @@ __device__ __forceinline__ void diff_cell(const wf_case& c, const Geo& g, double
 // cells, which do not change in between -- and the diffusion stencil never
 // reaches such cells, so the fused update reads the same values and gives
 // the same star.
-template <int COMP, bool DIFF>
+template <int COMP, bool DIFF, int PC>
 __global__ void __launch_bounds__(TPB) k_conv(const wf_case c, Geo g, double alpha,
                                              const double* dtp, const Divs dv, int planes,
                                              const Batch bt) {
@@ -452,9 +456,9 @@ __global__ void __launch_bounds__(TPB) k_conv(const wf_case c, Geo g, double alp
   double* star = bt_fld(c, bt, WF_USTAR + COMP);
   if (bt.tab) dtp = &bt_sc(c, bt)->dt;
   const double dt = *dtp;
-  const long X = g.sI, Y = g.sJ, Z = 1;
+  const long X = PC ? (long)PC * PC : g.sI, Y = PC ? (long)PC : g.sJ, Z = 1;
   int ni, nj, nk;
-  op_dims(COMP, g.n, ni, nj, nk);
+  op_dims(COMP, PC ? PC - 2 * NPL : g.n, ni, nj, nk);
   // one thread per (j, k) column and `planes` consecutive planes i: x = k,
   // y = j (the CTA's shape and the planes are chosen per size, 32 x 8 x 1 by
   // default), z = group of planes.  A CTA that walks through several planes
@@ -468,7 +472,7 @@ __global__ void __launch_bounds__(TPB) k_conv(const wf_case c, Geo g, double alp
 #pragma unroll 1
   for (int ii = bt_z(bt) * planes; ii < i_end; ++ii) {
     const int i = NPL + ii;
-    const long id = g.at(i, j, k);
+    const long id = (long)i * X + (long)j * Y + k;
     double tot3;
     if (COMP == 0) {
       double a;
@@ -528,7 +532,7 @@ __global__ void __launch_bounds__(TPB) k_conv(const wf_case c, Geo g, double alp
     const double s1 = LD(oo, id) - dt * alpha * tot3;
     star[id] = DIFF ? diff_add(s1, dt, alpha,
                                diff_term<COMP>(COMP == 0 ? u : (COMP == 1 ? v : w),
-                                               bt_fld(c, bt, WF_VIS), g, dv, id))
+                                               bt_fld(c, bt, WF_VIS), X, Y, dv, id))
                     : s1;
   }
 }
@@ -608,11 +612,22 @@ int launch_conv(const wf_case& c, int comp, double alpha, const double* dt,
   launch_shape(SHAPE_CONV, c.n, &bx, &by, &planes);
   const dim3 gr((nk + bx - 1) / bx, (nj + by - 1) / by, (ni + planes - 1) / planes), bl(bx, by);
   if (comp < 0 || comp > 2) return fail(WF_EINVAL, "conv: comp must be 0, 1 or 2");
-  void (*const kern[2][3])(const wf_case, Geo, double, const double*, const Divs, int,
-                           const Batch) = {
-      {k_conv<0, false>, k_conv<1, false>, k_conv<2, false>},
-      {k_conv<0, true>, k_conv<1, true>, k_conv<2, true>}};
-  WF_CK(launch_k(kern[with_diff ? 1 : 0][comp], gr, bl, 0, s, c, g, alpha, dt, divs_of(c),
+  using KC = void (*)(const wf_case, Geo, double, const double*, const Divs, int, const Batch);
+  static const KC kern[3][2][3] = {
+      {{k_conv<0, false, 0>, k_conv<1, false, 0>, k_conv<2, false, 0>},
+       {k_conv<0, true, 0>, k_conv<1, true, 0>, k_conv<2, true, 0>}},
+      {{k_conv<0, false, 86>, k_conv<1, false, 86>, k_conv<2, false, 86>},
+       {k_conv<0, true, 86>, k_conv<1, true, 86>, k_conv<2, true, 86>}},
+      {{k_conv<0, false, 262>, k_conv<1, false, 262>, k_conv<2, false, 262>},
+       {k_conv<0, true, 262>, k_conv<1, true, 262>, k_conv<2, true, 262>}}};
+  // the size-specialised forms (80^3 and 256^3); WF_CONV_PC=0 keeps the generic one
+  static int spec = -1;
+  if (spec < 0) {
+    const char* e = getenv("WF_CONV_PC");
+    spec = (e && e[0] == '0') ? 0 : 1;
+  }
+  const int form = !spec ? 0 : (c.n == 80 ? 1 : (c.n == 256 ? 2 : 0));
+  WF_CK(launch_k(kern[form][with_diff ? 1 : 0][comp], gr, bl, 0, s, c, g, alpha, dt, divs_of(c),
                  planes));
   WF_CKL("k_conv");
   return WF_OK;
