@@ -92,7 +92,7 @@ __global__ void k_scalars_init(wf_scalars* sc, double dt0, double rrey, double u
   sc->dtvisc = 0.0;
   for (int i = 0; i < 32; ++i) sc->rmax_trace[i] = 0.0;
   sc->red[0] = sc->red[1] = sc->red[2] = okey(0.0);
-  sc->red[3] = okey(1.0e10);  // solver.py:127 initialiser of the min
+  sc->red[3] = 0ull;          // rate key of k_checkdt (0: the key of +0)
   sc->red[4] = okey(0.0);
   sc->red[5] = okey(0.0);
   sc->itime = 0;
@@ -160,7 +160,17 @@ __global__ void __launch_bounds__(TPB) k_checkdt(const wf_case c, Geo g, const D
   const double* vis = bt_fld(c, bt, WF_VIS);
   const double dx = c.dx, dy = c.dy, dz = c.dz;
   const double inv2 = 1.0 / (dx * dx) + 1.0 / (dy * dy) + 1.0 / (dz * dz);
-  double mu = 0.0, mv = 0.0, mw = 0.0, mdt = 1.0e10;
+  // The reference's dtvisc is the min over cells of RN(1/x), x the cell's
+  // viscous/advective rate, initialised with 1e10 (solver.py:127).  On each
+  // side of zero the correctly rounded reciprocal falls as x grows, and
+  // every negative x gives a smaller reciprocal than every positive one, so
+  // the min is RN(1/x*) for the x* that maximises the order key of x with
+  // its top bit flipped (negatives above positives, ascending x within
+  // each sign; NaN skipped as fmin skips it): one division per step instead
+  // of one per cell, the same bits for every input.
+  double mu = 0.0, mv = 0.0, mw = 0.0;
+  unsigned long long kx = 0ull;
+  __shared__ unsigned long long skx[32];
   const int k = NPL + blockIdx.x * 32 + (threadIdx.x & 31);
   const int j = NPL + blockIdx.y * 8 + (threadIdx.x >> 5);
   const bool in = k < NPL + g.n && j < NPL + g.n;
@@ -173,31 +183,37 @@ __global__ void __launch_bounds__(TPB) k_checkdt(const wf_case c, Geo g, const D
     const double uc = 0.5 * (uu + LD(u, id - g.sI));
     const double vc = 0.5 * (vv + LD(v, id - g.sJ));
     const double wc = 0.5 * (ww + LD(w, id - 1));
-    const double val = 1.0 / (div_by_recip(fabs(uc), dv.dh[0], dv.yh[0]) +
-                              div_by_recip(fabs(vc), dv.dh[1], dv.yh[1]) +
-                              div_by_recip(fabs(wc), dv.dh[2], dv.yh[2]) +
-                              2.0 * LD(vis, id) * inv2 + 1.0e-30);
-    mdt = fmin(mdt, val);
+    const double x = div_by_recip(fabs(uc), dv.dh[0], dv.yh[0]) +
+                     div_by_recip(fabs(vc), dv.dh[1], dv.yh[1]) +
+                     div_by_recip(fabs(wc), dv.dh[2], dv.yh[2]) + 2.0 * LD(vis, id) * inv2 +
+                     1.0e-30;
+    if (x == x) kx = max(kx, okey(x) ^ 0x8000000000000000ull);
   }
   mu = block_max(mu, sm);
   mv = block_max(mv, sm);
   mw = block_max(mw, sm);
-  mdt = block_min(mdt, sm, 1.0e10);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) kx = max(kx, __shfl_xor_sync(0xffffffffu, kx, o));
+  if ((threadIdx.x & 31) == 0) skx[threadIdx.x >> 5] = kx;
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int q = 1; q < (int)((blockDim.x + 31) >> 5); ++q) kx = max(kx, skx[q]);
   wf_scalars* sc = bt_sc(c, bt);
   if (threadIdx.x == 0) {
     atomicMax(&sc->red[0], okey(mu));
     atomicMax(&sc->red[1], okey(mv));
     atomicMax(&sc->red[2], okey(mw));
-    atomicMin(&sc->red[3], okey(mdt));
+    atomicMax(&sc->red[3], kx);
   }
   if (!last_block(&sc->ticket, gridDim.x * gridDim.y * bt_gz(bt))) return;
   if (threadIdx.x != 0) return;
   const double umax = okey_inv(atomicAdd(&sc->red[0], 0ull));
   const double vmax = okey_inv(atomicAdd(&sc->red[1], 0ull));
   const double wmax = okey_inv(atomicAdd(&sc->red[2], 0ull));
-  const double dtvisc = okey_inv(atomicAdd(&sc->red[3], 0ull));
+  const double dtvisc =
+      fmin(1.0e10, 1.0 / okey_inv(atomicAdd(&sc->red[3], 0ull) ^ 0x8000000000000000ull));
   sc->red[0] = sc->red[1] = sc->red[2] = okey(0.0);
-  sc->red[3] = okey(1.0e10);
+  sc->red[3] = 0ull;
   const double big = 1.0e10;
   double dtcfl = big;
   if (umax > 0.0) dtcfl = fmin(dtcfl, dx / umax);
