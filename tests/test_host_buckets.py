@@ -67,14 +67,19 @@ def test_launch_shapes_set_validate_and_cache(tmp_path):
     """Launch-shape table (host only): defaults, accepted and rejected
     shapes, reset, and the JSON cache."""
     from warpflow import autotune
-    assert autotune.shape("conv", 80) == (32, 8, 1)
-    assert autotune.shape("split", 80) == (2, 8, 1)
+    # built-in shapes by size (the tuner's measurements on B200)
+    assert autotune.shape("conv", 80) == (32, 4, 2)
+    assert autotune.shape("conv", 48) == (32, 8, 1)
+    assert autotune.shape("conv", 256) == (32, 4, 4)
+    assert autotune.shape("split", 80) == (4, 8, 1)
+    assert autotune.shape("split", 128) == (2, 8, 1)
+    assert autotune.shape("split", 256) == (4, 2, 1)
     try:
         autotune.set_shape("conv", 80, 16, 16, 4)
         autotune.set_shape("split", 80, 4, 2)
         assert autotune.shape("conv", 80) == (16, 16, 4)
         assert autotune.shape("split", 80) == (4, 2, 1)
-        assert autotune.shape("conv", 96) == (32, 8, 1)      # per size
+        assert autotune.shape("conv", 96) == (32, 4, 2)      # per size
         for kind, a, b, c in (("conv", 24, 8, 1), ("conv", 32, 16, 1), ("conv", 16, 1, 1),
                               ("conv", 32, 8, 0), ("conv", 32, 8, 17),
                               ("split", 3, 8, 1), ("split", 2, 16, 1), ("split", 2, 8, 2)):
@@ -89,4 +94,4 @@ def test_launch_shapes_set_validate_and_cache(tmp_path):
     finally:
         autotune.set_shape("conv", 80, 0, 0, 0)
         autotune.set_shape("split", 80, 0, 0, 0)
-    assert autotune.shape("conv", 80) == (32, 8, 1)
+    assert autotune.shape("conv", 80) == (32, 4, 2)

@@ -573,26 +573,34 @@ __global__ void __launch_bounds__(TPB) k_diff(const wf_case c, Geo g, double alp
 static constexpr int SHAPE_MAX_N = 1024;
 static int g_shape[2][SHAPE_MAX_N + 1][3];
 
-static int split_cpt_default() {
-  static int v = -1;
-  if (v < 0) {
+// built-in shapes by size, from the tuner's measurements on B200 (80^3,
+// 128^3, 256^3): the convection pass walks more planes per thread as the
+// grid grows (neighbours across i found in L1), and the split half-sweep of
+// large levels takes 4 cells per thread in CTAs of 2 rows
+// (us per pass / half-sweep, default -> tuned: conv 39.5 -> 35.8 at 80,
+// 145.6 -> 131.2 at 128, 1019 -> 855 at 256; split 3.57 -> 3.29 at 80,
+// 51.7 -> 41.5 at 256)
+static void shape_default(int kind, int n, int* a, int* b, int* c) {
+  if (kind == SHAPE_CONV) {
+    *a = 32;
+    *b = n >= 64 ? 4 : 8;
+    *c = n >= 192 ? 4 : (n >= 64 ? 2 : 1);
+  } else {
     const char* e = getenv("WF_SPLIT_CPT");
-    v = e ? atoi(e) : 2;
-    if (v != 1 && v != 2 && v != 4) v = 2;
+    const int forced = e ? atoi(e) : 0;
+    *a = (forced == 1 || forced == 2 || forced == 4) ? forced : (n >= 192 || n < 100 ? 4 : 2);
+    *b = n >= 192 ? 2 : 8;
+    *c = 1;
   }
-  return v;
 }
 
 void launch_shape(int kind, int n, int* a, int* b, int* c) {
   const bool set = kind >= 0 && kind <= 1 && n >= 0 && n <= SHAPE_MAX_N && g_shape[kind][n][0];
-  if (kind == SHAPE_CONV) {
-    *a = set ? g_shape[kind][n][0] : 32;
-    *b = set ? g_shape[kind][n][1] : 8;
-    *c = set ? g_shape[kind][n][2] : 1;
-  } else {
-    *a = set ? g_shape[kind][n][0] : split_cpt_default();
-    *b = set ? g_shape[kind][n][1] : 8;
-    *c = 1;
+  shape_default(kind, n, a, b, c);
+  if (set) {
+    *a = g_shape[kind][n][0];
+    *b = g_shape[kind][n][1];
+    *c = kind == SHAPE_CONV ? g_shape[kind][n][2] : 1;
   }
 }
 
