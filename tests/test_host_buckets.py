@@ -82,7 +82,8 @@ def test_launch_shapes_set_validate_and_cache(tmp_path):
         assert autotune.shape("conv", 96) == (32, 4, 2)      # per size
         for kind, a, b, c in (("conv", 24, 8, 1), ("conv", 32, 16, 1), ("conv", 16, 1, 1),
                               ("conv", 32, 8, 0), ("conv", 32, 8, 17),
-                              ("split", 3, 8, 1), ("split", 2, 16, 1), ("split", 2, 8, 2)):
+                              ("split", 3, 8, 1), ("split", 16, 8, 1), ("split", 2, 16, 1),
+                              ("split", 2, 8, 2)):
             with pytest.raises(RuntimeError):
                 autotune.set_shape(kind, 80, a, b, c)
         p = tmp_path / "tune.json"

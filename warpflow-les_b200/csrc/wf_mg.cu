@@ -1831,10 +1831,13 @@ static int split_sweeps(const Lvl<T>& L, int nsweeps, cudaStream_t s) {
   T* sp = L.tmp;
   const T* sr = L.tmp + (long)m * m * m;
   int cpt, rows, one;
-  launch_shape(SHAPE_SPLIT, L.n, &cpt, &rows, &one);   // cpt in {1, 2, 4}, rows <= SPLIT_ROWS
+  launch_shape(SHAPE_SPLIT, L.n, &cpt, &rows, &one);   // cpt in {1, 2, 4, 8}, rows <= SPLIT_ROWS
   const dim3 grid((L.n / 2 + 32 * cpt - 1) / (32 * cpt), (L.n + rows - 1) / rows, L.n);
   const ApRecip<T> rt = ap_recip(L);
-  auto kern = cpt == 4 ? k_rbgs_split<T, 4> : cpt == 2 ? k_rbgs_split<T, 2> : k_rbgs_split<T, 1>;
+  auto kern = cpt == 8   ? k_rbgs_split<T, 8>
+              : cpt == 4 ? k_rbgs_split<T, 4>
+              : cpt == 2 ? k_rbgs_split<T, 2>
+                         : k_rbgs_split<T, 1>;
   for (int it = 0; it < nsweeps; ++it) {
     for (int color = 0; color < 2; ++color) {
       WF_CK(launch_k(kern, grid, dim3(32, rows), 0, s, L, sp, sr, color, rt));

@@ -588,7 +588,8 @@ static void shape_default(int kind, int n, int* a, int* b, int* c) {
   } else {
     const char* e = getenv("WF_SPLIT_CPT");
     const int forced = e ? atoi(e) : 0;
-    *a = (forced == 1 || forced == 2 || forced == 4) ? forced : (n >= 192 || n < 100 ? 4 : 2);
+    *a = (forced == 1 || forced == 2 || forced == 4 || forced == 8) ? forced
+                                                                    : (n >= 192 || n < 100 ? 4 : 2);
     *b = n >= 192 ? 2 : 8;
     *c = 1;
   }
@@ -618,8 +619,10 @@ int set_launch_shape(int kind, int n, int a, int b, int c) {
         c > 16)
       return fail(WF_EINVAL, "wf_set_launch_shape(k_conv): a a power of two, a*b a multiple "
                              "of 32 and at most 256, c in 1..16");
-  } else if ((a != 1 && a != 2 && a != 4) || (b != 1 && b != 2 && b != 4 && b != 8) || c != 1) {
-    return fail(WF_EINVAL, "wf_set_launch_shape(k_rbgs_split): a in {1,2,4}, b in {1,2,4,8}, c = 1");
+  } else if ((a != 1 && a != 2 && a != 4 && a != 8) || (b != 1 && b != 2 && b != 4 && b != 8) ||
+             c != 1) {
+    return fail(WF_EINVAL,
+                "wf_set_launch_shape(k_rbgs_split): a in {1,2,4,8}, b in {1,2,4,8}, c = 1");
   }
   g_shape[kind][n][0] = a;
   g_shape[kind][n][1] = b;

@@ -149,7 +149,7 @@ CONV_SHAPES = tuple((a, b, c) for a, b in ((32, 8), (16, 16), (64, 4), (32, 4), 
                                            (128, 2), (32, 2), (8, 32))
                     for c in (1, 2, 4, 8))
 # k_rbgs_split: cells per thread, rows per CTA
-SPLIT_SHAPES = tuple((c, r, 1) for c in (1, 2, 4) for r in (2, 4, 8))
+SPLIT_SHAPES = tuple((c, r, 1) for c in (1, 2, 4, 8) for r in (1, 2, 4, 8))
 _KIND = {"conv": SHAPE_CONV, "split": SHAPE_SPLIT}
 
 
