@@ -154,8 +154,9 @@ NCU_TRAFFIC = {("k_rbgs_split", 256): (189163264, "profiles/rbgs_split_256_full.
 
 def kernel_roofline(sol, args, peak, peak_kind):
     """The dominant kernel of the step (largest share of the step's launch
-    list), timed live with CUDA events on the launching stream after the
-    timed region.  Level 0 of 80^3 and larger (FP64): the split half-sweep
+    list), timed live with CUDA events after the timed region, as replays of
+    a CUDA graph of its launches (the form the step runs them in: host
+    launch overhead is not counted).  Level 0 of 80^3 and larger (FP64): the split half-sweep
     -- relax(6) and relax(12) differ by exactly 12 half-sweep launches, so
     their difference isolates the kernel; its algorithmic bytes are 1.5 words
     per cell (read the other colour, read the own colour's rhs, write the own
@@ -178,17 +179,36 @@ def kernel_roofline(sol, args, peak, peak_kind):
     return _coarse_roofline(mg, args, peak, peak_kind), None
 
 
-def _timed_relax(mg, l, sweeps, reps):
+def _timed_graph(fn, reps):
+    """Seconds per call of `fn` (kernel launches on the current stream),
+    timed as replays of a CUDA graph that captured one call -- the form the
+    step runs its kernels in, so host launch overhead is not counted; falls
+    back to timing direct calls if the capture is refused."""
     import torch
-    mg._relax(l, sweeps)
+    fn()
     torch.cuda.synchronize()
+    try:
+        s = torch.cuda.Stream()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(s):
+            with torch.cuda.graph(g, stream=s, capture_error_mode="thread_local"):
+                fn()
+        g.replay()
+        torch.cuda.synchronize()
+        run = g.replay
+    except Exception:
+        run = fn
     a, b = _events()
     a.record()
     for _ in range(reps):
-        mg._relax(l, sweeps)
+        run()
     b.record()
     torch.cuda.synchronize()
-    return a.elapsed_time(b) / reps / 1e3   # s per relax
+    return a.elapsed_time(b) / reps / 1e3
+
+
+def _timed_relax(mg, l, sweeps, reps):
+    return _timed_graph(lambda: mg._relax(l, sweeps), reps)   # s per relax
 
 
 def _roof(name, key, alg, t, peak, peak_kind):
@@ -204,7 +224,7 @@ def _split_roofline(mg, n, peak, peak_kind):
     import numpy as np
     lev0 = mg.levels[0]
     lev0.rhs.assign(np.random.default_rng(7).standard_normal(lev0.shape))
-    t = (_timed_relax(mg, 0, 12, 5) - _timed_relax(mg, 0, 6, 5)) / 12
+    t = (_timed_relax(mg, 0, 12, 20) - _timed_relax(mg, 0, 6, 20)) / 12
     return _roof("k_rbgs_split (level-0 half-sweep, FP64)", ("k_rbgs_split", n),
                  1.5 * n ** 3 * 8, t, peak, peak_kind)
 
@@ -223,21 +243,14 @@ def _coarse_roofline(mg, args, peak, peak_kind):
     # the coarse solve through the precomputed symmetric operator, against
     # the bytes of the work it replaces: n_coarse sweeps of the level
     # (read phi and rhs, write phi: 3 words per cell per sweep)
-    mg._coarse_solve()
-    torch.cuda.synchronize()
-    a, b = _events()
-    a.record()
-    for _ in range(10):
-        mg._coarse_solve()
-    b.record()
-    torch.cuda.synchronize()
-    t = a.elapsed_time(b) / 10 / 1e3
+    t = _timed_graph(mg._coarse_solve, 10)
     N = nc ** 3
     out = _roof("coarse %d^3 relax via the symmetric operator (k_cop_vg + k_cop_gemm + "
                 "k_cop_out + 2 k_rbgs)" % nc, ("cop", nc), 300 * 3 * N * 8, t, peak, peak_kind)
     out["note"] = ("alg_bytes = the reference's 300 sweeps of the level (3 words per cell "
                    "per sweep); the operator form moves far fewer, so frac is the sweeps' "
-                   "equivalent bandwidth, timed through the harness (k_zero + the kernels)")
+                   "equivalent bandwidth, timed through the harness (k_zero + the kernels) as "
+                   "CUDA-graph replays")
     return out
 
 
