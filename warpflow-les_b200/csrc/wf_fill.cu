@@ -2,11 +2,14 @@
 //
 // The reference issues each fill as an ordered list of face launches
 // (bcs.py:201-311), and later faces read what earlier faces wrote at edges
-// and corners, so the corner values depend on the order.  The faces of one
-// axis never touch each other (for n >= 4), so the list splits into three
-// ordered phases -- x faces, y faces, z faces -- and each phase runs as one
-// launch in which a thread owns one (a, b) line of every face op of that
-// phase and walks its layers in order.  Up to three fields share a launch.
+// and corners, so the corner values depend on the order.  Up to n = 256 a
+// fill runs as ONE launch of its composed program (k_fill_one, below): the
+// host composes the ordered face ops into independent gathers.  Larger
+// fills use the ordered form: the faces of one axis never touch each other
+// (for n >= 4), so the list splits into three ordered phases -- x faces, y
+// faces, z faces -- and each phase runs as one launch (k_fill_phase) in
+// which a thread owns one (a, b) line of every face op of that phase and
+// walks its layers in order.  Up to three fields share a launch either way.
 #include <algorithm>
 #include <cstdlib>
 #include <functional>
