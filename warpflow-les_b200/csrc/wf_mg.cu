@@ -1476,11 +1476,15 @@ template <> struct Vec2<float> { using type = float2; };
 // Y_s[x][g] = sum over the s-th slice of B cells u of C[x][u] * V[g][u]:
 // a CTA takes COP_RB representatives x and one slice, and first copies the
 // slice of every permuted copy V[g] into shared memory (each CTA reads it
-// once from L2; the operator rows are read once in all); warp w takes the
+// once from L2; the operator rows are read once in all) -- COP_SB loads per
+// thread issued before any is stored, a few rounds of L2 latency instead of
+// one per element (the 20^3 relax 28.8 -> 24.7 us); warp w takes the
 // representatives x0 + 2w, x0 + 2w + 1 and every symmetry; lanes step
 // through the slice two cells at a time (2-vector loads), each summing its
 // cells in ascending order, then the lanes are added by a butterfly (fixed
 // order)
+constexpr int COP_SB = 16;   // staging loads in flight per thread
+
 template <class T>
 __global__ void __launch_bounds__(256) k_cop_gemm(const T* C, const T* V, T* Y, int nrep,
                                                   int M, int ng, const Batch bt) {
@@ -1498,9 +1502,22 @@ __global__ void __launch_bounds__(256) k_cop_gemm(const T* C, const T* V, T* Y, 
   const int per = (((M + COP_KS - 1) / COP_KS) + 1) & ~1;   // even: 2-vector aligned
   const int h0 = s * per / 2, h1 = min(M, s * per + per) / 2;   // 2-vector range
   const int nh = max(0, h1 - h0);
-  for (int t = threadIdx.x; t < ng * nh; t += blockDim.x) {
-    const int g = t / nh, h = t - g * nh;
-    sv[t] = reinterpret_cast<const V2*>(V + (long)g * M)[h0 + h];
+  const int nv = ng * nh;
+  for (int t0 = threadIdx.x; t0 < nv; t0 += blockDim.x * COP_SB) {
+    V2 buf[COP_SB];
+#pragma unroll
+    for (int b = 0; b < COP_SB; ++b) {
+      const int t = t0 + b * blockDim.x;
+      if (t < nv) {
+        const int g = t / nh, h = t - g * nh;
+        buf[b] = reinterpret_cast<const V2*>(V + (long)g * M)[h0 + h];
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < COP_SB; ++b) {
+      const int t = t0 + b * blockDim.x;
+      if (t < nv) sv[t] = buf[b];
+    }
   }
   __syncthreads();
   const int r0 = x0 + 2 * w;
