@@ -1438,6 +1438,9 @@ __global__ void __launch_bounds__(256) k_cop_vg(const Lvl<T> L0, T* V,
   int c[3] = {0, 0, 0};
   if (on) b_cell(w, n, c[0], c[1], c[2]);
   const int i = c[0], j = c[1], k = c[2];
+  // the cell's own rhs, loaded together with the neighbour's (one round of
+  // memory latency instead of two)
+  const T own = on ? L.rhs[lid(L, i + 1, j + 1, k + 1)] : T(0);
   // the neighbour of this thread's term and the coefficient towards it
   T term = T(0);
   if (on && t < 6) {
@@ -1456,7 +1459,7 @@ __global__ void __launch_bounds__(256) k_cop_vg(const Lvl<T> L0, T* V,
 #pragma unroll
   for (int q = 0; q < 6; ++q) nb[q] = __shfl_sync(0xffffffffu, term, (threadIdx.x & 24) | q);
   T x = T(0);
-  if (on) x = L.rhs[lid(L, i + 1, j + 1, k + 1)] - (nb[0] + nb[1] + nb[2] + nb[3] + nb[4] + nb[5]);
+  if (on) x = own - (nb[0] + nb[1] + nb[2] + nb[3] + nb[4] + nb[5]);
   if (!on) return;
   for (int g = t; g < G.ng; g += 8) {
     int q[3];
