@@ -294,7 +294,12 @@ __global__ void __launch_bounds__(MG_TPB) k_prolong(const Lvl<T> C0, Lvl<T> F0, 
 // the same prolongation with one thread per COARSE cell writing its 2x2x2
 // fine cells from the 27 coarse values around it, each loaded once (27 loads
 // for 8 outputs instead of 64); every output sums the same terms in the
-// same order as k_prolong, so the results are the same bits
+// same order as k_prolong, so the results are the same bits.  The 8 fine
+// values are loaded before the first store: the stores go through the same
+// pointer, so the compiler would otherwise issue each load after the
+// previous cell's store, eight dependent memory round trips per thread.
+// Loading them first is safe because each fine cell is written by this
+// thread only, and ring_mirror writes ring cells, which are never loaded.
 template <class T>
 __global__ void __launch_bounds__(MG_TPB) k_prolong8(const Lvl<T> C0, Lvl<T> F0, const Batch bt) {
   pdl_entry();
@@ -317,6 +322,17 @@ __global__ void __launch_bounds__(MG_TPB) k_prolong8(const Lvl<T> C0, Lvl<T> F0,
 #pragma unroll
       for (int q = 0; q < 3; ++q)
         Q[a][b][q] = C.phi[(long)(ci + a) * C.sI + (long)(cj + b) * C.sJ + kq[q]];
+  long fc[2][2][2];
+  T fv[2][2][2];
+#pragma unroll
+  for (int pi = 0; pi < 2; ++pi)
+#pragma unroll
+    for (int pj = 0; pj < 2; ++pj)
+#pragma unroll
+      for (int pk = 0; pk < 2; ++pk) {
+        fc[pi][pj][pk] = lid(F, 2 * ci + pi + 1, 2 * cj + pj + 1, 2 * ck + pk + 1);
+        fv[pi][pj][pk] = F.phi[fc[pi][pj][pk]];
+      }
 #pragma unroll
   for (int pi = 0; pi < 2; ++pi)
 #pragma unroll
@@ -341,8 +357,8 @@ __global__ void __launch_bounds__(MG_TPB) k_prolong8(const Lvl<T> C0, Lvl<T> F0,
           }
         }
         const int i = 2 * ci + pi, j = 2 * cj + pj, k = 2 * ck + pk;
-        const long c = lid(F, i + 1, j + 1, k + 1);
-        const T x = F.phi[c] + acc;
+        const long c = fc[pi][pj][pk];
+        const T x = fv[pi][pj][pk] + acc;
         F.phi[c] = x;
         if (!F.split) ring_mirror(F, i, j, k, c, x);
       }
@@ -1739,8 +1755,10 @@ __global__ void __launch_bounds__(32 * SPLIT_ROWS)
   const long dst = (long)i * L.tI + (long)j * L.tJ;
   for (int a = threadIdx.x & 31; a < m; a += 32) {
     const int q = spos(a, H);
-    sp[dst + q] = L.phi[src + a];
-    if (with_rhs) sr[dst + q] = L.rhs[src + a];
+    const T x = L.phi[src + a];
+    const T y = with_rhs ? L.rhs[src + a] : T(0);   // both loads before the stores
+    sp[dst + q] = x;
+    if (with_rhs) sr[dst + q] = y;
   }
 }
 
@@ -1812,11 +1830,23 @@ __global__ void __launch_bounds__(32 * SPLIT_ROWS)
   if (row >= n * n) return;
   const int i = row / n, j = row - i * n;
   const long r = (long)(i + 1) * L.tI + (long)(j + 1) * L.tJ;
-  for (int k = threadIdx.x & 31; k < n; k += 32) {
-    const T x = sp[r + spos(k + 1, H)];
-    const long c = lid(L, i + 1, j + 1, k + 1);
-    L.phi[c] = x;
-    ring_mirror(L, i, j, k, c, x);
+  // four loads in flight before their stores (the copy and the level are
+  // different buffers; the compiler cannot tell, and would otherwise wait
+  // for each load's round trip after the previous store)
+  for (int k0 = threadIdx.x & 31; k0 < n; k0 += 128) {
+    T x[4];
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+      if (k0 + 32 * b < n) x[b] = sp[r + spos(k0 + 32 * b + 1, H)];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int k = k0 + 32 * b;
+      if (k < n) {
+        const long c = lid(L, i + 1, j + 1, k + 1);
+        L.phi[c] = x[b];
+        ring_mirror(L, i, j, k, c, x[b]);
+      }
+    }
   }
 }
 

@@ -702,13 +702,15 @@ __global__ void __launch_bounds__(TPB) k_calvel(const wf_case c, Geo g, double a
     const int j = NPL + jy_;
     const int i = NPL + bt_z(bt);
     const long id = g.at(i, j, k);
+    // every load before the first store: the stores go through pointers the
+    // compiler cannot separate from the loads, so a load placed after a
+    // store would wait for the round trip of the loads before it
     const double p0 = LD(p, id);
-    if (i < hi)
-      fu[id] = LD(us, id) - div_by_recip(dt * alpha * (LD(p, id + g.sI) - p0), dv.dh[0], dv.yh[0]);
-    if (j < hi)
-      fv[id] = LD(vs, id) - div_by_recip(dt * alpha * (LD(p, id + g.sJ) - p0), dv.dh[1], dv.yh[1]);
-    if (k < hi)
-      fw[id] = LD(ws, id) - div_by_recip(dt * alpha * (LD(p, id + 1) - p0), dv.dh[2], dv.yh[2]);
+    const double pi1 = LD(p, id + g.sI), pj1 = LD(p, id + g.sJ), pk1 = LD(p, id + 1);
+    const double u0 = LD(us, id), v0 = LD(vs, id), w0 = LD(ws, id);
+    if (i < hi) fu[id] = u0 - div_by_recip(dt * alpha * (pi1 - p0), dv.dh[0], dv.yh[0]);
+    if (j < hi) fv[id] = v0 - div_by_recip(dt * alpha * (pj1 - p0), dv.dh[1], dv.yh[1]);
+    if (k < hi) fw[id] = w0 - div_by_recip(dt * alpha * (pk1 - p0), dv.dh[2], dv.yh[2]);
   }
 }
 
