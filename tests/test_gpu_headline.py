@@ -10,7 +10,7 @@ are compared with the FP64 CPU oracle:
 * FP64: every field, ghosts included, within 1e-10 max abs after the first
   step; identical outer-iteration counts every step, the divergence trace
   of every outer iteration within 1e-5 relative, dt within 1e-12 relative;
-  u, v, w within 1e-8 rms at the end (north_star's 100-step tolerance,
+  u, v, w within 1e-8 rms at the end (the solver's 100-step tolerance,
   here after 6 and 200 steps).
 * Mixed-precision multigrid: every step's divergence below div_tolerance
   (1e-6) and u, v, w within 1e-7 rms of the FP64 oracle at the end.

@@ -6,7 +6,7 @@
 Runs `time.n_steps` (or --steps) FlowSolver steps, prints the reference's
 log line every `output.log_interval` steps and writes a snapshot every
 `output.n_out` steps and at the end.  --resume continues from a snapshot
-written by this build.
+written by this package's snapshot writer (it also holds vis and itime).
 
 A case whose `mpi.domains` has more than one sub-domain runs one process
 per rank under torchrun, where the reference runs under mpirun:
