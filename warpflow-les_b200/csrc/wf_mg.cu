@@ -2535,54 +2535,75 @@ static int build_levels(const wf_case& c, T* phi0, const T* rhs0, long sI, long 
 // In exact arithmetic a V-cycle from phi equals phi + V(rhs - A phi), so the
 // FP64 schedule of n_vcycles cycles is reproduced up to FP32 rounding of the
 // corrections; residual and accumulation stay FP64.
-__global__ void __launch_bounds__(MG_TPB) k_defect(const Lvl<double> F0, float* rhs_f,
-                                                   float* phi_f, int n, const Batch bt) {
-  pdl_entry();
-  if (bt_skip(bt)) return;
-  const Lvl<double> F = rebase(F0, bt);
-  if (bt.tab) {
-    rhs_f = (float*)bt.tab[bt_case(bt)].mg_rhs[0];
-    phi_f = (float*)bt.tab[bt_case(bt)].mg_phi[0];
-  }
-  const long m = (long)n + 2;
-  const long tot = (long)n * n * n;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
-       t += (long)gridDim.x * blockDim.x) {
-    const int k = (int)(t % n);
-    const int j = (int)((t / n) % n);
-    const int i = (int)(t / ((long)n * n));
-    const long c = lid(F, i + 1, j + 1, k + 1);
-    const double aw = i > 0 ? F.ax : 0.0, ae = i < n - 1 ? F.ax : 0.0;
-    const double as = j > 0 ? F.ay : 0.0, an = j < n - 1 ? F.ay : 0.0;
-    const double ab = k > 0 ? F.az : 0.0, at = k < n - 1 ? F.az : 0.0;
-    const double ap = -(aw + ae + as + an + ab + at);
-    const double* p = F.phi;
-    const double r = F.rhs[c] - (aw * p[c - F.sI] + ae * p[c + F.sI] + as * p[c - F.sJ] +
-                                 an * p[c + F.sJ] + ab * p[c - 1] + at * p[c + 1] + ap * p[c]);
-    const long cf = ((long)(i + 1) * m + (j + 1)) * m + (k + 1);
-    rhs_f[cf] = (float)r;
-  }
-  // the FP32 correction starts from zero, ring included
-  const long all = m * m * m;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < all;
-       t += (long)gridDim.x * blockDim.x)
-    phi_f[t] = 0.0f;
+// One thread per real cell (x = k in runs of 32, y = j in groups of 8, z = i),
+// as the other stencil kernels: no 64-bit index division per cell.
+__device__ __forceinline__ double defect_at(const Lvl<double>& F, int n, int i, int j, int k) {
+  const long c = lid(F, i + 1, j + 1, k + 1);
+  const double aw = i > 0 ? F.ax : 0.0, ae = i < n - 1 ? F.ax : 0.0;
+  const double as = j > 0 ? F.ay : 0.0, an = j < n - 1 ? F.ay : 0.0;
+  const double ab = k > 0 ? F.az : 0.0, at = k < n - 1 ? F.az : 0.0;
+  const double ap = -(aw + ae + as + an + ab + at);
+  const double* p = F.phi;
+  return F.rhs[c] - (aw * p[c - F.sI] + ae * p[c + F.sI] + as * p[c - F.sJ] +
+                     an * p[c + F.sJ] + ab * p[c - 1] + at * p[c + 1] + ap * p[c]);
 }
 
-__global__ void k_correct(const Lvl<double> F0, const float* phi_f, int n, const Batch bt) {
+// zero cell (i, j, k) (0-based real index) of an FP32 level array and the
+// ring cells nearest to it (faces, edges, corners), so that the real cells'
+// threads together zero every cell of the (n+2)^3 array exactly once
+__device__ __forceinline__ void zero_with_ring(const Lvl<float>& L, int n, int i, int j, int k) {
+  const int zi0 = i == 0 ? -1 : 0, zi1 = i == n - 1 ? 1 : 0;
+  const int zj0 = j == 0 ? -1 : 0, zj1 = j == n - 1 ? 1 : 0;
+  const int zk0 = k == 0 ? -1 : 0, zk1 = k == n - 1 ? 1 : 0;
+  for (int oi = zi0; oi <= zi1; ++oi)
+    for (int oj = zj0; oj <= zj1; ++oj)
+      for (int ok = zk0; ok <= zk1; ++ok) L.phi[lid(L, i + 1 + oi, j + 1 + oj, k + 1 + ok)] = 0.0f;
+}
+
+// Lf: the FP32 level 0 (its own arrays, or with LV_SPLIT its split copies)
+__global__ void __launch_bounds__(MG_TPB) k_defect(const Lvl<double> F0, const Lvl<float> Lf0,
+                                                   const Batch bt) {
   pdl_entry();
   if (bt_skip(bt)) return;
   const Lvl<double> F = rebase(F0, bt);
-  if (bt.tab) phi_f = (const float*)bt.tab[bt_case(bt)].mg_phi[0];
-  const long m = (long)n + 2;
-  const long tot = m * m * m;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot;
-       t += (long)gridDim.x * blockDim.x) {
-    const int k = (int)(t % m);
-    const int j = (int)((t / m) % m);
-    const int i = (int)(t / (m * m));
-    F.phi[lid(F, i, j, k)] += (double)phi_f[t];
+  const Lvl<float> Lf = rebase(Lf0, bt);
+  const int n = F.n;
+  const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
+  if (k >= n || j >= n) return;
+  const int i = bt_z(bt);
+  const double r = defect_at(F, n, i, j, k);
+  const_cast<float*>(Lf.rhs)[lid(Lf, i + 1, j + 1, k + 1)] = (float)r;
+  // the FP32 correction starts from zero, ring included
+  zero_with_ring(Lf, n, i, j, k);
+}
+
+// phi += the FP32 correction over the real cells and the ring.  With a split
+// Lf the correction is read from the split copy, and the ring gets exactly
+// what copying it back would have left in the level's own array: the face
+// ring the value of the real cell next to it, edges and corners zero.
+__global__ void k_correct(const Lvl<double> F0, const Lvl<float> Lf0, const Batch bt) {
+  pdl_entry();
+  if (bt_skip(bt)) return;
+  const Lvl<double> F = rebase(F0, bt);
+  const Lvl<float> Lf = rebase(Lf0, bt);
+  const int n = F.n, m = n + 2;
+  const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
+  if (k >= m || j >= m) return;
+  const int i = bt_z(bt);
+  float v;
+  if (Lf.split) {
+    const int oi = i == 0 || i == m - 1, oj = j == 0 || j == m - 1, ok = k == 0 || k == m - 1;
+    v = 0.0f;
+    if (oi + oj + ok <= 1) {
+      const int ri = i == 0 ? 1 : (i == m - 1 ? n : i);
+      const int rj = j == 0 ? 1 : (j == m - 1 ? n : j);
+      const int rk = k == 0 ? 1 : (k == m - 1 ? n : k);
+      v = Lf.phi[lid(Lf, ri, rj, rk)];
+    }
+  } else {
+    v = Lf.phi[lid(Lf, i, j, k)];
   }
+  F.phi[lid(F, i, j, k)] += (double)v;
 }
 
 static int build_levels_f32(const wf_case& c, std::vector<Lvl<float>>& lv) {
@@ -2613,13 +2634,15 @@ static int build_levels_f32(const wf_case& c, std::vector<Lvl<float>>& lv) {
 
 static int dc_cycle(const Lvl<double>& F, std::vector<Lvl<float>>& lvf, const wf_case& c,
                     cudaStream_t s) {
-  const int n = F.n;
-  WF_CK(launch_k(k_defect, mg_blocks((long)n * n * n), MG_TPB, 0, s, F, const_cast<float*>(lvf[0].rhs),
-                                                       lvf[0].phi, n));
+  const int n = F.n, m = n + 2;
+  // a split-resident FP32 level 0 stays in its split copy from the defect to
+  // the correction: no copy into the split layout and none back
+  const bool sp = lvf.size() > 1 && split_resident(lvf[0], c);
+  const Lvl<float> Lf = sp ? split_view(lvf[0]) : lvf[0];
+  WF_CK(launch_k(k_defect, cells3(n, n, n), cell_block(), 0, s, F, Lf));
   WF_CKL("k_defect");
-  WF_TRY(vcycle<float>(lvf, c, s));
-  const long m = (long)n + 2;
-  WF_CK(launch_k(k_correct, mg_blocks(m * m * m), MG_TPB, 0, s, F, lvf[0].phi, n));
+  WF_TRY(vcycle<float>(lvf, c, s, sp, sp, sp));
+  WF_CK(launch_k(k_correct, cells3(m, m, m), cell_block(), 0, s, F, Lf));
   WF_CKL("k_correct");
   return WF_OK;
 }
